@@ -1,0 +1,202 @@
+/*
+ * stwo_b200: C ABI of the B200 (sm_100a) backend for the stwo-zig circle-STARK
+ * prover. A Zig backend type (or any FFI caller) binds these functions the way
+ * src/backends/cuda/ffi.zig binds the stwo-cuda prototypes; INTEGRATION.md
+ * shows the binding.
+ *
+ * Conventions
+ *  - Every function returns int32_t status: 0 = STWO_B200_OK, negative = error.
+ *    stwo_b200_last_error() returns a message for the calling thread's last error.
+ *    (The stwo-cuda precedent returns void, src/backends/cuda/ffi.zig:43-70.)
+ *  - M31 columns are uint32_t canonical values in bit-reversed circle-domain
+ *    order. A column set is (base, stride): column c starts at base + c * stride
+ *    (src/backends/cpu_scalar/mod.zig:185-197).
+ *  - QM31 values are stwo_b200_qm31 {a, b, c, d} = (c0.a, c0.b, c1.a, c1.b),
+ *    the layout of CudaQM31 (src/backends/cuda/ffi.zig:12-21).
+ *  - Secure (QM31) columns are 4 coordinate columns (SecureColumnByCoords,
+ *    src/backend/secure_column.zig).
+ *  - Hashes are 32 bytes. Merkle layer buffers hold 2^(L+1)-1 hashes: the 2^L
+ *    leaves first, then each parent layer, the root last.
+ *  - Op-level functions take DEVICE pointers and a cudaStream_t (as void*); they
+ *    enqueue work and return without synchronizing unless stated.
+ *  - Handles are released only by their *_destroy function; no function frees
+ *    caller buffers (ownership rules of src/prover/engine.zig:28-31).
+ */
+#ifndef STWO_B200_H
+#define STWO_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define STWO_B200_OK 0
+#define STWO_B200_E_INVALID (-1)
+#define STWO_B200_E_OOM (-2)
+#define STWO_B200_E_CUDA (-3)
+#define STWO_B200_E_TIMEOUT (-4)
+#define STWO_B200_E_CONSTRAINTS (-5)
+#define STWO_B200_E_BUFFER_TOO_SMALL (-6)
+#define STWO_B200_E_FALLBACK (-7)
+#define STWO_B200_E_NO_DEVICE (-8)
+
+typedef struct stwo_b200_context stwo_b200_context;
+
+typedef struct {
+  uint32_t a, b, c, d;
+} stwo_b200_qm31;
+
+/* PcsConfig (src/core/pcs/mod.zig:23-52) with FriConfig fold_step 1 and no lifting override. */
+typedef struct {
+  uint32_t pow_bits;
+  uint32_t log_blowup_factor;
+  uint32_t log_last_layer_degree_bound;
+  uint32_t n_queries;
+} stwo_b200_pcs_config;
+
+/* Wide-Fibonacci proving request: the Statement (src/examples/wide_fibonacci/trace.zig:18-21)
+ * plus the prepared trace. Exactly one trace source is used, in this order: trace_device,
+ * trace_host, generated (trace_kind 0 = the reference's (1, row) seeds, 1 = seeded uniform
+ * col0/col1 in [0, p-1)). has_channel_seed mixes channel_seed (mixU64) right after the
+ * statement; 0 keeps the reference transcript. */
+typedef struct {
+  uint32_t log_n_rows;
+  uint32_t sequence_len;
+  stwo_b200_pcs_config config;
+  const uint32_t* trace_host;
+  const uint32_t* trace_device;
+  uint32_t trace_kind;
+  uint32_t has_channel_seed;
+  uint64_t trace_seed;
+  uint64_t channel_seed;
+} stwo_b200_wide_fib_request;
+
+/* Device time per proving stage, in milliseconds. */
+typedef struct {
+  float upload, trace, main_commit, composition, composition_commit, oods, quotients, fri, pow, decommit, total;
+} stwo_b200_stage_times;
+
+/* ---- Runtime --------------------------------------------------------------------------------- */
+
+/* Creates a context on `device`: point tables and twiddle towers for domains up to 2^23
+ * (M31TwiddleTower, src/prover/poly/twiddle_tower.zig:29-81; Metal initializeRuntime,
+ * src/backends/metal/commit_backend.zig). */
+int32_t stwo_b200_context_create(int32_t device, stwo_b200_context** out);
+int32_t stwo_b200_context_destroy(stwo_b200_context* ctx);
+const char* stwo_b200_last_error(void);
+const char* stwo_b200_status_string(int32_t status);
+/* Library version string (build identity). */
+const char* stwo_b200_version(void);
+
+/* ---- Engine level ------------------------------------------------------------------------------ */
+
+/* One proof; writes the JSON wire bytes (src/interop/proof_wire.zig:19-77). Replaces
+ * ProverEngine(B,...).prove for the wide-Fibonacci AIR (src/prover/engine.zig:163-181 via
+ * src/examples/wide_fibonacci.zig:200-220 provePreparedWithEngine). If `proof_cap` is too small
+ * the call returns STWO_B200_E_BUFFER_TOO_SMALL with *proof_len set. `times` may be NULL. */
+int32_t stwo_b200_prove_wide_fibonacci(stwo_b200_context* ctx, const stwo_b200_wide_fib_request* req,
+                                       uint8_t* proof_out, size_t proof_cap, size_t* proof_len,
+                                       stwo_b200_stage_times* times);
+
+/* Batched proving: n independent requests, up to `max_in_flight` proofs resident and
+ * overlapping on the device (one stream and workspace each). statuses[i] and proof_lens[i]
+ * are per request; the call returns STWO_B200_OK when every request succeeded. */
+int32_t stwo_b200_prove_wide_fibonacci_batch(stwo_b200_context* ctx, const stwo_b200_wide_fib_request* reqs,
+                                             size_t n, uint8_t* const* proof_outs, const size_t* proof_caps,
+                                             size_t* proof_lens, int32_t* statuses, uint32_t max_in_flight);
+
+/* ---- PolyOps (src/backend/poly_ops.zig:12-24) --------------------------------------------------- */
+
+/* In-place interpolation (evaluations -> coefficients) of n_cols columns on CanonicCoset(log_size).
+ * Replaces interpolateCircleBuffers (src/prover/pcs/columns/circle_transforms.zig:212) and
+ * ntt_b2n_column (src/backends/cuda/ffi.zig:52). */
+int32_t stwo_b200_interpolate_columns(stwo_b200_context* ctx, uint32_t log_size, uint32_t n_cols, uint32_t* cols,
+                                      uint64_t stride, void* stream);
+/* In-place evaluation (coefficients -> evaluations) on CanonicCoset(log_size). Replaces
+ * evaluateCircleBuffers (circle_transforms.zig:248) and ntt_n2b_columns (ffi.zig:51). */
+int32_t stwo_b200_evaluate_columns(stwo_b200_context* ctx, uint32_t log_size, uint32_t n_cols, uint32_t* cols,
+                                   uint64_t stride, void* stream);
+/* Evaluations on CanonicCoset(log_size) -> coefficients and evaluations on
+ * CanonicCoset(log_size + log_blowup), fused. Replaces interpolateAndEvaluateCircleBuffers
+ * (src/backends/cpu_scalar/mod.zig:185-266, src/prover/pcs/columns/preparation.zig:212-352). */
+int32_t stwo_b200_interpolate_and_extend(stwo_b200_context* ctx, uint32_t log_size, uint32_t log_blowup,
+                                         uint32_t n_cols, const uint32_t* evals, uint64_t evals_stride,
+                                         uint32_t* coeffs, uint64_t coeffs_stride, uint32_t* lde,
+                                         uint64_t lde_stride, void* stream);
+/* Coefficients -> evaluations on CanonicCoset(log_size + log_blowup) (evaluateExtensionBufferWithTwiddles,
+ * src/prover/poly/circle/transforms.zig:132-147; extendCoefficientColumnsByGroupForBackend,
+ * src/prover/pcs/commit_polys.zig:33). */
+int32_t stwo_b200_extend_columns(stwo_b200_context* ctx, uint32_t log_size, uint32_t log_blowup, uint32_t n_cols,
+                                 const uint32_t* coeffs, uint64_t coeffs_stride, uint32_t* lde, uint64_t lde_stride,
+                                 void* stream);
+/* Value of each coefficient column at a QM31 circle point (CircleCoefficients.evalAtPoint,
+ * src/prover/poly/circle/poly.zig:62-230; evaluateCoefficientPlans hook,
+ * src/prover/pcs/sampled_values.zig:68; eval_at_point / batch_eval_at_points, ffi.zig:55,:89).
+ * out_dev: n_cols QM31 on the device. Allocates its scratch from the stream's pool. */
+int32_t stwo_b200_eval_at_point(stwo_b200_context* ctx, uint32_t log_size, uint32_t n_cols, const uint32_t* coeffs,
+                                uint64_t stride, stwo_b200_qm31 px, stwo_b200_qm31 py, stwo_b200_qm31* out_dev,
+                                void* stream);
+
+/* ---- MerkleOps (src/backend/merkle_ops.zig:20-56) ------------------------------------------------ */
+
+/* Blake2s lifted Merkle commitment of n_cols columns of 2^log_size rows ("leaf"/"node" prefixed
+ * hasher, src/core/vcs_lifted/blake2_merkle.zig). layers_dev: 2^(log_size+1)-1 hashes. root_host
+ * (nullable) receives the root after the stream synchronizes. Replaces commitMerkle
+ * (merkle_ops.zig:20-56, src/prover/vcs_lifted/prover.zig:61-70) and commit_on_first_layer_in_gpu /
+ * commit_on_layer_in_gpu (ffi.zig:69-70). */
+int32_t stwo_b200_merkle_commit(stwo_b200_context* ctx, uint32_t log_size, uint32_t n_cols, const uint32_t* cols,
+                                uint64_t stride, uint8_t* layers_dev, uint8_t* root_host, void* stream);
+
+/* ---- FriOps (src/backend/fri_ops.zig:19-37) ------------------------------------------------------ */
+
+/* dst = dst * alpha^2 + fold(src) when accumulate, else fold(src); src 4 coordinate columns of
+ * 2^src_log on CanonicCoset(src_log), dst 4 columns of 2^(src_log-1). Replaces foldCircleIntoLine
+ * (src/core/fri/folding.zig:558-602; fold_circle_into_line, ffi.zig:62). */
+int32_t stwo_b200_fold_circle_into_line(stwo_b200_context* ctx, uint32_t src_log, const uint32_t* src,
+                                        uint64_t src_stride, stwo_b200_qm31 alpha, uint32_t* dst,
+                                        uint64_t dst_stride, int32_t accumulate, void* stream);
+/* One fold of a line evaluation of 2^src_log on the line domain halfOdds(src_log) (the FRI
+ * inner-layer tower). Replaces foldLine (folding.zig:352-384; fold_line, ffi.zig:61). */
+int32_t stwo_b200_fold_line(stwo_b200_context* ctx, uint32_t src_log, const uint32_t* src, uint64_t src_stride,
+                            stwo_b200_qm31 alpha, uint32_t* dst, uint64_t dst_stride, void* stream);
+
+/* ---- QuotientOps (src/backend/quotient_ops.zig:10-16) ------------------------------------------- */
+
+/* DEEP quotient of columns sampled at one point, on CanonicCoset(log_size) in bit-reversed order:
+ * out(row) = (sum_i c_i v_i(row) - (sum_a y + sum_b)) / ((Re Px - x) Im Py - (Re Py - y) Im Px).
+ * col_ptrs_dev: device array of n_cols device pointers; c_dev: n_cols QM31 line coefficients c
+ * (random-coefficient scaled), sum_a / sum_b the batch's summed a and b line coefficients
+ * (src/core/pcs/quotients/row_evaluation.zig:71-101,400-521). Replaces accumulateQuotients and
+ * accumulate_quotients (ffi.zig:94). */
+int32_t stwo_b200_accumulate_quotients(stwo_b200_context* ctx, uint32_t log_size, uint32_t n_cols,
+                                       const uint32_t* const* col_ptrs_dev, const stwo_b200_qm31* c_dev,
+                                       stwo_b200_qm31 px, stwo_b200_qm31 py, stwo_b200_qm31 sum_a,
+                                       stwo_b200_qm31 sum_b, uint32_t* out, uint64_t out_stride, void* stream);
+
+/* ---- Wide-Fibonacci AIR -------------------------------------------------------------------------- */
+
+/* Trace generation in bit-reversed circle order (fillQuadraticRecurrenceTrace hook,
+ * src/examples/wide_fibonacci/trace.zig:63-74; generate_wide_fibonacci_trace, ffi.zig:263). */
+int32_t stwo_b200_wide_fib_trace(stwo_b200_context* ctx, uint32_t log_n_rows, uint32_t sequence_len,
+                                 uint32_t trace_kind, uint64_t seed, uint32_t* out, uint64_t stride, void* stream);
+/* Composition evaluation on CanonicCoset(log_n_rows+1): out (4 columns) = sum_k coeffs[k] *
+ * (c_k - a_k^2 - b_k^2) * den_inv[row >> log_n_rows] (computeCompositionEvaluation hook,
+ * src/prover/air/component_prover.zig:269; src/examples/wide_fibonacci/component.zig:138-236). */
+int32_t stwo_b200_wide_fib_composition(stwo_b200_context* ctx, uint32_t log_n_rows, uint32_t sequence_len,
+                                       const uint32_t* eval, uint64_t stride, const stwo_b200_qm31* coeffs_dev,
+                                       uint32_t den_inv0, uint32_t den_inv1, uint32_t* out, uint64_t out_stride,
+                                       void* stream);
+
+/* ---- Channel proof of work ---------------------------------------------------------------------- */
+
+/* Lowest nonce whose Blake2s(prefix_digest || LE64 nonce) has >= n_bits trailing zero bits in its
+ * first 16 bytes (src/core/channel/blake2s.zig:135-240). Synchronous. */
+int32_t stwo_b200_pow_grind(stwo_b200_context* ctx, const uint8_t prefix_digest[32], uint32_t n_bits,
+                            uint64_t* nonce_out);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* STWO_B200_H */

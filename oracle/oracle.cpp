@@ -474,7 +474,11 @@ uint64_t pow_grind(const Hash& digest, uint32_t n_bits, int n_threads) {
   if (n_bits == 0) return 0;
   Hash prefix = pow_prefix(digest, n_bits);
   std::atomic<uint64_t> found(~0ull);
-  if (n_threads < 1) n_threads = 1;
+#ifdef _OPENMP
+  if (n_threads < 1) n_threads = omp_get_max_threads();
+#else
+  n_threads = 1;
+#endif
 #pragma omp parallel num_threads(n_threads)
   {
     int tid = 0, nt = 1;

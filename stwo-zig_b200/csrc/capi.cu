@@ -1,0 +1,310 @@
+// C ABI of libstwo_b200 (declarations and reference citations: include/stwo_b200.h).
+#include <atomic>
+#include <cstring>
+#include <string>
+#include <thread>
+#include <vector>
+
+#include "../../include/stwo_b200.h"
+#include "prover.hpp"
+
+struct stwo_b200_context {
+  sb::Context ctx;
+};
+
+namespace {
+
+thread_local std::string g_last_error;
+
+int32_t set_error(int32_t code, const std::string& msg) {
+  g_last_error = msg;
+  return code;
+}
+
+#define CK_CTX(c)                                                      \
+  do {                                                                 \
+    if (!(c)) return set_error(STWO_B200_E_INVALID, "null context");   \
+    cudaSetDevice((c)->ctx.device);                                    \
+  } while (0)
+
+int32_t cuda_status(cudaError_t e, const char* what) {
+  if (e == cudaSuccess) return STWO_B200_OK;
+  return set_error(STWO_B200_E_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+inline sb::QM31 q(stwo_b200_qm31 v) { return sb::qmake(v.a, v.b, v.c, v.d); }
+inline cudaStream_t st(void* s) { return reinterpret_cast<cudaStream_t>(s); }
+
+constexpr uint32_t TOWER_LOG = 22;  // domains up to 2^23
+
+sb::ProveRequest to_request(const stwo_b200_wide_fib_request& r) {
+  sb::ProveRequest p;
+  p.log_n_rows = r.log_n_rows;
+  p.sequence_len = r.sequence_len;
+  p.config.pow_bits = r.config.pow_bits;
+  p.config.log_blowup_factor = r.config.log_blowup_factor;
+  p.config.log_last_layer_degree_bound = r.config.log_last_layer_degree_bound;
+  p.config.n_queries = r.config.n_queries;
+  p.trace_host = r.trace_host;
+  p.trace_device = r.trace_device;
+  p.trace_kind = (int)r.trace_kind;
+  p.trace_seed = r.trace_seed;
+  p.has_channel_seed = r.has_channel_seed != 0;
+  p.channel_seed = r.channel_seed;
+  return p;
+}
+
+bool domain_ok(const stwo_b200_context* c, uint32_t log_size) {
+  return log_size >= 1 && log_size <= c->ctx.tables.tower_log + 1;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* stwo_b200_last_error(void) { return g_last_error.c_str(); }
+const char* stwo_b200_status_string(int32_t s) { return sb::status_string(s); }
+const char* stwo_b200_version(void) { return "stwo_b200 0.1 sm_100a"; }
+
+int32_t stwo_b200_context_create(int32_t device, stwo_b200_context** out) {
+  if (!out) return set_error(STWO_B200_E_INVALID, "null output");
+  *out = nullptr;
+  auto* c = new stwo_b200_context();
+  int32_t rc = c->ctx.init(device, TOWER_LOG);
+  if (rc != STWO_B200_OK) {
+    delete c;
+    return set_error(rc, std::string("context init failed: ") + sb::status_string(rc));
+  }
+  *out = c;
+  return STWO_B200_OK;
+}
+
+int32_t stwo_b200_context_destroy(stwo_b200_context* ctx) {
+  if (!ctx) return STWO_B200_OK;
+  cudaSetDevice(ctx->ctx.device);
+  cudaDeviceSynchronize();
+  delete ctx;
+  return STWO_B200_OK;
+}
+
+int32_t stwo_b200_prove_wide_fibonacci(stwo_b200_context* ctx, const stwo_b200_wide_fib_request* req,
+                                       uint8_t* proof_out, size_t proof_cap, size_t* proof_len,
+                                       stwo_b200_stage_times* times) {
+  CK_CTX(ctx);
+  if (!req) return set_error(STWO_B200_E_INVALID, "null request");
+  sb::WideFibProver* p = ctx->ctx.acquire();
+  if (!p) return set_error(STWO_B200_E_CUDA, "stream creation failed");
+  std::string proof;
+  sb::StageTimes t;
+  int32_t rc = p->prove(to_request(*req), proof, times ? &t : nullptr);
+  std::string err = p->error();
+  ctx->ctx.release(p);
+  if (rc != STWO_B200_OK) return set_error(rc, err);
+  if (times) std::memcpy(times, &t, sizeof(t));
+  if (proof_len) *proof_len = proof.size();
+  if (!proof_out || proof_cap < proof.size()) return set_error(STWO_B200_E_BUFFER_TOO_SMALL, "proof buffer too small");
+  std::memcpy(proof_out, proof.data(), proof.size());
+  return STWO_B200_OK;
+}
+
+int32_t stwo_b200_prove_wide_fibonacci_batch(stwo_b200_context* ctx, const stwo_b200_wide_fib_request* reqs,
+                                             size_t n, uint8_t* const* proof_outs, const size_t* proof_caps,
+                                             size_t* proof_lens, int32_t* statuses, uint32_t max_in_flight) {
+  CK_CTX(ctx);
+  if (n == 0) return STWO_B200_OK;
+  if (!reqs || !proof_outs || !proof_caps || !proof_lens || !statuses)
+    return set_error(STWO_B200_E_INVALID, "null batch argument");
+  if (max_in_flight == 0) max_in_flight = 1;
+  std::atomic<size_t> next(0);
+  std::vector<std::string> errors(n);
+  auto worker = [&]() {
+    cudaSetDevice(ctx->ctx.device);
+    sb::WideFibProver* p = ctx->ctx.acquire();
+    for (;;) {
+      size_t i = next.fetch_add(1);
+      if (i >= n) break;
+      if (!p) { statuses[i] = STWO_B200_E_CUDA; continue; }
+      std::string proof;
+      int32_t rc = p->prove(to_request(reqs[i]), proof, nullptr);
+      if (rc == STWO_B200_OK) {
+        proof_lens[i] = proof.size();
+        if (proof_outs[i] && proof_caps[i] >= proof.size()) std::memcpy(proof_outs[i], proof.data(), proof.size());
+        else rc = STWO_B200_E_BUFFER_TOO_SMALL;
+      } else {
+        errors[i] = p->error();
+      }
+      statuses[i] = rc;
+    }
+    if (p) ctx->ctx.release(p);
+  };
+  size_t n_threads = std::min<size_t>(max_in_flight, n);
+  std::vector<std::thread> threads;
+  for (size_t t = 1; t < n_threads; ++t) threads.emplace_back(worker);
+  worker();
+  for (auto& t : threads) t.join();
+  for (size_t i = 0; i < n; ++i)
+    if (statuses[i] != STWO_B200_OK) return set_error(statuses[i], "request " + std::to_string(i) + ": " + errors[i]);
+  return STWO_B200_OK;
+}
+
+int32_t stwo_b200_interpolate_columns(stwo_b200_context* ctx, uint32_t log_size, uint32_t n_cols, uint32_t* cols,
+                                      uint64_t stride, void* stream) {
+  CK_CTX(ctx);
+  if (!domain_ok(ctx, log_size) || (!cols && n_cols)) return set_error(STWO_B200_E_INVALID, "bad interpolate arguments");
+  return cuda_status(sb::fft_columns(ctx->ctx.tables, true, log_size, n_cols, cols, stride, st(stream)), "interpolate");
+}
+
+int32_t stwo_b200_evaluate_columns(stwo_b200_context* ctx, uint32_t log_size, uint32_t n_cols, uint32_t* cols,
+                                   uint64_t stride, void* stream) {
+  CK_CTX(ctx);
+  if (!domain_ok(ctx, log_size) || (!cols && n_cols)) return set_error(STWO_B200_E_INVALID, "bad evaluate arguments");
+  return cuda_status(sb::fft_columns(ctx->ctx.tables, false, log_size, n_cols, cols, stride, st(stream)), "evaluate");
+}
+
+int32_t stwo_b200_interpolate_and_extend(stwo_b200_context* ctx, uint32_t log_size, uint32_t log_blowup,
+                                         uint32_t n_cols, const uint32_t* evals, uint64_t evals_stride,
+                                         uint32_t* coeffs, uint64_t coeffs_stride, uint32_t* lde,
+                                         uint64_t lde_stride, void* stream) {
+  CK_CTX(ctx);
+  if (!domain_ok(ctx, log_size + log_blowup) || log_blowup == 0 || log_blowup > 4 || (n_cols && (!evals || !coeffs || !lde)))
+    return set_error(STWO_B200_E_INVALID, "bad interpolate_and_extend arguments");
+  return cuda_status(sb::interpolate_extend(ctx->ctx.tables, log_size, log_blowup, n_cols, evals, evals_stride, coeffs,
+                                            coeffs_stride, lde, lde_stride, st(stream)),
+                     "interpolate_and_extend");
+}
+
+int32_t stwo_b200_extend_columns(stwo_b200_context* ctx, uint32_t log_size, uint32_t log_blowup, uint32_t n_cols,
+                                 const uint32_t* coeffs, uint64_t coeffs_stride, uint32_t* lde, uint64_t lde_stride,
+                                 void* stream) {
+  CK_CTX(ctx);
+  if (!domain_ok(ctx, log_size + log_blowup) || log_blowup == 0 || log_blowup > 4 || (n_cols && (!coeffs || !lde)))
+    return set_error(STWO_B200_E_INVALID, "bad extend arguments");
+  return cuda_status(sb::extend(ctx->ctx.tables, log_size, log_blowup, n_cols, coeffs, coeffs_stride, lde, lde_stride,
+                                st(stream)),
+                     "extend");
+}
+
+int32_t stwo_b200_eval_at_point(stwo_b200_context* ctx, uint32_t log_size, uint32_t n_cols, const uint32_t* coeffs,
+                                uint64_t stride, stwo_b200_qm31 px, stwo_b200_qm31 py, stwo_b200_qm31* out_dev,
+                                void* stream) {
+  CK_CTX(ctx);
+  if (log_size > 28 || (n_cols && (!coeffs || !out_dev))) return set_error(STWO_B200_E_INVALID, "bad eval_at_point arguments");
+  if (n_cols == 0) return STWO_B200_OK;
+  size_t parts = sb::eval_at_point_partial_count(log_size, n_cols);
+  void* scratch = nullptr;
+  cudaError_t e = cudaMallocAsync(&scratch, parts * sizeof(sb::QM31), st(stream));
+  if (e != cudaSuccess) return cuda_status(e, "eval_at_point scratch");
+  e = sb::eval_at_point(ctx->ctx.tables, log_size, n_cols, coeffs, stride, sb::PointQ{q(px), q(py)}, nullptr,
+                        static_cast<sb::QM31*>(scratch), reinterpret_cast<sb::QM31*>(out_dev), st(stream));
+  cudaError_t e2 = cudaFreeAsync(scratch, st(stream));
+  if (e != cudaSuccess) return cuda_status(e, "eval_at_point");
+  return cuda_status(e2, "eval_at_point scratch free");
+}
+
+int32_t stwo_b200_merkle_commit(stwo_b200_context* ctx, uint32_t log_size, uint32_t n_cols, const uint32_t* cols,
+                                uint64_t stride, uint8_t* layers_dev, uint8_t* root_host, void* stream) {
+  CK_CTX(ctx);
+  if (log_size > 28 || !layers_dev || (n_cols && !cols)) return set_error(STWO_B200_E_INVALID, "bad merkle arguments");
+  if (n_cols == 0) log_size = 0;
+  cudaError_t e = sb::merkle_commit(log_size, n_cols, cols, stride, layers_dev, st(stream));
+  if (e != cudaSuccess) return cuda_status(e, "merkle_commit");
+  if (root_host) {
+    uint64_t root_node = (2ull << log_size) - 2;
+    e = cudaMemcpyAsync(root_host, layers_dev + root_node * 32, 32, cudaMemcpyDeviceToHost, st(stream));
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st(stream));
+    return cuda_status(e, "merkle root readback");
+  }
+  return STWO_B200_OK;
+}
+
+int32_t stwo_b200_fold_circle_into_line(stwo_b200_context* ctx, uint32_t src_log, const uint32_t* src,
+                                        uint64_t src_stride, stwo_b200_qm31 alpha, uint32_t* dst,
+                                        uint64_t dst_stride, int32_t accumulate, void* stream) {
+  CK_CTX(ctx);
+  if (!domain_ok(ctx, src_log) || src_log < 2 || !src || !dst) return set_error(STWO_B200_E_INVALID, "bad fold arguments");
+  return cuda_status(sb::fold_circle_into_line(ctx->ctx.tables, src_log, src, src_stride, q(alpha), dst, dst_stride,
+                                               accumulate != 0, st(stream)),
+                     "fold_circle_into_line");
+}
+
+int32_t stwo_b200_fold_line(stwo_b200_context* ctx, uint32_t src_log, const uint32_t* src, uint64_t src_stride,
+                            stwo_b200_qm31 alpha, uint32_t* dst, uint64_t dst_stride, void* stream) {
+  CK_CTX(ctx);
+  if (src_log < 1 || !domain_ok(ctx, src_log + 1) || !src || !dst) return set_error(STWO_B200_E_INVALID, "bad fold arguments");
+  return cuda_status(sb::fold_line(ctx->ctx.tables, src_log, src, src_stride, q(alpha), dst, dst_stride, st(stream)),
+                     "fold_line");
+}
+
+int32_t stwo_b200_accumulate_quotients(stwo_b200_context* ctx, uint32_t log_size, uint32_t n_cols,
+                                       const uint32_t* const* col_ptrs_dev, const stwo_b200_qm31* c_dev,
+                                       stwo_b200_qm31 px, stwo_b200_qm31 py, stwo_b200_qm31 sum_a,
+                                       stwo_b200_qm31 sum_b, uint32_t* out, uint64_t out_stride, void* stream) {
+  CK_CTX(ctx);
+  if (!domain_ok(ctx, log_size) || n_cols == 0 || n_cols > 1024 || !col_ptrs_dev || !c_dev || !out)
+    return set_error(STWO_B200_E_INVALID, "bad quotient arguments");
+  sb::QuotientBatchDev hb;
+  hb.point = sb::PointQ{q(px), q(py)};
+  hb.sum_a = q(sum_a);
+  hb.sum_b = q(sum_b);
+  hb.first = 0;
+  hb.count = n_cols;
+  void* dbatch = nullptr;
+  cudaError_t e = cudaMallocAsync(&dbatch, sizeof(hb), st(stream));
+  if (e != cudaSuccess) return cuda_status(e, "quotient batch");
+  e = cudaMemcpyAsync(dbatch, &hb, sizeof(hb), cudaMemcpyHostToDevice, st(stream));
+  if (e == cudaSuccess)
+    e = sb::accumulate_quotients(ctx->ctx.tables, log_size, 1, static_cast<sb::QuotientBatchDev*>(dbatch), col_ptrs_dev,
+                                 reinterpret_cast<const sb::QM31*>(c_dev), out, out_stride, st(stream));
+  cudaError_t e2 = cudaStreamSynchronize(st(stream));  // the batch descriptor lives on this host frame
+  cudaFreeAsync(dbatch, st(stream));
+  if (e != cudaSuccess) return cuda_status(e, "accumulate_quotients");
+  return cuda_status(e2, "accumulate_quotients sync");
+}
+
+int32_t stwo_b200_wide_fib_trace(stwo_b200_context* ctx, uint32_t log_n_rows, uint32_t sequence_len,
+                                 uint32_t trace_kind, uint64_t seed, uint32_t* out, uint64_t stride, void* stream) {
+  CK_CTX(ctx);
+  if (log_n_rows == 0 || log_n_rows > 28 || sequence_len < 2 || !out || trace_kind > 1)
+    return set_error(STWO_B200_E_INVALID, "bad trace arguments");
+  return cuda_status(sb::wide_fib_trace(log_n_rows, sequence_len, (int)trace_kind, seed, out, stride, st(stream)),
+                     "wide_fib_trace");
+}
+
+int32_t stwo_b200_wide_fib_composition(stwo_b200_context* ctx, uint32_t log_n_rows, uint32_t sequence_len,
+                                       const uint32_t* eval, uint64_t stride, const stwo_b200_qm31* coeffs_dev,
+                                       uint32_t den_inv0, uint32_t den_inv1, uint32_t* out, uint64_t out_stride,
+                                       void* stream) {
+  CK_CTX(ctx);
+  if (log_n_rows == 0 || log_n_rows > 27 || sequence_len < 3 || sequence_len > 3000 || !eval || !coeffs_dev || !out)
+    return set_error(STWO_B200_E_INVALID, "bad composition arguments");
+  return cuda_status(sb::wide_fib_composition(log_n_rows, sequence_len, eval, stride,
+                                              reinterpret_cast<const sb::QM31*>(coeffs_dev), den_inv0, den_inv1, out,
+                                              out_stride, st(stream)),
+                     "wide_fib_composition");
+}
+
+int32_t stwo_b200_pow_grind(stwo_b200_context* ctx, const uint8_t prefix_digest[32], uint32_t n_bits,
+                            uint64_t* nonce_out) {
+  CK_CTX(ctx);
+  if (!prefix_digest || !nonce_out || n_bits > 64) return set_error(STWO_B200_E_INVALID, "bad pow arguments");
+  if (n_bits == 0) { *nonce_out = 0; return STWO_B200_OK; }
+  cudaStream_t s = ctx->ctx.stream;
+  void* res = nullptr;
+  cudaError_t e = cudaMallocAsync(&res, 16, s);
+  if (e != cudaSuccess) return cuda_status(e, "pow result");
+  uint32_t w[8];
+  std::memcpy(w, prefix_digest, 32);
+  uint64_t max_nonce = n_bits >= 48 ? ~0ull : (1ull << (n_bits + 16));
+  e = sb::pow_grind(w, n_bits, max_nonce, static_cast<uint32_t*>(res), s);
+  uint32_t host[3] = {0, 0, 0};
+  if (e == cudaSuccess) e = cudaMemcpyAsync(host, res, 12, cudaMemcpyDeviceToHost, s);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  cudaFreeAsync(res, s);
+  if (e != cudaSuccess) return cuda_status(e, "pow_grind");
+  uint64_t nonce = (uint64_t)host[0] | ((uint64_t)host[1] << 32);
+  if (nonce == ~0ull) return set_error(STWO_B200_E_TIMEOUT, "proof-of-work search bound reached");
+  *nonce_out = nonce;
+  return STWO_B200_OK;
+}
+
+}  // extern "C"

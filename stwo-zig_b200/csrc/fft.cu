@@ -1,0 +1,370 @@
+// Circle FFT over M31 columns, B200 layout.
+//
+// Semantics: the reference's butterfly network (src/prover/poly/circle/transforms.zig:
+// evaluate :132-248, interpolate :249-362, first-layer [y,-y,-x,x] twiddles
+// :233-247/:309-321, extension :132-147). A transform of 2^D words has D layers;
+// layer s pairs indices at distance 2^s (s = 0 is the circle layer, s >= 1 line
+// layer s-1) and uses twiddle block h = i >> (s+1).
+//
+// Decomposition: with b = min(D, LOW_BITS), layers s < b act inside aligned
+// blocks of 2^b words (k_fft_low: one CTA per block, shared memory), layers
+// s >= b act on the strided sets {g*T + t + m*2^b} (k_fft_high: one CTA per
+// group of T adjacent low indices, all m). Both passes apply two layers per
+// shared-memory round trip (radix-4 quads in registers).
+// interpolate_extend fuses, per strided set: inverse high layers -> 1/n scale ->
+// store coefficients -> extension to the blown-up domain -> forward high layers,
+// so coefficients and the blown-up evaluations come out of one pass.
+#include <algorithm>
+
+#include "kernels.cuh"
+
+namespace sb {
+
+namespace {
+
+constexpr uint32_t LOW_BITS = 11;          // low-pass block: 2^11 words = 8 KiB
+constexpr uint32_t LOW_THREADS = 256;
+constexpr uint32_t HIGH_T_BITS = 3;        // T = 8 adjacent columns of the strided view (32 B rows)
+constexpr uint32_t HIGH_T = 1u << HIGH_T_BITS;
+constexpr uint32_t HIGH_THREADS = 512;
+
+__device__ __forceinline__ uint32_t twiddle(const TwiddleView& tv, uint32_t s, uint32_t gi) {
+  return s == 0 ? tv.circ(gi >> 1) : tv.line(s, gi >> (s + 1));
+}
+
+// Applies layers [s_lo, s_hi) to a shared array of 2^local_bits words whose
+// local index l maps to global index base + l (low pass).
+template <bool INV>
+__device__ void low_layers(uint32_t* sm, uint32_t local_bits, uint64_t base, const TwiddleView& tv,
+                           uint32_t s_lo, uint32_t s_hi) {
+  const uint32_t n = 1u << local_bits;
+  uint32_t nl = s_hi - s_lo;
+  // Radix-2 leftover layer first (forward: the top one; inverse: the bottom one).
+  if (nl & 1) {
+    uint32_t s = INV ? s_lo : s_hi - 1;
+    for (uint32_t q = threadIdx.x; q < n / 2; q += blockDim.x) {
+      uint32_t l0 = ((q >> s) << (s + 1)) | (q & ((1u << s) - 1));
+      uint32_t l1 = l0 + (1u << s);
+      uint32_t t = twiddle(tv, s, (uint32_t)(base + l0));
+      uint32_t a = sm[l0], b = sm[l1];
+      if (INV) ibutterfly(a, b, t); else butterfly(a, b, t);
+      sm[l0] = a; sm[l1] = b;
+    }
+    __syncthreads();
+    if (INV) s_lo += 1; else s_hi -= 1;
+    nl -= 1;
+  }
+  for (uint32_t k = 0; k < nl / 2; ++k) {
+    uint32_t s = INV ? s_lo + 2 * k : s_hi - 2 - 2 * k;  // pair (s, s+1)
+    for (uint32_t q = threadIdx.x; q < n / 4; q += blockDim.x) {
+      uint32_t l0 = ((q >> s) << (s + 2)) | (q & ((1u << s) - 1));
+      uint32_t l1 = l0 + (1u << s), l2 = l0 + (2u << s), l3 = l2 + (1u << s);
+      uint32_t g0 = (uint32_t)(base + l0), g2 = (uint32_t)(base + l2);
+      uint32_t tb = twiddle(tv, s + 1, g0);
+      uint32_t ta0 = twiddle(tv, s, g0), ta2 = twiddle(tv, s, g2);
+      uint32_t v0 = sm[l0], v1 = sm[l1], v2 = sm[l2], v3 = sm[l3];
+      if (INV) {
+        ibutterfly(v0, v1, ta0); ibutterfly(v2, v3, ta2);
+        ibutterfly(v0, v2, tb); ibutterfly(v1, v3, tb);
+      } else {
+        butterfly(v0, v2, tb); butterfly(v1, v3, tb);
+        butterfly(v0, v1, ta0); butterfly(v2, v3, ta2);
+      }
+      sm[l0] = v0; sm[l1] = v1; sm[l2] = v2; sm[l3] = v3;
+    }
+    __syncthreads();
+  }
+}
+
+// Low pass: grid (n_blocks, n_cols). Loads block blockIdx.x of 2^block_bits words
+// (a source column holding only 2^src_valid_bits words is zero-extended), applies
+// layers [0, block_bits) and an optional scale, stores to dst.
+template <bool INV>
+__global__ void k_fft_low(const uint32_t* __restrict__ src, uint64_t src_stride, uint32_t src_valid_bits,
+                          uint32_t* dst, uint64_t dst_stride, uint32_t block_bits, TwiddleView tv,
+                          uint32_t scale) {
+  extern __shared__ uint32_t sm[];
+  const uint32_t n = 1u << block_bits;
+  const uint64_t base = (uint64_t)blockIdx.x << block_bits;
+  const uint32_t* s = src + blockIdx.y * src_stride;
+  const uint32_t valid = src_valid_bits >= block_bits ? n : (1u << src_valid_bits);
+  for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) sm[i] = i < valid ? s[base + i] : 0u;
+  __syncthreads();
+  low_layers<INV>(sm, block_bits, base, tv, 0, block_bits);
+  uint32_t* d = dst + blockIdx.y * dst_stride;
+  for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) {
+    uint32_t v = sm[i];
+    if (scale) v = mmul(v, scale);
+    d[base + i] = v;
+  }
+}
+
+// High-pass shared layout: sm[m * T + t] is global index m*2^b + g*T + t.
+// Applies layers [s_lo, s_hi) (global s >= b) over rows [0, 2^(row_bits)).
+template <bool INV>
+__device__ void high_layers(uint32_t* sm, uint32_t row_bits, uint32_t b, const TwiddleView& tv,
+                            uint32_t s_lo, uint32_t s_hi) {
+  const uint32_t rows = 1u << row_bits;
+  uint32_t nl = s_hi - s_lo;
+  if (nl & 1) {
+    uint32_t s = INV ? s_lo : s_hi - 1;
+    uint32_t r = s - b;  // row distance 2^r
+    for (uint32_t q = threadIdx.x; q < (rows / 2) * HIGH_T; q += blockDim.x) {
+      uint32_t t = q & (HIGH_T - 1), p = q >> HIGH_T_BITS;
+      uint32_t m0 = ((p >> r) << (r + 1)) | (p & ((1u << r) - 1));
+      uint32_t m1 = m0 + (1u << r);
+      uint32_t tw = tv.line(s, m0 >> (r + 1));
+      uint32_t a = sm[m0 * HIGH_T + t], c = sm[m1 * HIGH_T + t];
+      if (INV) ibutterfly(a, c, tw); else butterfly(a, c, tw);
+      sm[m0 * HIGH_T + t] = a; sm[m1 * HIGH_T + t] = c;
+    }
+    __syncthreads();
+    if (INV) s_lo += 1; else s_hi -= 1;
+    nl -= 1;
+  }
+  for (uint32_t k = 0; k < nl / 2; ++k) {
+    uint32_t s = INV ? s_lo + 2 * k : s_hi - 2 - 2 * k;
+    uint32_t r = s - b;
+    for (uint32_t q = threadIdx.x; q < (rows / 4) * HIGH_T; q += blockDim.x) {
+      uint32_t t = q & (HIGH_T - 1), p = q >> HIGH_T_BITS;
+      uint32_t m0 = ((p >> r) << (r + 2)) | (p & ((1u << r) - 1));
+      uint32_t m1 = m0 + (1u << r), m2 = m0 + (2u << r), m3 = m2 + (1u << r);
+      uint32_t tb = tv.line(s + 1, m0 >> (r + 2));
+      uint32_t ta0 = tv.line(s, m0 >> (r + 1)), ta2 = tv.line(s, m2 >> (r + 1));
+      uint32_t v0 = sm[m0 * HIGH_T + t], v1 = sm[m1 * HIGH_T + t], v2 = sm[m2 * HIGH_T + t], v3 = sm[m3 * HIGH_T + t];
+      if (INV) {
+        ibutterfly(v0, v1, ta0); ibutterfly(v2, v3, ta2);
+        ibutterfly(v0, v2, tb); ibutterfly(v1, v3, tb);
+      } else {
+        butterfly(v0, v2, tb); butterfly(v1, v3, tb);
+        butterfly(v0, v1, ta0); butterfly(v2, v3, ta2);
+      }
+      sm[m0 * HIGH_T + t] = v0; sm[m1 * HIGH_T + t] = v1; sm[m2 * HIGH_T + t] = v2; sm[m3 * HIGH_T + t] = v3;
+    }
+    __syncthreads();
+  }
+}
+
+struct HighParams {
+  const uint32_t* src; uint64_t src_stride; uint32_t src_log;  // 2^(src_log - b) rows valid
+  uint32_t b;
+  // inverse phase (optional): layers [b, src_log), then scale, then store to coef
+  int do_inverse; TwiddleView itv; uint32_t scale; uint32_t* coef; uint64_t coef_stride;
+  // forward phase (optional): domain out_log >= src_log, rows beyond src rows are
+  // duplicated when out_log == src_log + 1 (top layer skipped) and zero otherwise.
+  int do_forward; TwiddleView ftv; uint32_t out_log; uint32_t* out; uint64_t out_stride;
+};
+
+// Grid (2^b / T groups, n_cols).
+__global__ void k_fft_high(HighParams p) {
+  extern __shared__ uint32_t sm[];
+  const uint32_t g = blockIdx.x, col = blockIdx.y;
+  const uint32_t in_rows = 1u << (p.src_log - p.b);
+  const uint32_t* s = p.src + col * p.src_stride + g * HIGH_T;
+  for (uint32_t i = threadIdx.x; i < in_rows * HIGH_T; i += blockDim.x) {
+    uint32_t m = i >> HIGH_T_BITS, t = i & (HIGH_T - 1);
+    sm[i] = s[((uint64_t)m << p.b) + t];
+  }
+  __syncthreads();
+  if (p.do_inverse) {
+    high_layers<true>(sm, p.src_log - p.b, p.b, p.itv, p.b, p.src_log);
+    if (p.scale) {
+      for (uint32_t i = threadIdx.x; i < in_rows * HIGH_T; i += blockDim.x) sm[i] = mmul(sm[i], p.scale);
+      __syncthreads();
+    }
+    if (p.coef) {
+      uint32_t* c = p.coef + col * p.coef_stride + g * HIGH_T;
+      for (uint32_t i = threadIdx.x; i < in_rows * HIGH_T; i += blockDim.x) {
+        uint32_t m = i >> HIGH_T_BITS, t = i & (HIGH_T - 1);
+        c[((uint64_t)m << p.b) + t] = sm[i];
+      }
+    }
+  }
+  if (p.do_forward) {
+    const uint32_t out_rows = 1u << (p.out_log - p.b);
+    uint32_t s_hi = p.out_log;
+    if (p.out_log == p.src_log + 1) {
+      // The top layer pairs each value with a zero: it duplicates the lower half.
+      for (uint32_t i = threadIdx.x; i < in_rows * HIGH_T; i += blockDim.x) sm[in_rows * HIGH_T + i] = sm[i];
+      s_hi = p.src_log;
+    } else {
+      for (uint32_t i = in_rows * HIGH_T + threadIdx.x; i < out_rows * HIGH_T; i += blockDim.x) sm[i] = 0;
+    }
+    __syncthreads();
+    high_layers<false>(sm, p.out_log - p.b, p.b, p.ftv, p.b, s_hi);
+    uint32_t* o = p.out + col * p.out_stride + g * HIGH_T;
+    for (uint32_t i = threadIdx.x; i < out_rows * HIGH_T; i += blockDim.x) {
+      uint32_t m = i >> HIGH_T_BITS, t = i & (HIGH_T - 1);
+      o[((uint64_t)m << p.b) + t] = sm[i];
+    }
+  } else if (!p.coef) {
+    // pure forward/inverse in place without extension: store back to src layout
+    uint32_t* o = p.out + col * p.out_stride + g * HIGH_T;
+    for (uint32_t i = threadIdx.x; i < in_rows * HIGH_T; i += blockDim.x) {
+      uint32_t m = i >> HIGH_T_BITS, t = i & (HIGH_T - 1);
+      o[((uint64_t)m << p.b) + t] = sm[i];
+    }
+  }
+}
+
+__global__ void k_build_tower(PointTable pts, uint32_t R, uint32_t* tw, uint32_t* itw) {
+  // Entry e < 2^R - 1 belongs to layer k with offset 2^R - 2^(R-k).
+  uint64_t total = 1ull << R;
+  for (uint64_t e = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; e < total; e += (uint64_t)gridDim.x * blockDim.x) {
+    if (e == total - 1) { tw[e] = 1; itw[e] = 1; continue; }
+    // k = number of leading ones of e in R bits
+    uint32_t k = 0;
+    while ((e >> (R - 1 - k)) & 1) ++k;
+    uint64_t off = total - (total >> k);
+    uint32_t i = (uint32_t)(e - off);
+    uint32_t len_log = R - 1 - k;  // layer has 2^len_log entries
+    Coset c = coset_half_odds(R - k);
+    uint32_t nat = bitrev(i, len_log);
+    uint32_t x = pts.at(c.index_at(nat)).x;
+    tw[e] = x;
+    itw[e] = minv(x);
+  }
+}
+
+inline uint32_t inv_pow2(uint32_t log) { return minv(1u << log); }
+
+}  // namespace
+
+TwiddleView DeviceTables::view(uint32_t domain_log, bool inverse) const {
+  TwiddleView v;
+  v.tower = inverse ? itw : tw;
+  v.root_log = tower_log;
+  v.line_log = domain_log - 1;
+  v.y0 = 0;
+  if (domain_log <= 2) {
+    // y of halfOdds(L)'s first point, from the host point table.
+    static std::vector<PointM> host_pts = build_point_table();
+    PointTable pt{host_pts.data()};
+    Coset c = coset_half_odds(domain_log - 1);
+    uint32_t y = pt.at(c.initial).y;
+    v.y0 = inverse ? minv(y) : y;
+  }
+  return v;
+}
+
+cudaError_t build_twiddle_tower(DeviceTables& t, uint32_t root_log, cudaStream_t stream) {
+  k_build_tower<<<1024, 256, 0, stream>>>(PointTable{t.points}, root_log, t.tw, t.itw);
+  t.tower_log = root_log;
+  return cudaGetLastError();
+}
+
+static cudaError_t launch_low(const DeviceTables& t, bool inverse, uint32_t domain_log, uint32_t n_cols,
+                              const uint32_t* src, uint64_t src_stride, uint32_t src_valid_log, uint32_t* dst,
+                              uint64_t dst_stride, uint32_t scale, cudaStream_t stream) {
+  uint32_t b = std::min(domain_log, LOW_BITS);
+  dim3 grid(1u << (domain_log - b), n_cols);
+  size_t smem = (size_t)4 << b;
+  TwiddleView tv = t.view(domain_log, inverse);
+  if (inverse)
+    k_fft_low<true><<<grid, LOW_THREADS, smem, stream>>>(src, src_stride, src_valid_log, dst, dst_stride, b, tv, scale);
+  else
+    k_fft_low<false><<<grid, LOW_THREADS, smem, stream>>>(src, src_stride, src_valid_log, dst, dst_stride, b, tv, scale);
+  return cudaGetLastError();
+}
+
+static cudaError_t launch_high(const HighParams& p, uint32_t n_cols, cudaStream_t stream) {
+  uint32_t rows_log = std::max(p.src_log, p.do_forward ? p.out_log : p.src_log) - p.b;
+  size_t smem = ((size_t)HIGH_T * 4) << rows_log;
+  static bool attr_set = false;
+  if (!attr_set) {
+    cudaFuncSetAttribute(k_fft_high, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+    attr_set = true;
+  }
+  dim3 grid((1u << p.b) / HIGH_T, n_cols);
+  k_fft_high<<<grid, HIGH_THREADS, smem, stream>>>(p);
+  return cudaGetLastError();
+}
+
+cudaError_t fft_columns(const DeviceTables& t, bool inverse, uint32_t log_size, uint32_t n_cols, uint32_t* cols,
+                        uint64_t stride, cudaStream_t stream) {
+  if (n_cols == 0) return cudaSuccess;
+  const uint32_t b = std::min(log_size, LOW_BITS);
+  const uint32_t scale = inverse ? inv_pow2(log_size) : 0;
+  if (log_size <= b)
+    return launch_low(t, inverse, log_size, n_cols, cols, stride, log_size, cols, stride, scale, stream);
+  HighParams p{};
+  p.src = cols; p.src_stride = stride; p.src_log = log_size; p.b = b;
+  p.out = cols; p.out_stride = stride;
+  if (inverse) {
+    cudaError_t e = launch_low(t, true, log_size, n_cols, cols, stride, log_size, cols, stride, 0, stream);
+    if (e != cudaSuccess) return e;
+    p.do_inverse = 1; p.itv = t.view(log_size, true); p.scale = scale; p.coef = cols; p.coef_stride = stride;
+    return launch_high(p, n_cols, stream);
+  }
+  p.do_forward = 1; p.ftv = t.view(log_size, false); p.out_log = log_size;
+  // out_log == src_log: no duplication, all layers [b, log_size)
+  cudaError_t e = launch_high(p, n_cols, stream);
+  if (e != cudaSuccess) return e;
+  return launch_low(t, false, log_size, n_cols, cols, stride, log_size, cols, stride, 0, stream);
+}
+
+cudaError_t extend(const DeviceTables& t, uint32_t log_size, uint32_t log_blowup, uint32_t n_cols,
+                   const uint32_t* coeffs, uint64_t co_stride, uint32_t* lde, uint64_t lde_stride,
+                   cudaStream_t stream) {
+  if (n_cols == 0) return cudaSuccess;
+  const uint32_t out_log = log_size + log_blowup;
+  const uint32_t b = std::min(out_log, LOW_BITS);
+  if (out_log <= b)  // single low pass with zero extension
+    return launch_low(t, false, out_log, n_cols, coeffs, co_stride, log_size, lde, lde_stride, 0, stream);
+  HighParams p{};
+  p.b = b;
+  if (log_size >= b) {
+    p.src = coeffs; p.src_stride = co_stride; p.src_log = log_size;
+  } else {
+    // Tiny source: zero-extend to 2^b first through a low pass of the identity (no layers).
+    p.src = coeffs; p.src_stride = co_stride; p.src_log = log_size;
+  }
+  if (log_size < b) {
+    // Route: treat the coefficient column as rows of the strided view with only
+    // the first 2^log_size words non-zero. Build a zero-extended copy in lde.
+    // lde[0 .. 2^b) = coeffs, rest zero; then forward high + low on lde.
+    cudaError_t e = cudaMemset2DAsync(lde, lde_stride * 4, 0, (size_t)4 << out_log, n_cols, stream);
+    if (e != cudaSuccess) return e;
+    e = cudaMemcpy2DAsync(lde, lde_stride * 4, coeffs, co_stride * 4, (size_t)4 << log_size, n_cols,
+                          cudaMemcpyDeviceToDevice, stream);
+    if (e != cudaSuccess) return e;
+    return fft_columns(t, false, out_log, n_cols, lde, lde_stride, stream);
+  }
+  p.do_forward = 1; p.ftv = t.view(out_log, false); p.out_log = out_log; p.out = lde; p.out_stride = lde_stride;
+  cudaError_t e = launch_high(p, n_cols, stream);
+  if (e != cudaSuccess) return e;
+  return launch_low(t, false, out_log, n_cols, lde, lde_stride, out_log, lde, lde_stride, 0, stream);
+}
+
+cudaError_t interpolate_extend(const DeviceTables& t, uint32_t log_size, uint32_t log_blowup, uint32_t n_cols,
+                               const uint32_t* evals, uint64_t ev_stride, uint32_t* coeffs, uint64_t co_stride,
+                               uint32_t* lde, uint64_t lde_stride, cudaStream_t stream) {
+  if (n_cols == 0) return cudaSuccess;
+  const uint32_t b = std::min(log_size, LOW_BITS);
+  const uint32_t out_log = log_size + log_blowup;
+  if (log_size <= b || out_log > LOW_BITS + 12) {
+    // Small domains (or unsupported fused sizes): separate transforms.
+    if (coeffs != evals) {
+      cudaError_t e = cudaMemcpy2DAsync(coeffs, co_stride * 4, evals, ev_stride * 4, (size_t)4 << log_size, n_cols,
+                                        cudaMemcpyDeviceToDevice, stream);
+      if (e != cudaSuccess) return e;
+    }
+    cudaError_t e = fft_columns(t, true, log_size, n_cols, coeffs, co_stride, stream);
+    if (e != cudaSuccess) return e;
+    return extend(t, log_size, log_blowup, n_cols, coeffs, co_stride, lde, lde_stride, stream);
+  }
+  // 1. inverse low layers: evals -> coeffs (partial)
+  cudaError_t e = launch_low(t, true, log_size, n_cols, evals, ev_stride, log_size, coeffs, co_stride, 0, stream);
+  if (e != cudaSuccess) return e;
+  // 2. inverse high layers + scale -> coeffs; extension + forward high layers -> lde
+  HighParams p{};
+  p.src = coeffs; p.src_stride = co_stride; p.src_log = log_size; p.b = b;
+  p.do_inverse = 1; p.itv = t.view(log_size, true); p.scale = inv_pow2(log_size); p.coef = coeffs; p.coef_stride = co_stride;
+  p.do_forward = 1; p.ftv = t.view(out_log, false); p.out_log = out_log; p.out = lde; p.out_stride = lde_stride;
+  e = launch_high(p, n_cols, stream);
+  if (e != cudaSuccess) return e;
+  // 3. forward low layers on lde in place
+  return launch_low(t, false, out_log, n_cols, lde, lde_stride, out_log, lde, lde_stride, 0, stream);
+}
+
+}  // namespace sb

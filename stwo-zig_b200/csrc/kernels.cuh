@@ -1,0 +1,125 @@
+// Launch interface of the device kernels. Every launcher enqueues on `stream`
+// and returns the launch status; none synchronizes.
+//
+// Column sets are (base, stride) pairs: column c starts at base + c * stride
+// (the reference CPU backend's column view, src/backends/cpu_scalar/mod.zig:185-197).
+// Columns hold canonical M31 words in bit-reversed circle-domain order.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#include "circle.cuh"
+#include "field.cuh"
+
+namespace sb {
+
+// Per-device read-only tables.
+struct DeviceTables {
+  PointM* points = nullptr;    // point table (circle.cuh)
+  uint32_t* tw = nullptr;      // forward twiddle tower
+  uint32_t* itw = nullptr;     // inverse twiddle tower
+  uint32_t tower_log = 0;      // R: root half coset halfOdds(R)
+  TwiddleView view(uint32_t domain_log, bool inverse) const;
+};
+
+// Builds the twiddle towers for root log R on the device (one-time).
+cudaError_t build_twiddle_tower(DeviceTables& t, uint32_t root_log, cudaStream_t stream);
+
+// ---- Circle FFT (src/prover/poly/circle/transforms.zig) -------------------
+// In-place forward (evaluate) or inverse (interpolate, scaled by 1/n) transform
+// of n_cols columns on CanonicCoset(log_size).
+cudaError_t fft_columns(const DeviceTables& t, bool inverse, uint32_t log_size, uint32_t n_cols,
+                        uint32_t* cols, uint64_t stride, cudaStream_t stream);
+// Evaluations on CanonicCoset(log_size) -> coefficients (written to `coeffs`)
+// and their evaluations on CanonicCoset(log_size + log_blowup) (written to `lde`).
+// `evals` may alias `coeffs`. `coeffs` may be null when the caller only needs `lde`
+// (then `scratch` of n_cols * 2^log_size words must be given).
+cudaError_t interpolate_extend(const DeviceTables& t, uint32_t log_size, uint32_t log_blowup,
+                               uint32_t n_cols, const uint32_t* evals, uint64_t ev_stride,
+                               uint32_t* coeffs, uint64_t co_stride, uint32_t* lde,
+                               uint64_t lde_stride, cudaStream_t stream);
+// Coefficients (2^log_size) -> evaluations on CanonicCoset(log_size + log_blowup).
+cudaError_t extend(const DeviceTables& t, uint32_t log_size, uint32_t log_blowup, uint32_t n_cols,
+                   const uint32_t* coeffs, uint64_t co_stride, uint32_t* lde, uint64_t lde_stride,
+                   cudaStream_t stream);
+
+// ---- Lifted Blake2s Merkle (src/prover/vcs_lifted/leaves.zig, layers.zig) --
+// Leaves of n_cols equal-size columns (2^log_size rows) plus all node layers.
+// `layers` holds 2^(log_size+1) - 1 hashes: leaves first (2^log_size), then
+// each parent layer, the root last. n_cols == 0 gives the empty-tree root.
+cudaError_t merkle_commit(uint32_t log_size, uint32_t n_cols, const uint32_t* cols, uint64_t stride,
+                          uint8_t* layers, cudaStream_t stream);
+// Leaves of columns with mixed log sizes (lifted), columns in leaf order
+// (stably sorted by log size ascending), pointers and logs in device memory.
+cudaError_t merkle_commit_lifted(uint32_t max_log, uint32_t n_cols, const uint32_t* const* col_ptrs,
+                                 const uint32_t* col_logs, uint8_t* layers, cudaStream_t stream);
+SB_HD uint64_t merkle_layer_offset(uint32_t max_log, uint32_t layer_log) {
+  // layer with 2^layer_log nodes starts after the larger layers
+  return (1ull << (max_log + 1)) - (1ull << (layer_log + 1));
+}
+
+// ---- Wide-Fibonacci composition (src/examples/wide_fibonacci/component.zig:138-236)
+// out: 4 coordinate columns of 2^(log_n+1). `eval` holds the W trace columns on
+// CanonicCoset(log_n + 1). `coeffs` has W-2 QM31 (constraint k uses coeffs[k]).
+cudaError_t wide_fib_composition(uint32_t log_n, uint32_t W, const uint32_t* eval, uint64_t stride,
+                                 const QM31* coeffs_dev, uint32_t den_inv0, uint32_t den_inv1,
+                                 uint32_t* out, uint64_t out_stride, cudaStream_t stream);
+
+// ---- OODS evaluation of coefficient columns at a QM31 point ---------------
+// partial: scratch of n_cols * ceil(2^log_size / 4096) QM31; out: n_cols QM31 (device).
+cudaError_t eval_at_point(const DeviceTables& t, uint32_t log_size, uint32_t n_cols, const uint32_t* coeffs,
+                          uint64_t stride, PointQ p, QM31* factors_dev, QM31* partial, QM31* out,
+                          cudaStream_t stream);
+size_t eval_at_point_partial_count(uint32_t log_size, uint32_t n_cols);
+
+// ---- DEEP quotients (src/core/pcs/quotients/row_evaluation.zig) -----------
+struct QuotientBatchDev {
+  PointQ point;          // sample point
+  QM31 sum_a, sum_b;     // batch linear term
+  uint32_t first, count; // range in the column/coefficient lists
+};
+// Single-size quotient: all columns have log size `log_size` (the lifting size).
+// col_ptrs/coeff_c are device arrays of length n_entries; batches device array.
+cudaError_t accumulate_quotients(const DeviceTables& t, uint32_t log_size, uint32_t n_batches,
+                                 const QuotientBatchDev* batches, const uint32_t* const* col_ptrs,
+                                 const QM31* coeff_c, uint32_t* out, uint64_t out_stride,
+                                 cudaStream_t stream);
+
+// ---- FRI folds (src/core/fri/folding.zig:352-602) --------------------------
+cudaError_t fold_circle_into_line(const DeviceTables& t, uint32_t src_log, const uint32_t* src,
+                                  uint64_t src_stride, QM31 alpha, uint32_t* dst, uint64_t dst_stride,
+                                  bool accumulate, cudaStream_t stream);
+// Line domain of the source: halfOdds(first_line_log) doubled (first_line_log - src_log) times.
+cudaError_t fold_line(const DeviceTables& t, uint32_t src_log, const uint32_t* src, uint64_t src_stride,
+                      QM31 alpha, uint32_t* dst, uint64_t dst_stride, cudaStream_t stream);
+
+// ---- Proof of work (src/core/channel/blake2s.zig:135-240) ------------------
+// result[0..1] = lowest valid nonce (u64), result[2] = status (0 ok, 1 gave up).
+cudaError_t pow_grind(const uint32_t prefix_words[8], uint32_t n_bits, uint64_t max_nonce,
+                      uint32_t* result_dev, cudaStream_t stream);
+
+// ---- Trace generation (src/examples/wide_fibonacci/trace.zig:34-162) -------
+cudaError_t wide_fib_trace(uint32_t log_n, uint32_t W, int kind, uint64_t seed, uint32_t* out,
+                           uint64_t stride, cudaStream_t stream);
+
+// ---- Gathers for decommitment ----------------------------------------------
+struct GatherItem {
+  const uint32_t* src;  // word source (device)
+  uint64_t index;       // word index
+};
+cudaError_t gather_words(const GatherItem* items, uint32_t n, uint32_t* out, cudaStream_t stream);
+struct HashGatherItem {
+  const uint8_t* layers;  // tree layer buffer
+  uint64_t node;          // global node index in the buffer (hash units)
+};
+cudaError_t gather_hashes(const HashGatherItem* items, uint32_t n, uint8_t* out, cudaStream_t stream);
+
+// ---- LogUp fraction / prefix scan (a20) ------------------------------------
+// out (4 coord columns): cumulative sum in coset order of 1/(z - sum_j alpha^j v_j)
+// (the reference's scalar law), see logup.cu.
+cudaError_t logup_cumsum(uint32_t log_size, uint32_t n_vals, const uint32_t* vals, uint64_t stride,
+                         const uint32_t* mult, QM31 z, QM31 alpha, uint32_t* out, uint64_t out_stride,
+                         QM31* scratch, cudaStream_t stream);
+
+}  // namespace sb

@@ -1,0 +1,225 @@
+// Lifted Blake2s Merkle commitment on the device.
+//
+// Leaf = Blake2s("leaf" prefix block || LE32 of each column value at the row)
+// (src/core/vcs_lifted/blake2_merkle.zig:193-262, src/prover/vcs_lifted/leaves.zig:24-115);
+// node = Blake2s("node" prefix block || left || right) (blake2_merkle.zig:77-130).
+// The prefix block's chaining value is a constant seed, so a leaf costs
+// ceil(4 n_cols / 64) compressions and a node one compression.
+//
+// One thread per leaf: a warp reads 32 consecutive rows of a column as one
+// 128-byte transaction; the message schedule and state stay in registers.
+// Each CTA hashes 256 leaves and then folds them to its subtree root in shared
+// memory (8 node levels), writing every level; the upper levels are folded by
+// k_merkle_nodes, up to 9 levels per launch.
+#include "blake2s.cuh"
+#include "kernels.cuh"
+
+namespace sb {
+
+namespace {
+
+constexpr uint32_t LEAF_THREADS = 256;  // leaves per CTA
+constexpr uint32_t LEAF_LEVELS = 8;     // node levels folded inside a leaf CTA
+constexpr uint32_t NODE_THREADS = 256;  // parents per CTA at the first level
+
+struct Seeds { uint32_t leaf[8], node[8]; };
+
+Seeds make_seeds() {
+  Seeds s;
+  b2s_prefix_seed("leaf", s.leaf);
+  b2s_prefix_seed("node", s.node);
+  return s;
+}
+
+__device__ __forceinline__ void store_hash(uint8_t* layers, uint64_t node, const uint32_t h[8]) {
+  uint4* d = reinterpret_cast<uint4*>(layers + node * 32);
+  d[0] = make_uint4(h[0], h[1], h[2], h[3]);
+  d[1] = make_uint4(h[4], h[5], h[6], h[7]);
+}
+
+__device__ __forceinline__ void node_hash(const uint32_t seed[8], const uint32_t* l, const uint32_t* r, uint32_t h[8]) {
+  uint32_t m[16];
+#pragma unroll
+  for (int i = 0; i < 8; ++i) { m[i] = l[i]; m[8 + i] = r[i]; }
+#pragma unroll
+  for (int i = 0; i < 8; ++i) h[i] = seed[i];
+  b2s_compress(h, m, 128, true);
+}
+
+// Folds `count` hashes in shared memory (sm[i*8 .. i*8+8)) `levels` times;
+// level j's nodes are written to the layer of log size (top_log - j).
+__device__ void fold_levels(uint32_t* sm, uint32_t count, uint32_t levels, uint8_t* layers, uint32_t max_log,
+                            uint32_t child_log, uint64_t first_child, const uint32_t seed[8]) {
+  for (uint32_t j = 1; j <= levels; ++j) {
+    uint32_t n = count >> j;
+    uint32_t h[8];
+    bool active = threadIdx.x < n;
+    if (active) node_hash(seed, sm + (2 * threadIdx.x) * 8, sm + (2 * threadIdx.x + 1) * 8, h);
+    __syncthreads();
+    if (active) {
+#pragma unroll
+      for (int i = 0; i < 8; ++i) sm[threadIdx.x * 8 + i] = h[i];
+      uint32_t layer_log = child_log - j;
+      uint64_t node = merkle_layer_offset(max_log, layer_log) + (first_child >> j) + threadIdx.x;
+      store_hash(layers, node, h);
+    }
+    __syncthreads();
+  }
+}
+
+__global__ void __launch_bounds__(LEAF_THREADS) k_merkle_leaves(uint32_t log_size, uint32_t n_cols,
+                                                                 const uint32_t* __restrict__ cols, uint64_t stride,
+                                                                 uint8_t* layers, Seeds seeds, uint32_t levels) {
+  __shared__ uint32_t sm[LEAF_THREADS * 8];
+  const uint64_t row = (uint64_t)blockIdx.x * LEAF_THREADS + threadIdx.x;
+  const uint64_t n_rows = 1ull << log_size;
+  uint32_t h[8];
+  if (row < n_rows) {
+#pragma unroll
+    for (int i = 0; i < 8; ++i) h[i] = seeds.leaf[i];
+    const uint32_t n_blocks = (n_cols + 15) / 16;
+    const uint32_t total = 64 + 4 * n_cols;
+    for (uint32_t blk = 0; blk < n_blocks; ++blk) {
+      uint32_t m[16];
+      const uint32_t c0 = blk * 16;
+#pragma unroll
+      for (int i = 0; i < 16; ++i) {
+        uint32_t c = c0 + i;
+        m[i] = c < n_cols ? __ldg(cols + c * stride + row) : 0u;
+      }
+      const bool last = blk + 1 == n_blocks;
+      const uint32_t t = last ? total : 64 + 64 * (blk + 1);
+      b2s_compress(h, m, t, last);
+    }
+    store_hash(layers, row, h);
+#pragma unroll
+    for (int i = 0; i < 8; ++i) sm[threadIdx.x * 8 + i] = h[i];
+  }
+  __syncthreads();
+  uint32_t count = n_rows < LEAF_THREADS ? (uint32_t)n_rows : LEAF_THREADS;
+  fold_levels(sm, count, levels, layers, log_size, log_size, (uint64_t)blockIdx.x * LEAF_THREADS, seeds.node);
+}
+
+// Children layer of log size child_log -> `levels` parent levels; each CTA folds
+// 2 * NODE_THREADS children (or the whole layer when smaller).
+__global__ void __launch_bounds__(NODE_THREADS) k_merkle_nodes(uint8_t* layers, uint32_t max_log, uint32_t child_log,
+                                                                uint32_t levels, Seeds seeds) {
+  __shared__ uint32_t sm[2 * NODE_THREADS * 8];
+  const uint64_t n_children = 1ull << child_log;
+  const uint32_t per_cta = n_children < 2 * NODE_THREADS ? (uint32_t)n_children : 2 * NODE_THREADS;
+  const uint64_t first = (uint64_t)blockIdx.x * per_cta;
+  const uint4* src = reinterpret_cast<const uint4*>(layers + (merkle_layer_offset(max_log, child_log) + first) * 32);
+  for (uint32_t i = threadIdx.x; i < per_cta * 2; i += blockDim.x) {
+    uint4 v = src[i];
+    sm[i * 4 + 0] = v.x; sm[i * 4 + 1] = v.y; sm[i * 4 + 2] = v.z; sm[i * 4 + 3] = v.w;
+  }
+  __syncthreads();
+  fold_levels(sm, per_cta, levels, layers, max_log, child_log, first, seeds.node);
+}
+
+__global__ void k_empty_root(uint8_t* layers, Seeds seeds) {
+  // No columns: the single leaf hashes the prefix block alone, as the final block.
+  uint32_t h[8];
+  b2s_init(h);
+  uint32_t m[16] = {0};
+  m[0] = 0x6661656cu;  // "leaf" little-endian
+  b2s_compress(h, m, 64, true);
+  store_hash(layers, 0, h);
+}
+
+}  // namespace
+
+cudaError_t merkle_commit(uint32_t log_size, uint32_t n_cols, const uint32_t* cols, uint64_t stride,
+                          uint8_t* layers, cudaStream_t stream) {
+  static const Seeds seeds = make_seeds();
+  if (n_cols == 0) {
+    k_empty_root<<<1, 1, 0, stream>>>(layers, seeds);
+    return cudaGetLastError();
+  }
+  const uint64_t n_rows = 1ull << log_size;
+  uint32_t leaf_levels = log_size < LEAF_LEVELS ? log_size : LEAF_LEVELS;
+  uint32_t grid = (uint32_t)((n_rows + LEAF_THREADS - 1) / LEAF_THREADS);
+  k_merkle_leaves<<<grid, LEAF_THREADS, 0, stream>>>(log_size, n_cols, cols, stride, layers, seeds, leaf_levels);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  uint32_t child_log = log_size - leaf_levels;
+  while (child_log > 0) {
+    uint32_t levels = child_log < 9 ? child_log : 9;
+    uint64_t n_children = 1ull << child_log;
+    uint32_t per_cta = n_children < 2 * NODE_THREADS ? (uint32_t)n_children : 2 * NODE_THREADS;
+    uint32_t blocks = (uint32_t)(n_children / per_cta);
+    k_merkle_nodes<<<blocks, NODE_THREADS, 0, stream>>>(layers, log_size, child_log, levels, seeds);
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    child_log -= levels;
+  }
+  return cudaSuccess;
+}
+
+// ---------------------------------------------------------------------------
+// Proof of work: lowest nonce with ctz(Blake2s(prefix_digest || LE64 nonce)[0..16]) >= n_bits.
+// Thread k tests nonces k, k + stride, ... and stops once its next nonce is not
+// below the best found so far, so every nonce below the result is tested and
+// the result does not depend on scheduling (src/core/channel/blake2s.zig:168-240).
+// ---------------------------------------------------------------------------
+namespace {
+
+__device__ __forceinline__ uint32_t ctz128(uint32_t a, uint32_t b, uint32_t c, uint32_t d) {
+  if (a) return __ffs(a) - 1;
+  if (b) return 32 + __ffs(b) - 1;
+  if (c) return 64 + __ffs(c) - 1;
+  if (d) return 96 + __ffs(d) - 1;
+  return 128;
+}
+
+struct PowPrefix { uint32_t w[8]; };
+
+__global__ void __launch_bounds__(256) k_pow(PowPrefix pre, uint32_t n_bits, uint64_t max_nonce,
+                                             unsigned long long* found, uint32_t* status) {
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  uint64_t nonce = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  uint32_t iter = 0;
+  unsigned long long best = *((volatile unsigned long long*)found);
+  while (nonce < max_nonce && nonce < best) {
+    uint32_t h[8];
+    b2s_init(h);
+    uint32_t m[16];
+#pragma unroll
+    for (int i = 0; i < 8; ++i) m[i] = pre.w[i];
+    m[8] = (uint32_t)nonce; m[9] = (uint32_t)(nonce >> 32);
+#pragma unroll
+    for (int i = 10; i < 16; ++i) m[i] = 0;
+    b2s_compress(h, m, 40, true);
+    if (ctz128(h[0], h[1], h[2], h[3]) >= n_bits) {
+      atomicMin(found, (unsigned long long)nonce);
+      return;
+    }
+    nonce += stride;
+    if ((++iter & 15) == 0) best = *((volatile unsigned long long*)found);
+  }
+  if (nonce >= max_nonce && threadIdx.x == 0 && blockIdx.x == 0) {
+    // Reached the search bound: the host reports a timeout unless a nonce was found.
+    atomicExch(status, 1u);
+  }
+}
+
+}  // namespace
+
+cudaError_t pow_grind(const uint32_t prefix_words[8], uint32_t n_bits, uint64_t max_nonce, uint32_t* result_dev,
+                      cudaStream_t stream) {
+  PowPrefix pre;
+  for (int i = 0; i < 8; ++i) pre.w[i] = prefix_words[i];
+  // result: [0..1] found nonce (init ~0), [2] status
+  cudaError_t e = cudaMemsetAsync(result_dev, 0xff, 8, stream);
+  if (e != cudaSuccess) return e;
+  e = cudaMemsetAsync(result_dev + 2, 0, 4, stream);
+  if (e != cudaSuccess) return e;
+  int dev = 0, sms = 148;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  k_pow<<<sms * 8, 256, 0, stream>>>(pre, n_bits, max_nonce, reinterpret_cast<unsigned long long*>(result_dev),
+                                     result_dev + 2);
+  return cudaGetLastError();
+}
+
+}  // namespace sb

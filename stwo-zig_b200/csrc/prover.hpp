@@ -1,0 +1,93 @@
+// Host orchestration of one wide-Fibonacci proof on one device stream.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "kernels.cuh"
+
+namespace sb {
+
+struct PcsConfig {
+  uint32_t pow_bits = 10;
+  uint32_t log_blowup_factor = 1;
+  uint32_t log_last_layer_degree_bound = 0;
+  uint32_t n_queries = 3;
+};
+
+struct ProveRequest {
+  uint32_t log_n_rows = 0, sequence_len = 0;
+  PcsConfig config;
+  const uint32_t* trace_host = nullptr;    // column-major, bit-reversed circle order
+  const uint32_t* trace_device = nullptr;  // same layout, device memory
+  int trace_kind = 0;                      // when neither pointer is given: 0 (1,row), 1 seeded
+  uint64_t trace_seed = 0;
+  bool has_channel_seed = false;
+  uint64_t channel_seed = 0;
+};
+
+// Stage timings of one proof (milliseconds of device time between events).
+struct StageTimes {
+  float upload = 0, trace = 0, main_commit = 0, composition = 0, composition_commit = 0, oods = 0,
+        quotients = 0, fri = 0, pow = 0, decommit = 0, total = 0;
+};
+
+// Status codes shared with the C ABI.
+enum : int32_t {
+  OK = 0,
+  E_INVALID = -1,
+  E_OOM = -2,
+  E_CUDA = -3,
+  E_TIMEOUT = -4,
+  E_CONSTRAINTS = -5,
+  E_BUFFER_TOO_SMALL = -6,
+  E_FALLBACK = -7,
+  E_NO_DEVICE = -8,
+};
+
+struct Context;
+
+// Per-proof device workspace, reused across proofs of the same shape.
+class WideFibProver {
+ public:
+  WideFibProver(Context* ctx, cudaStream_t stream);
+  ~WideFibProver();
+  int32_t prove(const ProveRequest& req, std::string& proof_json, StageTimes* times);
+  const std::string& error() const { return err_; }
+
+ private:
+  int32_t ensure_workspace(uint32_t log_n, uint32_t W, uint32_t B);
+  void release();
+  int32_t fail(int32_t code, const std::string& msg) { err_ = msg; return code; }
+
+  Context* ctx_;
+  cudaStream_t stream_;
+  std::string err_;
+  // workspace
+  uint8_t* arena_ = nullptr;
+  size_t arena_size_ = 0;
+  uint32_t ws_log_n_ = 0, ws_W_ = 0, ws_B_ = 0;
+  uint8_t* pinned_ = nullptr;
+  size_t pinned_size_ = 0;
+  cudaEvent_t ev_[12];
+};
+
+struct Context {
+  int device = 0;
+  int sm_count = 0;
+  DeviceTables tables;
+  std::mutex mu;
+  std::vector<WideFibProver*> pool;  // idle provers
+  cudaStream_t stream = nullptr;
+  ~Context();
+  int32_t init(int device, uint32_t tower_log);
+  WideFibProver* acquire();
+  void release(WideFibProver* p);
+};
+
+const char* status_string(int32_t code);
+
+}  // namespace sb

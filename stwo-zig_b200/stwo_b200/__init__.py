@@ -1,0 +1,305 @@
+"""Python host binding of libstwo_b200 (the B200 circle-STARK backend).
+
+The API mirrors the reference's wide-Fibonacci proving entry points
+(src/examples/wide_fibonacci.zig: prove / provePreparedWithEngine, Statement,
+PcsConfig) and the backend-contract operations (src/backend/*.zig). Every call
+goes through the C ABI declared in include/stwo_b200.h; there is no CPU
+fallback: importing this module without the built library raises.
+
+Device buffers are torch tensors (int32 storage of canonical M31 words, the
+values are < 2^31); torch is used for device memory and streams only.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from dataclasses import dataclass, field
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(os.path.dirname(_HERE), "lib", "libstwo_b200.so")
+
+if not os.path.exists(LIB_PATH):
+    raise ImportError(f"libstwo_b200.so is not built ({LIB_PATH}); run `make -C stwo-zig_b200`")
+
+_lib = ctypes.CDLL(LIB_PATH)
+
+OK = 0
+E_INVALID = -1
+E_OOM = -2
+E_CUDA = -3
+E_TIMEOUT = -4
+E_CONSTRAINTS = -5
+E_BUFFER_TOO_SMALL = -6
+E_FALLBACK = -7
+E_NO_DEVICE = -8
+
+_u32 = ctypes.c_uint32
+_u64 = ctypes.c_uint64
+_i32 = ctypes.c_int32
+_vp = ctypes.c_void_p
+
+
+class QM31C(ctypes.Structure):
+    _fields_ = [("a", _u32), ("b", _u32), ("c", _u32), ("d", _u32)]
+
+
+class PcsConfigC(ctypes.Structure):
+    _fields_ = [("pow_bits", _u32), ("log_blowup_factor", _u32), ("log_last_layer_degree_bound", _u32),
+                ("n_queries", _u32)]
+
+
+class RequestC(ctypes.Structure):
+    _fields_ = [("log_n_rows", _u32), ("sequence_len", _u32), ("config", PcsConfigC), ("trace_host", _vp),
+                ("trace_device", _vp), ("trace_kind", _u32), ("has_channel_seed", _u32), ("trace_seed", _u64),
+                ("channel_seed", _u64)]
+
+
+class StageTimesC(ctypes.Structure):
+    _fields_ = [(n, ctypes.c_float) for n in ("upload", "trace", "main_commit", "composition", "composition_commit",
+                                              "oods", "quotients", "fri", "pow", "decommit", "total")]
+
+
+_SIGS = {
+    "stwo_b200_context_create": [_i32, ctypes.POINTER(_vp)],
+    "stwo_b200_context_destroy": [_vp],
+    "stwo_b200_prove_wide_fibonacci": [_vp, ctypes.POINTER(RequestC), _vp, ctypes.c_size_t,
+                                       ctypes.POINTER(ctypes.c_size_t), ctypes.POINTER(StageTimesC)],
+    "stwo_b200_prove_wide_fibonacci_batch": [_vp, ctypes.POINTER(RequestC), ctypes.c_size_t,
+                                             ctypes.POINTER(_vp), ctypes.POINTER(ctypes.c_size_t),
+                                             ctypes.POINTER(ctypes.c_size_t), ctypes.POINTER(_i32), _u32],
+    "stwo_b200_interpolate_columns": [_vp, _u32, _u32, _vp, _u64, _vp],
+    "stwo_b200_evaluate_columns": [_vp, _u32, _u32, _vp, _u64, _vp],
+    "stwo_b200_interpolate_and_extend": [_vp, _u32, _u32, _u32, _vp, _u64, _vp, _u64, _vp, _u64, _vp],
+    "stwo_b200_extend_columns": [_vp, _u32, _u32, _u32, _vp, _u64, _vp, _u64, _vp],
+    "stwo_b200_eval_at_point": [_vp, _u32, _u32, _vp, _u64, QM31C, QM31C, _vp, _vp],
+    "stwo_b200_merkle_commit": [_vp, _u32, _u32, _vp, _u64, _vp, _vp, _vp],
+    "stwo_b200_fold_circle_into_line": [_vp, _u32, _vp, _u64, QM31C, _vp, _u64, _i32, _vp],
+    "stwo_b200_fold_line": [_vp, _u32, _vp, _u64, QM31C, _vp, _u64, _vp],
+    "stwo_b200_accumulate_quotients": [_vp, _u32, _u32, _vp, _vp, QM31C, QM31C, QM31C, QM31C, _vp, _u64, _vp],
+    "stwo_b200_wide_fib_trace": [_vp, _u32, _u32, _u32, _u64, _vp, _u64, _vp],
+    "stwo_b200_wide_fib_composition": [_vp, _u32, _u32, _vp, _u64, _vp, _u32, _u32, _vp, _u64, _vp],
+    "stwo_b200_pow_grind": [_vp, ctypes.c_char_p, _u32, ctypes.POINTER(_u64)],
+}
+for _name, _args in _SIGS.items():
+    _fn = getattr(_lib, _name)
+    _fn.argtypes = _args
+    _fn.restype = _i32
+_lib.stwo_b200_last_error.restype = ctypes.c_char_p
+_lib.stwo_b200_status_string.restype = ctypes.c_char_p
+_lib.stwo_b200_status_string.argtypes = [_i32]
+_lib.stwo_b200_version.restype = ctypes.c_char_p
+
+EXPORTED_SYMBOLS = sorted(list(_SIGS) + ["stwo_b200_last_error", "stwo_b200_status_string", "stwo_b200_version"])
+
+
+class StwoError(RuntimeError):
+    def __init__(self, status: int, message: str):
+        super().__init__(f"{_lib.stwo_b200_status_string(status).decode()} ({status}): {message}")
+        self.status = status
+
+
+def _check(status: int) -> None:
+    if status != OK:
+        raise StwoError(status, (_lib.stwo_b200_last_error() or b"").decode())
+
+
+def lib():
+    return _lib
+
+
+# ---------------------------------------------------------------------------
+# Protocol types (src/core/pcs/mod.zig:23-52, src/core/fri/config.zig,
+# src/examples/wide_fibonacci/trace.zig:18-21, presets src/prover/native/config.zig:140-160)
+# ---------------------------------------------------------------------------
+@dataclass
+class FriConfig:
+    log_blowup_factor: int = 1
+    log_last_layer_degree_bound: int = 0
+    n_queries: int = 3
+
+
+@dataclass
+class PcsConfig:
+    pow_bits: int = 10
+    fri_config: FriConfig = field(default_factory=FriConfig)
+
+    @staticmethod
+    def preset(name: str) -> "PcsConfig":
+        if name == "smoke":
+            return PcsConfig(0, FriConfig(1, 0, 3))
+        if name == "functional":
+            return PcsConfig(10, FriConfig(1, 0, 3))
+        if name == "secure":
+            return PcsConfig(26, FriConfig(1, 0, 70))
+        raise ValueError(name)
+
+    def _c(self) -> PcsConfigC:
+        f = self.fri_config
+        return PcsConfigC(self.pow_bits, f.log_blowup_factor, f.log_last_layer_degree_bound, f.n_queries)
+
+
+@dataclass
+class Statement:
+    log_n_rows: int
+    sequence_len: int
+
+
+TRACE_REFERENCE = 0   # (1, row) seeds of the reference's trace generator
+TRACE_SEEDED = 1      # seeded uniform col0/col1 in [0, p-1)
+
+
+def _qm(v) -> QM31C:
+    return QM31C(*[int(x) for x in v])
+
+
+def _ptr(t) -> int:
+    if t is None:
+        return 0
+    if hasattr(t, "data_ptr"):
+        return t.data_ptr()
+    return t.ctypes.data  # numpy
+
+
+def _stream(stream) -> int:
+    if stream is None:
+        import torch
+        return torch.cuda.current_stream().cuda_stream
+    return stream if isinstance(stream, int) else stream.cuda_stream
+
+
+class Context:
+    """One device context (point tables, twiddle towers, per-proof workspaces)."""
+
+    def __init__(self, device: int = 0):
+        h = _vp()
+        _check(_lib.stwo_b200_context_create(device, ctypes.byref(h)))
+        self._h = h
+        self.device = device
+
+    def close(self) -> None:
+        if self._h:
+            _lib.stwo_b200_context_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # ---- engine level ------------------------------------------------------
+    def _request(self, statement: Statement, config: PcsConfig, trace=None, trace_kind=TRACE_REFERENCE,
+                 trace_seed=0, channel_seed=None) -> tuple[RequestC, object]:
+        req = RequestC()
+        req.log_n_rows = statement.log_n_rows
+        req.sequence_len = statement.sequence_len
+        req.config = config._c()
+        keep = None
+        if trace is not None:
+            if hasattr(trace, "is_cuda") and trace.is_cuda:
+                assert trace.is_contiguous()
+                req.trace_device = trace.data_ptr()
+            else:
+                import numpy as np
+                keep = np.ascontiguousarray(trace, dtype=np.uint32)
+                req.trace_host = keep.ctypes.data
+            keep = (keep, trace)
+        req.trace_kind = trace_kind
+        req.trace_seed = trace_seed
+        req.has_channel_seed = int(channel_seed is not None)
+        req.channel_seed = channel_seed or 0
+        return req, keep
+
+    def prove_wide_fibonacci(self, statement: Statement, config: PcsConfig, trace=None,
+                             trace_kind: int = TRACE_REFERENCE, trace_seed: int = 0, channel_seed: int | None = None,
+                             with_times: bool = False):
+        """Proves the wide-Fibonacci AIR; returns the JSON wire proof bytes (and stage times)."""
+        req, keep = self._request(statement, config, trace, trace_kind, trace_seed, channel_seed)
+        cap = 1 << 24
+        buf = ctypes.create_string_buffer(cap)
+        n = ctypes.c_size_t(0)
+        times = StageTimesC()
+        _check(_lib.stwo_b200_prove_wide_fibonacci(self._h, ctypes.byref(req), buf, cap, ctypes.byref(n),
+                                                   ctypes.byref(times)))
+        del keep
+        proof = buf.raw[: n.value]
+        if with_times:
+            return proof, {name: getattr(times, name) for name, _ in StageTimesC._fields_}
+        return proof
+
+    def prove_wide_fibonacci_batch(self, requests: list[dict], max_in_flight: int = 4) -> list[bytes]:
+        """requests: dicts with statement, config and optional trace / trace_kind / trace_seed / channel_seed."""
+        n = len(requests)
+        arr = (RequestC * n)()
+        keeps = []
+        for i, r in enumerate(requests):
+            req, keep = self._request(r["statement"], r["config"], r.get("trace"), r.get("trace_kind", TRACE_REFERENCE),
+                                      r.get("trace_seed", 0), r.get("channel_seed"))
+            arr[i] = req
+            keeps.append(keep)
+        cap = 1 << 24
+        bufs = [ctypes.create_string_buffer(cap) for _ in range(n)]
+        outs = (_vp * n)(*[ctypes.cast(b, _vp) for b in bufs])
+        caps = (ctypes.c_size_t * n)(*([cap] * n))
+        lens = (ctypes.c_size_t * n)()
+        statuses = (_i32 * n)()
+        _check(_lib.stwo_b200_prove_wide_fibonacci_batch(self._h, arr, n, outs, caps, lens, statuses, max_in_flight))
+        del keeps
+        return [bufs[i].raw[: lens[i]] for i in range(n)]
+
+    # ---- backend-contract operations (device tensors) ------------------------
+    def interpolate(self, cols, log_size: int, n_cols: int, stride: int, stream=None) -> None:
+        _check(_lib.stwo_b200_interpolate_columns(self._h, log_size, n_cols, _ptr(cols), stride, _stream(stream)))
+
+    def evaluate(self, cols, log_size: int, n_cols: int, stride: int, stream=None) -> None:
+        _check(_lib.stwo_b200_evaluate_columns(self._h, log_size, n_cols, _ptr(cols), stride, _stream(stream)))
+
+    def interpolate_and_extend(self, evals, coeffs, lde, log_size: int, log_blowup: int, n_cols: int,
+                               stream=None) -> None:
+        _check(_lib.stwo_b200_interpolate_and_extend(self._h, log_size, log_blowup, n_cols, _ptr(evals), 1 << log_size,
+                                                     _ptr(coeffs), 1 << log_size, _ptr(lde),
+                                                     1 << (log_size + log_blowup), _stream(stream)))
+
+    def extend(self, coeffs, lde, log_size: int, log_blowup: int, n_cols: int, stream=None) -> None:
+        _check(_lib.stwo_b200_extend_columns(self._h, log_size, log_blowup, n_cols, _ptr(coeffs), 1 << log_size,
+                                             _ptr(lde), 1 << (log_size + log_blowup), _stream(stream)))
+
+    def merkle_commit(self, cols, log_size: int, n_cols: int, layers, stream=None) -> bytes:
+        root = ctypes.create_string_buffer(32)
+        _check(_lib.stwo_b200_merkle_commit(self._h, log_size, n_cols, _ptr(cols), 1 << log_size, _ptr(layers), root,
+                                            _stream(stream)))
+        return root.raw
+
+    def fold_circle_into_line(self, src, dst, src_log: int, alpha, accumulate: bool = False, stream=None) -> None:
+        _check(_lib.stwo_b200_fold_circle_into_line(self._h, src_log, _ptr(src), 1 << src_log, _qm(alpha), _ptr(dst),
+                                                    1 << (src_log - 1), int(accumulate), _stream(stream)))
+
+    def fold_line(self, src, dst, src_log: int, alpha, stream=None) -> None:
+        _check(_lib.stwo_b200_fold_line(self._h, src_log, _ptr(src), 1 << src_log, _qm(alpha), _ptr(dst),
+                                        1 << (src_log - 1), _stream(stream)))
+
+    def eval_at_point(self, coeffs, log_size: int, n_cols: int, stride: int, px, py, out, stream=None) -> None:
+        _check(_lib.stwo_b200_eval_at_point(self._h, log_size, n_cols, _ptr(coeffs), stride, _qm(px), _qm(py),
+                                            _ptr(out), _stream(stream)))
+
+    def accumulate_quotients(self, log_size: int, col_ptrs, c, px, py, sum_a, sum_b, out, n_cols: int,
+                             stream=None) -> None:
+        _check(_lib.stwo_b200_accumulate_quotients(self._h, log_size, n_cols, _ptr(col_ptrs), _ptr(c), _qm(px),
+                                                   _qm(py), _qm(sum_a), _qm(sum_b), _ptr(out), 1 << log_size,
+                                                   _stream(stream)))
+
+    def wide_fib_trace(self, out, log_n_rows: int, sequence_len: int, trace_kind: int = TRACE_REFERENCE,
+                       seed: int = 0, stream=None) -> None:
+        _check(_lib.stwo_b200_wide_fib_trace(self._h, log_n_rows, sequence_len, trace_kind, seed, _ptr(out),
+                                             1 << log_n_rows, _stream(stream)))
+
+    def wide_fib_composition(self, eval_cols, log_n_rows: int, sequence_len: int, coeffs, den0: int, den1: int,
+                             out, stream=None) -> None:
+        _check(_lib.stwo_b200_wide_fib_composition(self._h, log_n_rows, sequence_len, _ptr(eval_cols),
+                                                   2 << log_n_rows, _ptr(coeffs), den0, den1, _ptr(out),
+                                                   2 << log_n_rows, _stream(stream)))
+
+    def pow_grind(self, prefix_digest: bytes, n_bits: int) -> int:
+        nonce = _u64(0)
+        _check(_lib.stwo_b200_pow_grind(self._h, prefix_digest, n_bits, ctypes.byref(nonce)))
+        return nonce.value

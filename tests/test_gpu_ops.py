@@ -1,0 +1,141 @@
+"""Op-level parity of the CUDA kernels (through the C ABI) against the CPU oracle."""
+import struct
+
+import numpy as np
+import pytest
+
+import oracle
+
+pytestmark = pytest.mark.gpu
+P = 2**31 - 1
+
+
+def dev(a):
+    import torch
+    return torch.from_numpy(np.ascontiguousarray(a, dtype=np.uint32).view(np.int32)).cuda()
+
+
+def host(t):
+    import torch
+    torch.cuda.synchronize()
+    return t.cpu().numpy().view(np.uint32)
+
+
+def rand_cols(rng, n_cols, log):
+    return rng.integers(0, P, size=(n_cols, 1 << log), dtype=np.uint32)
+
+
+@pytest.mark.parametrize("log", [1, 2, 3, 4, 7, 11, 12, 13, 16, 20])
+def test_interpolate_evaluate(ctx, log):
+    rng = np.random.default_rng(log)
+    n_cols = 3
+    cols = rand_cols(rng, n_cols, log)
+    d = dev(cols)
+    ctx.interpolate(d, log, n_cols, 1 << log)
+    got = host(d).reshape(n_cols, -1)
+    for c in range(n_cols):
+        assert np.array_equal(got[c], oracle.interpolate(cols[c])), c
+    ctx.evaluate(d, log, n_cols, 1 << log)
+    assert np.array_equal(host(d).reshape(n_cols, -1), cols)
+
+
+@pytest.mark.parametrize("log,blowup", [(1, 1), (3, 1), (10, 1), (11, 1), (12, 1), (15, 1), (20, 1), (12, 2), (5, 3)])
+def test_interpolate_and_extend(ctx, log, blowup):
+    import torch
+    rng = np.random.default_rng(100 + log)
+    n_cols = 4
+    cols = rand_cols(rng, n_cols, log)
+    ev = dev(cols)
+    coeffs = torch.empty_like(ev)
+    lde = torch.empty(n_cols << (log + blowup), dtype=torch.int32, device="cuda")
+    ctx.interpolate_and_extend(ev, coeffs, lde, log, blowup, n_cols)
+    co = host(coeffs).reshape(n_cols, -1)
+    le = host(lde).reshape(n_cols, -1)
+    for c in range(n_cols):
+        ref_c = oracle.interpolate(cols[c])
+        assert np.array_equal(co[c], ref_c), c
+        assert np.array_equal(le[c], oracle.extend(ref_c, blowup)), c
+    # the unmodified input
+    assert np.array_equal(host(ev).reshape(n_cols, -1), cols)
+
+
+@pytest.mark.parametrize("log,n_cols", [(0, 0), (1, 1), (4, 3), (8, 16), (9, 17), (12, 100), (17, 8)])
+def test_merkle(ctx, log, n_cols):
+    import torch
+    rng = np.random.default_rng(7 + log + n_cols)
+    cols = rand_cols(rng, max(n_cols, 1), log)[:n_cols]
+    d = dev(cols if n_cols else np.zeros(1, np.uint32))
+    layers = torch.empty(((2 << log) - 1) * 32, dtype=torch.uint8, device="cuda")
+    root = ctx.merkle_commit(d, log, n_cols, layers)
+    ref_layers = oracle.merkle_layers(list(cols))
+    assert root == ref_layers[-1][0].tobytes()
+    got = host(layers).view(np.uint8).reshape(-1, 32)
+    at = 0
+    for lay in ref_layers:
+        assert np.array_equal(got[at:at + lay.shape[0]], lay)
+        at += lay.shape[0]
+
+
+@pytest.mark.parametrize("log", [2, 3, 5, 12, 21])
+def test_fold_circle_into_line(ctx, log):
+    import torch
+    rng = np.random.default_rng(log)
+    src = rand_cols(rng, 4, log)
+    alpha = rng.integers(0, P, size=4, dtype=np.uint32)
+    prev = rand_cols(rng, 4, log - 1)
+    for acc in (False, True):
+        dst = dev(prev)
+        ctx.fold_circle_into_line(dev(src), dst, log, alpha, accumulate=acc)
+        ref = oracle.fold_circle_into_line(src, alpha, prev if acc else None)
+        assert np.array_equal(host(dst).reshape(4, -1), ref)
+
+
+@pytest.mark.parametrize("log", [1, 2, 4, 11, 20])
+def test_fold_line(ctx, log):
+    import torch
+    rng = np.random.default_rng(log + 50)
+    src = rand_cols(rng, 4, log)
+    alpha = rng.integers(0, P, size=4, dtype=np.uint32)
+    dst = torch.empty(4 << (log - 1), dtype=torch.int32, device="cuda")
+    ctx.fold_line(dev(src), dst, log, alpha)
+    assert np.array_equal(host(dst).reshape(4, -1), oracle.fold_line(src, alpha, log))
+
+
+@pytest.mark.parametrize("log", [0, 1, 3, 12, 13, 20])
+def test_eval_at_point(ctx, log):
+    import torch
+    rng = np.random.default_rng(log + 9)
+    n_cols = 5
+    cols = rand_cols(rng, n_cols, log)
+    px = rng.integers(0, P, size=4, dtype=np.uint32)
+    py = rng.integers(0, P, size=4, dtype=np.uint32)
+    out = torch.empty(4 * n_cols, dtype=torch.int32, device="cuda")
+    ctx.eval_at_point(dev(cols), log, n_cols, 1 << log, px, py, out)
+    got = host(out).reshape(n_cols, 4)
+    for c in range(n_cols):
+        assert np.array_equal(got[c], oracle.eval_at_point(cols[c], px, py)), c
+
+
+@pytest.mark.parametrize("kind", [0, 1])
+def test_trace_generation(ctx, kind):
+    import torch
+    out = torch.empty(12 << 9, dtype=torch.int32, device="cuda")
+    ctx.wide_fib_trace(out, 9, 12, kind, seed=1234)
+    assert np.array_equal(host(out).reshape(12, -1), oracle.gen_trace(9, 12, kind, 1234))
+
+
+@pytest.mark.parametrize("bits", [1, 8, 14])
+def test_pow_grind(ctx, bits):
+    digest = bytes((i * 37 + bits) & 0xFF for i in range(32))
+    prefix = oracle.blake2s(struct.pack("<I", 0x12345678) + b"\0" * 12 + digest + struct.pack("<I", bits))
+    assert ctx.pow_grind(prefix, bits) == oracle.pow_grind(digest, bits, 8)
+
+
+def test_bad_arguments_raise(ctx):
+    import stwo_b200
+    import torch
+    d = torch.zeros(16, dtype=torch.int32, device="cuda")
+    with pytest.raises(stwo_b200.StwoError):
+        ctx.interpolate(d, 40, 1, 16)
+    with pytest.raises(stwo_b200.StwoError):
+        ctx.fold_circle_into_line(d, d, 1, [1, 0, 0, 0])

@@ -1,0 +1,99 @@
+"""End-to-end proofs on the GPU, byte-for-byte against the oracle and the reference's stored proofs."""
+import hashlib
+import json
+import os
+
+import numpy as np
+import pytest
+
+import oracle
+
+pytestmark = pytest.mark.gpu
+GOLDEN = os.path.join(os.path.dirname(__file__), "golden")
+STORED = json.load(open(os.path.join(GOLDEN, "stored_proofs.json")))
+KATS = json.load(open(os.path.join(GOLDEN, "kats.json")))
+
+
+def cfg_pair(preset, **over):
+    import stwo_b200 as sb
+    c = oracle.config(preset, **over)
+    return c, sb.PcsConfig(c.pow_bits, sb.FriConfig(c.log_blowup_factor, c.log_last_layer_degree_bound, c.n_queries))
+
+
+def test_kat_5x8(ctx):
+    import stwo_b200 as sb
+    _, g = cfg_pair("smoke")
+    p = ctx.prove_wide_fibonacci(sb.Statement(5, 8), g)
+    assert len(p) == KATS["wf_5x8_proof"]["len"]
+    assert hashlib.sha256(p).hexdigest() == KATS["wf_5x8_proof"]["sha256"]
+
+
+@pytest.mark.parametrize("entry", STORED, ids=lambda e: f"{e['log_n_rows']}x{e['sequence_len']}")
+def test_stored_functional_proofs(ctx, entry):
+    import stwo_b200 as sb
+    g = sb.PcsConfig(entry["pow_bits"], sb.FriConfig(entry["log_blowup_factor"], entry["log_last_layer_degree_bound"],
+                                                     entry["n_queries"]))
+    p = ctx.prove_wide_fibonacci(sb.Statement(entry["log_n_rows"], entry["sequence_len"]), g)
+    assert len(p) == entry["len"]
+    assert hashlib.sha256(p).hexdigest() == entry["sha256"]
+
+
+@pytest.mark.parametrize("log_n,W,preset", [(1, 2, "smoke"), (2, 3, "smoke"), (3, 4, "functional"),
+                                            (6, 17, "functional"), (11, 16, "functional"), (12, 100, "secure"),
+                                            (13, 33, "functional")])
+def test_seeded_proofs_match_oracle(ctx, log_n, W, preset):
+    import stwo_b200 as sb
+    o, g = cfg_pair(preset)
+    ref = oracle.prove_wide_fib(log_n, W, o, trace_kind=1, trace_seed=99 + log_n)
+    got = ctx.prove_wide_fibonacci(sb.Statement(log_n, W), g, trace_kind=sb.TRACE_SEEDED, trace_seed=99 + log_n)
+    assert got == ref
+
+
+def test_host_and_device_traces(ctx):
+    import stwo_b200 as sb
+    import torch
+    o, g = cfg_pair("functional")
+    trace = oracle.gen_trace(10, 20, trace_kind=1, seed=5)
+    ref = oracle.prove_wide_fib(10, 20, o, trace=trace)
+    assert ctx.prove_wide_fibonacci(sb.Statement(10, 20), g, trace=trace) == ref
+    dtrace = torch.from_numpy(trace.view(np.int32)).cuda()
+    assert ctx.prove_wide_fibonacci(sb.Statement(10, 20), g, trace=dtrace) == ref
+
+
+def test_channel_seed_and_blowup(ctx):
+    import stwo_b200 as sb
+    o, g = cfg_pair("functional", log_blowup_factor=2, n_queries=5, log_last_layer_degree_bound=1)
+    ref = oracle.prove_wide_fib(9, 10, o, trace_kind=1, trace_seed=3, channel_seed=77)
+    got = ctx.prove_wide_fibonacci(sb.Statement(9, 10), g, trace_kind=1, trace_seed=3, channel_seed=77)
+    assert got == ref
+    assert got != ctx.prove_wide_fibonacci(sb.Statement(9, 10), g, trace_kind=1, trace_seed=3, channel_seed=78)
+
+
+def test_corrupted_trace_fails_closed(ctx):
+    import stwo_b200 as sb
+    _, g = cfg_pair("smoke")
+    t = oracle.gen_trace(6, 8, 0)
+    t[4, 11] ^= 3
+    with pytest.raises(sb.StwoError) as e:
+        ctx.prove_wide_fibonacci(sb.Statement(6, 8), g, trace=t)
+    assert e.value.status == sb.E_CONSTRAINTS
+
+
+def test_batch_matches_single(ctx):
+    import stwo_b200 as sb
+    _, g = cfg_pair("functional")
+    reqs = [dict(statement=sb.Statement(8 + (i % 4), 8 + 3 * i), config=g, trace_kind=1, trace_seed=i,
+                 channel_seed=1000 + i) for i in range(8)]
+    batch = ctx.prove_wide_fibonacci_batch(reqs, max_in_flight=4)
+    for r, p in zip(reqs, batch):
+        single = ctx.prove_wide_fibonacci(r["statement"], g, trace_kind=1, trace_seed=r["trace_seed"],
+                                          channel_seed=r["channel_seed"])
+        assert p == single
+
+
+def test_repeat_determinism(ctx):
+    import stwo_b200 as sb
+    _, g = cfg_pair("functional")
+    a = ctx.prove_wide_fibonacci(sb.Statement(14, 32), g, trace_kind=1, trace_seed=1)
+    b = ctx.prove_wide_fibonacci(sb.Statement(14, 32), g, trace_kind=1, trace_seed=1)
+    assert a == b

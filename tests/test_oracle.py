@@ -1,0 +1,104 @@
+"""Pins the CPU oracle to the reference's known answers and stored proofs (no GPU)."""
+import hashlib
+import json
+import os
+import struct
+
+import numpy as np
+import pytest
+
+import oracle
+
+GOLDEN = os.path.join(os.path.dirname(__file__), "golden")
+KATS = json.load(open(os.path.join(GOLDEN, "kats.json")))
+STORED = json.load(open(os.path.join(GOLDEN, "stored_proofs.json")))
+
+
+def test_blake2s_merkle_kats():
+    # src/core/vcs_lifted/blake2_merkle.zig:339-370
+    assert oracle.merkle_root([]).hex() == KATS["prefixed_empty_leaf"]
+    node = b"node" + b"\0" * 60
+    assert oracle.blake2s(node + b"\x01" * 32 + b"\x02" * 32).hex() == KATS["prefixed_parent_01_02"]
+    assert oracle.blake2s(struct.pack("<3I", 1, 2, 3)).hex() == KATS["plain_leaf_1_2_3"]
+    assert oracle.blake2s(b"\x01" * 32 + b"\x02" * 32).hex() == KATS["plain_parent_01_02"]
+    assert oracle.blake2s(b"abc") == hashlib.blake2s(b"abc").digest()
+    for n in (0, 1, 63, 64, 65, 128, 200):
+        data = bytes(range(256))[:n]
+        assert oracle.blake2s(data) == hashlib.blake2s(data).digest()
+
+
+def test_wide_fib_5x16_commitments():
+    # src/examples/wide_fibonacci/session_test.zig:75-96
+    proof = json.loads(oracle.prove_wide_fib(5, 16, oracle.config("smoke")))
+    assert [bytes(c).hex() for c in proof["commitments"]] == KATS["wf_5x16_commitments"]
+
+
+def test_wide_fib_5x8_proof_kat():
+    # src/examples/wide_fibonacci/session_test.zig:63-72
+    p = oracle.prove_wide_fib(5, 8, oracle.config("smoke"))
+    assert len(p) == KATS["wf_5x8_proof"]["len"]
+    assert hashlib.sha256(p).hexdigest() == KATS["wf_5x8_proof"]["sha256"]
+
+
+@pytest.mark.parametrize("entry", STORED, ids=lambda e: f"{e['log_n_rows']}x{e['sequence_len']}")
+def test_stored_functional_proofs(entry):
+    cfg = oracle.PcsConfig(entry["pow_bits"], entry["log_blowup_factor"], entry["log_last_layer_degree_bound"],
+                           entry["n_queries"])
+    p = oracle.prove_wide_fib(entry["log_n_rows"], entry["sequence_len"], cfg)
+    assert len(p) == entry["len"]
+    assert hashlib.sha256(p).hexdigest() == entry["sha256"]
+    if "proof_hex" in entry:
+        assert p == bytes.fromhex(entry["proof_hex"])
+
+
+def test_fft_roundtrip_and_linearity():
+    rng = np.random.default_rng(1)
+    for log in (1, 2, 3, 5, 10):
+        v = rng.integers(0, 2**31 - 1, size=1 << log, dtype=np.uint32)
+        c = oracle.interpolate(v)
+        assert np.array_equal(oracle.evaluate(c), v)
+        w = rng.integers(0, 2**31 - 1, size=1 << log, dtype=np.uint32)
+        s = ((v.astype(np.uint64) + w) % (2**31 - 1)).astype(np.uint32)
+        cs = ((oracle.interpolate(v).astype(np.uint64) + oracle.interpolate(w)) % (2**31 - 1)).astype(np.uint32)
+        assert np.array_equal(oracle.interpolate(s), cs)
+
+
+def test_extension_agrees_with_evaluation():
+    # The blown-up evaluation of a low-degree column restricted back interpolates to
+    # the same coefficients zero-padded.
+    rng = np.random.default_rng(2)
+    c = rng.integers(0, 2**31 - 1, size=1 << 6, dtype=np.uint32)
+    e = oracle.extend(c, 1)
+    back = oracle.interpolate(e)
+    assert np.array_equal(back[: c.size], c) and not back[c.size:].any()
+
+
+def test_pow_grind_is_lowest_valid_nonce():
+    digest = bytes(range(32))
+    nonce = oracle.pow_grind(digest, 8, 4)
+    prefix = oracle.blake2s(struct.pack("<I", 0x12345678) + b"\0" * 12 + digest + struct.pack("<I", 8))
+
+    def ok(n):
+        h = oracle.blake2s(prefix + struct.pack("<Q", n))
+        v = int.from_bytes(h[:16], "little")
+        return v & 0xFF == 0
+
+    assert ok(nonce)
+    assert not any(ok(n) for n in range(nonce))
+
+
+def test_seeded_trace_recurrence():
+    t = oracle.gen_trace(6, 10, trace_kind=1, seed=7).astype(np.uint64)
+    p = 2**31 - 1
+    assert (t[:2] < p - 1).all()
+    for k in range(2, 10):
+        assert np.array_equal(t[k], (t[k - 2] ** 2 + t[k - 1] ** 2) % p)
+    assert not np.array_equal(oracle.gen_trace(6, 10, 1, 7), oracle.gen_trace(6, 10, 1, 8))
+
+
+def test_corrupted_trace_is_rejected():
+    # src/examples/wide_fibonacci.zig:651-678: corrupting one cell fails the OODS self-check.
+    t = oracle.gen_trace(5, 8, 0)
+    t[3, 5] ^= 1
+    with pytest.raises(RuntimeError):
+        oracle.prove_wide_fib(5, 8, oracle.config("smoke"), trace=t)
