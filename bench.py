@@ -1,0 +1,351 @@
+"""Benchmark of the B200 wide-Fibonacci prover (one JSON line on rank 0).
+
+Workload: wide-Fibonacci AIR, 2^20 rows x 100 columns, `secure` preset (pow 26,
+70 queries, blowup 2, FRI to a constant), seeded uniform col0/col1 traces (a
+distinct seed per proof), every proof byte-identical to the CPU oracle's.
+A step is one proof. `value` is the batched throughput (proofs in flight on
+separate streams) with traces already resident in HBM; the single-proof path
+(one proof at a time) is reported beside it with its p50/p99 latency; `e2e`
+goes through the C ABI with pinned host traces (host-to-device copy of every
+trace and device-to-host of every proof inside the timed region).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+N > 1 runs under torchrun as independent replicas (proofs do not shard): each
+rank proves its own K proofs; value = N*K / max over ranks of the timed region.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "stwo-zig_b200"))
+
+METRIC = "proofs/s & p99 ms: batched vs single-proof on 1 B200, wide-Fib 2^20x100, exact"
+LOG_N, WIDTH = 20, 100
+IN_FLIGHT = 4
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--log-n", type=int, default=LOG_N)
+    ap.add_argument("--width", type=int, default=WIDTH)
+    ap.add_argument("--preset", default="secure")
+    ap.add_argument("--in-flight", type=int, default=IN_FLIGHT)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+def dist_env():
+    return int(os.environ.get("RANK", 0)), int(os.environ.get("WORLD_SIZE", 1)), int(os.environ.get("LOCAL_RANK", 0))
+
+
+def pct(xs, q):
+    xs = sorted(xs)
+    if not xs:
+        return None
+    k = (len(xs) - 1) * q / 100.0
+    lo, hi = int(k), min(int(k) + 1, len(xs) - 1)
+    return xs[lo] + (xs[hi] - xs[lo]) * (k - lo)
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+              "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.lines: list[str] = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except (OSError, FileNotFoundError):
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx = float(parts[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"], "samples": 0}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def cpu_oracle_prove(log_n, width, preset, seed, n_threads=0):
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
+    t = time.perf_counter()
+    proof = oracle.prove_wide_fib(log_n, width, oracle.config(preset), trace_kind=1, trace_seed=seed,
+                                  n_threads=n_threads)
+    return time.perf_counter() - t, proof
+
+
+def run_reference(args, rank, world):
+    """The reference CPU path on the host cores: the C++ restatement of the reference prover (the Zig
+    reference cannot be built here), all host threads, one proof per step."""
+    if rank != 0:
+        return
+    cores = os.cpu_count() or 1
+    for i in range(args.warmup):
+        cpu_oracle_prove(args.log_n, args.width, args.preset, 10_000 + i)
+    times = []
+    for i in range(args.steps):
+        dt, _ = cpu_oracle_prove(args.log_n, args.width, args.preset, 20_000 + i)
+        times.append(dt)
+    total = sum(times)
+    value = args.steps / total
+    out = {
+        "metric": METRIC, "value": value, "unit": "proofs/s", "impl": "reference", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * total / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u32",
+        "data": "synthetic: seeded uniform col0/col1 wide-Fibonacci traces",
+        "config": config_block(args),
+        "p50_ms": 1e3 * pct(times, 50), "p99_ms": 1e3 * pct(times, 99),
+        "cpu_baseline": {"value": value, "unit": "proofs/s", "cores": cores, "kind": "port",
+                         "sample": f"{args.steps} full {args.preset} proofs of 2^{args.log_n}x{args.width}, "
+                                   "C++ restatement of the reference CPU prover, all host threads"},
+        "e2e": {"value": value, "unit": "proofs/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(out), flush=True)
+
+
+def config_block(args):
+    return {"workload": f"wide-Fibonacci 2^{args.log_n}x{args.width}, {args.preset} preset, one proof per step",
+            "log_n_rows": args.log_n, "sequence_len": args.width, "protocol": args.preset,
+            "in_flight": args.in_flight, "l2": "inputs larger than L2 (400 MB trace per proof)",
+            "parallelism": "replicas"}
+
+
+def main():
+    args = parse()
+    rank, world, local = dist_env()
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        import torch
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600), device_id=torch.device("cuda", local))
+    if args.impl == "reference":
+        run_reference(args, rank, world)
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+        return
+
+    import torch
+    import stwo_b200 as sb
+
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    ctx = sb.Context(local)
+    cfg = sb.PcsConfig.preset(args.preset)
+    st = sb.Statement(args.log_n, args.width)
+    n_words = args.width << args.log_n
+    K, W = args.steps, args.warmup
+
+    def barrier():
+        if world > 1:
+            import torch.distributed as dist
+            dist.barrier()
+
+    def max_over_ranks(x: float) -> float:
+        if world == 1:
+            return x
+        import torch.distributed as dist
+        t = torch.tensor([x], device=dev, dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    # Device-resident traces, a distinct seed per proof (generated untimed by the library's kernel).
+    seeds = [1_000_003 * (rank + 1) + i for i in range(K + W)]
+    traces = []
+    for s in seeds:
+        t = torch.empty(n_words, dtype=torch.int32, device=dev)
+        ctx.wide_fib_trace(t, args.log_n, args.width, sb.TRACE_SEEDED, s)
+        traces.append(t)
+    torch.cuda.synchronize()
+
+    def requests(idx, host=None):
+        out = []
+        for i in idx:
+            tr = host[i % len(host)] if host is not None else traces[i]
+            out.append(dict(statement=st, config=cfg, trace=tr))
+        return out
+
+    # ---- warmup (both paths)
+    ctx.prove_wide_fibonacci_batch(requests(range(K, K + W)), max_in_flight=args.in_flight)
+    for i in range(K, K + W):
+        ctx.prove_wide_fibonacci(st, cfg, trace=traces[i])
+    torch.cuda.synchronize()
+
+    stream = torch.cuda.current_stream()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+
+    # ---- batched path: the headline value
+    launches0 = sb.kernel_launches()
+    with ClockSampler(local) as clocks:
+        barrier()
+        torch.cuda.synchronize()
+        ev0.record(stream)
+        proofs_b, times_b = ctx.prove_wide_fibonacci_batch(requests(range(K)), max_in_flight=args.in_flight,
+                                                           with_times=True)
+        ev1.record(stream)
+        torch.cuda.synchronize()
+        barrier()
+    batched_ms = max_over_ranks(ev0.elapsed_time(ev1))
+    launches = sb.kernel_launches() - launches0
+    value = world * K / (batched_ms / 1e3)
+
+    # ---- single-proof path
+    lat = []
+    barrier()
+    torch.cuda.synchronize()
+    e_start, e_end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e_start.record(stream)
+    for i in range(K):
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        p = ctx.prove_wide_fibonacci(st, cfg, trace=traces[i])
+        b.record(stream)
+        b.synchronize()
+        lat.append(a.elapsed_time(b))
+        assert p == proofs_b[i], "single and batched proofs differ"
+    e_end.record(stream)
+    torch.cuda.synchronize()
+    barrier()
+    single_ms = max_over_ranks(e_start.elapsed_time(e_end))
+
+    # ---- end to end through the C ABI: pinned host traces, proofs back to the host
+    host_traces = []
+    for i in range(min(K, 3)):
+        h = torch.empty(n_words, dtype=torch.int32, pin_memory=True)
+        h.copy_(traces[i])
+        host_traces.append(h.numpy().view("uint32"))  # same pinned pages, the ABI's uint32 type
+    torch.cuda.synchronize()
+    barrier()
+    ev0.record(stream)
+    proofs_e = ctx.prove_wide_fibonacci_batch(requests(range(K), host=host_traces), max_in_flight=args.in_flight)
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    barrier()
+    e2e_ms = max_over_ranks(ev0.elapsed_time(ev1))
+    for i in range(len(host_traces)):
+        assert proofs_e[i] == proofs_b[i], "host-trace and device-trace proofs differ"
+    proof_bytes = statistics.mean(len(p) for p in proofs_e)
+
+    # ---- roofline of the FFT pass (interpolate + blow-up extend of all trace columns)
+    coeffs = torch.empty(n_words, dtype=torch.int32, device=dev)
+    lde = torch.empty(2 * n_words, dtype=torch.int32, device=dev)
+    for _ in range(2):
+        ctx.interpolate_and_extend(traces[0], coeffs, lde, args.log_n, 1, args.width)
+    reps = 5
+    ev0.record(stream)
+    for _ in range(reps):
+        ctx.interpolate_and_extend(traces[0], coeffs, lde, args.log_n, 1, args.width)
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    fft_ms = ev0.elapsed_time(ev1) / reps
+    fft_bytes = 16 * n_words  # read evals, write coefficients, write 2x blown-up evaluations
+    peaks = {}
+    try:
+        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except (OSError, ValueError):
+        pass
+    hbm_peak = peaks.get("hbm_gbs", 6650.0)
+    fft_gbs = fft_bytes / (fft_ms / 1e3) / 1e9
+
+    # ---- INT32 rate of the proof-of-work grind (Blake2s, one compression per nonce)
+    digest = bytes(range(32))
+    pow_bits = 24
+    ctx.pow_grind(digest, pow_bits)
+    ev0.record(stream)
+    nonce = ctx.pow_grind(digest, pow_bits)
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    pow_ms = ev0.elapsed_time(ev1)
+    hashes_per_s = (nonce + 1) / (pow_ms / 1e3)
+
+    out = {
+        "metric": METRIC, "value": value, "unit": "proofs/s", "n_gpus": world, "steps": K, "warmup": W,
+        "ms_per_step": batched_ms / K, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "u32", "data": "synthetic: seeded uniform col0/col1 wide-Fibonacci traces, a distinct seed per proof",
+        "config": config_block(args),
+        "batched": {"proofs_per_s": value, "in_flight": args.in_flight,
+                    "p50_ms": pct([t["total"] for t in times_b], 50), "p99_ms": pct([t["total"] for t in times_b], 99)},
+        "single": {"proofs_per_s": world * K / (single_ms / 1e3), "p50_ms": pct(lat, 50), "p99_ms": pct(lat, 99)},
+        "p99_ms": pct(lat, 99),
+        "stage_ms_p50": {k: pct([t[k] for t in times_b], 50) for k in times_b[0]},
+        "e2e": {"value": world * K / (e2e_ms / 1e3), "unit": "proofs/s", "h2d_bytes_per_step": 4 * n_words,
+                "d2h_bytes_per_step": int(proof_bytes)},
+        "roofline": {"bound": "hbm", "kernel": "circle FFT pass: interpolate + blow-up extend (k_fft_low<1>, "
+                     "k_fft_high, k_fft_low<0>)", "achieved": fft_gbs, "peak": hbm_peak, "unit": "GB/s",
+                     "frac": fft_gbs / hbm_peak, "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)",
+                     "traffic": FFT_TRAFFIC_BYTES.get((args.log_n, args.width)),
+                     "algorithmic_bytes": fft_bytes, "ms": fft_ms},
+        "roofline_int32": {"kernel": "k_pow (Blake2s, 1 compression per nonce)", "hashes_per_s": hashes_per_s,
+                           "nonces": nonce + 1, "ms": pow_ms},
+        "gpu_launches": launches,
+        "clocks": clocks.summary(),
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        dt, ref = cpu_oracle_prove(args.log_n, args.width, args.preset, seeds[0])
+        out["cpu_baseline"] = {"value": 1.0 / dt, "unit": "proofs/s", "cores": os.cpu_count() or 1, "kind": "port",
+                               "sample": f"one {args.preset} proof of 2^{args.log_n}x{args.width} (seed of step 0), "
+                                         "C++ restatement of the reference CPU prover, all host threads"}
+        out["cpu_baseline"]["proof_identical"] = ref == proofs_b[0]
+    if rank == 0:
+        print(json.dumps(out), flush=True)
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+# DRAM bytes per launch-chain of the FFT pass, from ncu (profiles/fft_pass_*.md); None until captured.
+FFT_TRAFFIC_BYTES: dict = {}
+
+if __name__ == "__main__":
+    main()

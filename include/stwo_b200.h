@@ -90,6 +90,13 @@ const char* stwo_b200_status_string(int32_t status);
 /* Library version string (build identity). */
 const char* stwo_b200_version(void);
 
+/* Process-wide counters (Metal's telemetrySnapshot / TelemetrySnapshot,
+ * src/backends/metal/telemetry.zig:49-336): kernels launched by this library. */
+typedef struct {
+  uint64_t kernel_launches;
+} stwo_b200_telemetry;
+int32_t stwo_b200_telemetry_snapshot(stwo_b200_telemetry* out);
+
 /* ---- Engine level ------------------------------------------------------------------------------ */
 
 /* One proof; writes the JSON wire bytes (src/interop/proof_wire.zig:19-77). Replaces
@@ -101,11 +108,13 @@ int32_t stwo_b200_prove_wide_fibonacci(stwo_b200_context* ctx, const stwo_b200_w
                                        stwo_b200_stage_times* times);
 
 /* Batched proving: n independent requests, up to `max_in_flight` proofs resident and
- * overlapping on the device (one stream and workspace each). statuses[i] and proof_lens[i]
- * are per request; the call returns STWO_B200_OK when every request succeeded. */
+ * overlapping on the device (one stream and workspace each). statuses[i], proof_lens[i] and
+ * times[i] (nullable array) are per request; the call returns STWO_B200_OK when every request
+ * succeeded. No reference counterpart: the reference proves one statement per call. */
 int32_t stwo_b200_prove_wide_fibonacci_batch(stwo_b200_context* ctx, const stwo_b200_wide_fib_request* reqs,
                                              size_t n, uint8_t* const* proof_outs, const size_t* proof_caps,
-                                             size_t* proof_lens, int32_t* statuses, uint32_t max_in_flight);
+                                             size_t* proof_lens, int32_t* statuses, uint32_t max_in_flight,
+                                             stwo_b200_stage_times* times);
 
 /* ---- PolyOps (src/backend/poly_ops.zig:12-24) --------------------------------------------------- */
 

@@ -13,10 +13,6 @@
 
 namespace sb {
 
-#if defined(__CUDACC__)
-#define SB_CONST __device__ __constant__
-#endif
-
 SB_HD uint32_t rotr32(uint32_t x, int n) {
 #if defined(__CUDA_ARCH__)
   return __funnelshift_r(x, x, n);
@@ -30,12 +26,26 @@ struct B2sIv {
                             v4 = 0x510E527Fu, v5 = 0x9B05688Cu, v6 = 0x1F83D9ABu, v7 = 0x5BE0CD19u;
 };
 
-#define SB_B2S_G(a, b, c, d, x, y)          \
-  do {                                      \
-    a = a + b + (x); d = rotr32(d ^ a, 16); \
-    c = c + d;       b = rotr32(b ^ c, 12); \
-    a = a + b + (y); d = rotr32(d ^ a, 8);  \
-    c = c + d;       b = rotr32(b ^ c, 7);  \
+// Additions can be issued on the FMA pipe as IMAD x*one+y with a runtime `one`
+// (the XOR/rotate half of G keeps the ALU pipe busy; splitting the adds off
+// balances the two pipes). On the host `one` is ignored.
+#if defined(__CUDA_ARCH__)
+__device__ __forceinline__ uint32_t fadd(uint32_t a, uint32_t b, uint32_t one) {
+  uint32_t r;
+  asm("mad.lo.u32 %0, %1, %2, %3;" : "=r"(r) : "r"(a), "r"(one), "r"(b));
+  return r;
+}
+#define SB_ADD(a, b) fadd((a), (b), one)
+#else
+#define SB_ADD(a, b) ((a) + (b))
+#endif
+
+#define SB_B2S_G(a, b, c, d, x, y)                         \
+  do {                                                     \
+    a = SB_ADD(SB_ADD(a, b), (x)); d = rotr32(d ^ a, 16);  \
+    c = SB_ADD(c, d);              b = rotr32(b ^ c, 12);  \
+    a = SB_ADD(SB_ADD(a, b), (y)); d = rotr32(d ^ a, 8);   \
+    c = SB_ADD(c, d);              b = rotr32(b ^ c, 7);   \
   } while (0)
 
 // One round with the message schedule written out (sigma of RFC 7693 section 2.7).
@@ -53,7 +63,7 @@ struct B2sIv {
 
 // h <- compress(h, m, t, last). All indices are compile-time constants so the
 // message and state stay in registers.
-SB_HD void b2s_compress(uint32_t h[8], const uint32_t m[16], uint32_t t_lo, bool last) {
+SB_HD void b2s_compress(uint32_t h[8], const uint32_t m[16], uint32_t t_lo, bool last, uint32_t one = 1) {
   uint32_t v0 = h[0], v1 = h[1], v2 = h[2], v3 = h[3], v4 = h[4], v5 = h[5], v6 = h[6], v7 = h[7];
   uint32_t v8 = B2sIv::v0, v9 = B2sIv::v1, v10 = B2sIv::v2, v11 = B2sIv::v3;
   uint32_t v12 = B2sIv::v4 ^ t_lo, v13 = B2sIv::v5, v14 = last ? ~B2sIv::v6 : B2sIv::v6, v15 = B2sIv::v7;

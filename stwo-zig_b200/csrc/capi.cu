@@ -12,6 +12,12 @@ struct stwo_b200_context {
   sb::Context ctx;
 };
 
+namespace sb {
+static std::atomic<uint64_t> g_launches(0);
+void note_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
+uint64_t launch_count() { return g_launches.load(std::memory_order_relaxed); }
+}  // namespace sb
+
 namespace {
 
 thread_local std::string g_last_error;
@@ -66,6 +72,12 @@ const char* stwo_b200_last_error(void) { return g_last_error.c_str(); }
 const char* stwo_b200_status_string(int32_t s) { return sb::status_string(s); }
 const char* stwo_b200_version(void) { return "stwo_b200 0.1 sm_100a"; }
 
+int32_t stwo_b200_telemetry_snapshot(stwo_b200_telemetry* out) {
+  if (!out) return set_error(STWO_B200_E_INVALID, "null telemetry output");
+  out->kernel_launches = sb::launch_count();
+  return STWO_B200_OK;
+}
+
 int32_t stwo_b200_context_create(int32_t device, stwo_b200_context** out) {
   if (!out) return set_error(STWO_B200_E_INVALID, "null output");
   *out = nullptr;
@@ -109,7 +121,8 @@ int32_t stwo_b200_prove_wide_fibonacci(stwo_b200_context* ctx, const stwo_b200_w
 
 int32_t stwo_b200_prove_wide_fibonacci_batch(stwo_b200_context* ctx, const stwo_b200_wide_fib_request* reqs,
                                              size_t n, uint8_t* const* proof_outs, const size_t* proof_caps,
-                                             size_t* proof_lens, int32_t* statuses, uint32_t max_in_flight) {
+                                             size_t* proof_lens, int32_t* statuses, uint32_t max_in_flight,
+                                             stwo_b200_stage_times* times) {
   CK_CTX(ctx);
   if (n == 0) return STWO_B200_OK;
   if (!reqs || !proof_outs || !proof_caps || !proof_lens || !statuses)
@@ -125,7 +138,9 @@ int32_t stwo_b200_prove_wide_fibonacci_batch(stwo_b200_context* ctx, const stwo_
       if (i >= n) break;
       if (!p) { statuses[i] = STWO_B200_E_CUDA; continue; }
       std::string proof;
-      int32_t rc = p->prove(to_request(reqs[i]), proof, nullptr);
+      sb::StageTimes t;
+      int32_t rc = p->prove(to_request(reqs[i]), proof, times ? &t : nullptr);
+      if (times && rc == STWO_B200_OK) std::memcpy(&times[i], &t, sizeof(t));
       if (rc == STWO_B200_OK) {
         proof_lens[i] = proof.size();
         if (proof_outs[i] && proof_caps[i] >= proof.size()) std::memcpy(proof_outs[i], proof.data(), proof.size());

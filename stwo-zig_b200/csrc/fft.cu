@@ -16,6 +16,7 @@
 // so coefficients and the blown-up evaluations come out of one pass.
 #include <algorithm>
 
+#include "fft16.cuh"
 #include "kernels.cuh"
 
 namespace sb {
@@ -226,6 +227,140 @@ __global__ void k_build_tower(PointTable pts, uint32_t R, uint32_t* tw, uint32_t
   }
 }
 
+
+// ---------------------------------------------------------------------------
+// Radix-16 register kernels (domains 2^16 .. 2^22).
+// ---------------------------------------------------------------------------
+using fft16::radix16;
+using fft16::radix16_dyn;
+using fft16::spread;
+using fft16::swz;
+
+constexpr uint32_t B12 = 12;  // low pass: blocks of 4096 words, 256 threads x 16
+
+template <uint32_t WA, uint32_t WB>
+__device__ __forceinline__ void exchange12(uint32_t* sm, uint32_t (&x)[16], uint32_t ia, uint32_t ib) {
+  const uint32_t a = swz(ia);
+#pragma unroll
+  for (int k = 0; k < 16; ++k) sm[a ^ swz((uint32_t)k << WA)] = x[k];
+  __syncthreads();
+  const uint32_t b = swz(ib);
+#pragma unroll
+  for (int k = 0; k < 16; ++k) x[k] = sm[b ^ swz((uint32_t)k << WB)];
+}
+
+// Layers 0..11 of blocks of 4096 words. Forward: windows [8,12) -> [4,8) -> [0,4);
+// inverse: the reverse, then the optional scale.
+template <bool INV>
+__global__ void __launch_bounds__(256) k_fft_low12(const uint32_t* __restrict__ src, uint64_t ss, uint32_t* dst,
+                                                   uint64_t ds, TwiddleView tv, uint32_t scale) {
+  __shared__ uint32_t sm[1 << B12];
+  const uint32_t th = threadIdx.x;
+  const uint64_t blk = (uint64_t)blockIdx.x << B12;
+  const uint32_t* s = src + blockIdx.y * ss + blk;
+  uint32_t* d = dst + blockIdx.y * ds + blk;
+  const uint32_t ib2 = th;                            // elements ib2 + 256 k
+  const uint32_t ib1 = ((th >> 4) << 8) | (th & 15);  // elements ib1 + 16 k
+  const uint32_t ib0 = th << 4;                       // elements ib0 + k
+  uint32_t x[16];
+  if (!INV) {
+#pragma unroll
+    for (int k = 0; k < 16; ++k) x[k] = __ldg(s + ib2 + 256 * k);
+    radix16<false, 0, 4>(x, tv, 0, 8, blk + ib2);
+    exchange12<8, 4>(sm, x, ib2, ib1);
+    radix16<false, 0, 4>(x, tv, 0, 4, blk + ib1);
+    __syncthreads();
+    exchange12<4, 0>(sm, x, ib1, ib0);
+    radix16<false, 0, 4>(x, tv, 0, 0, blk + ib0);
+    uint4* o = reinterpret_cast<uint4*>(d + ib0);
+#pragma unroll
+    for (int q = 0; q < 4; ++q) o[q] = make_uint4(x[4 * q], x[4 * q + 1], x[4 * q + 2], x[4 * q + 3]);
+  } else {
+    const uint4* in = reinterpret_cast<const uint4*>(s + ib0);
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      uint4 v = __ldg(in + q);
+      x[4 * q] = v.x; x[4 * q + 1] = v.y; x[4 * q + 2] = v.z; x[4 * q + 3] = v.w;
+    }
+    radix16<true, 0, 4>(x, tv, 0, 0, blk + ib0);
+    exchange12<0, 4>(sm, x, ib0, ib1);
+    radix16<true, 0, 4>(x, tv, 0, 4, blk + ib1);
+    __syncthreads();
+    exchange12<4, 8>(sm, x, ib1, ib2);
+    radix16<true, 0, 4>(x, tv, 0, 8, blk + ib2);
+#pragma unroll
+    for (int k = 0; k < 16; ++k) d[ib2 + 256 * k] = scale ? mmul(x[k], scale) : x[k];
+  }
+}
+
+struct High16Params {
+  const uint32_t* src; uint64_t ss; uint32_t rows_in;  // 2^rows_in rows of 16 words per tile are loaded
+  int do_inverse; TwiddleView itv; uint32_t scale; uint32_t* coef; uint64_t cs;
+  int do_forward; TwiddleView ftv; uint32_t rows_out; uint32_t fwd_layers; int dup;
+  uint32_t* out; uint64_t os;
+};
+
+// One window stage over the tile: threads [0, 2^rows * ... ) own 16 rows each.
+template <bool INV>
+__device__ __forceinline__ void high_stage(uint32_t* sm, const TwiddleView& tv, uint32_t rows, uint32_t w0,
+                                           uint32_t nl) {
+  const uint32_t th = threadIdx.x;
+  if (th < (1u << rows)) {
+    const uint32_t t = th & 15, q = th >> 4;
+    const uint32_t mb = spread(q, w0);
+    const uint32_t a = swz((mb << 4) | t);
+    uint32_t x[16];
+#pragma unroll
+    for (int k = 0; k < 16; ++k) x[k] = sm[a ^ swz((uint32_t)k << (w0 + 4))];
+    radix16_dyn<INV>(x, tv, B12, w0, mb, nl);
+#pragma unroll
+    for (int k = 0; k < 16; ++k) sm[a ^ swz((uint32_t)k << (w0 + 4))] = x[k];
+  }
+  __syncthreads();
+}
+
+// Grid (256 tiles of 16 adjacent low indices, n_cols); blockDim = 2^rows_max threads.
+__global__ void __launch_bounds__(1024) k_fft_high16(High16Params p) {
+  extern __shared__ uint32_t sm[];
+  const uint32_t g = blockIdx.x, col = blockIdx.y, th = threadIdx.x, nt = blockDim.x;
+  const uint32_t n_in = 16u << p.rows_in;
+  const uint32_t* s = p.src + col * p.ss + g * 16;
+  for (uint32_t i = th; i < n_in; i += nt) sm[swz(i)] = __ldg(s + ((uint64_t)(i >> 4) << B12) + (i & 15));
+  __syncthreads();
+  if (p.do_inverse) {
+    const uint32_t RL = p.rows_in, rem = RL & 3;
+    uint32_t w0 = 0;
+    if (rem) { high_stage<true>(sm, p.itv, RL, 0, rem); w0 = rem; }
+    for (; w0 < RL; w0 += 4) high_stage<true>(sm, p.itv, RL, w0, 4);
+    for (uint32_t i = th; i < n_in; i += nt) {
+      uint32_t v = sm[swz(i)];
+      if (p.scale) { v = mmul(v, p.scale); sm[swz(i)] = v; }
+      if (p.coef) p.coef[col * p.cs + g * 16 + ((uint64_t)(i >> 4) << B12) + (i & 15)] = v;
+    }
+    __syncthreads();
+  }
+  uint32_t rows_now = p.rows_in;
+  if (p.do_forward) {
+    const uint32_t n_out = 16u << p.rows_out;
+    if (p.dup) {
+      for (uint32_t i = th; i < n_in; i += nt) sm[swz(i + n_in)] = sm[swz(i)];
+    } else {
+      for (uint32_t i = n_in + th; i < n_out; i += nt) sm[swz(i)] = 0;
+    }
+    __syncthreads();
+    const uint32_t RL = p.fwd_layers, rem = RL & 3;
+    int w0 = (int)RL - 4;
+    for (; w0 >= (int)rem; w0 -= 4) high_stage<false>(sm, p.ftv, p.rows_out, (uint32_t)w0, 4);
+    if (rem) high_stage<false>(sm, p.ftv, p.rows_out, 0, rem);
+    rows_now = p.rows_out;
+  }
+  if (p.out) {
+    const uint32_t n_now = 16u << rows_now;
+    uint32_t* o = p.out + col * p.os + g * 16;
+    for (uint32_t i = th; i < n_now; i += nt) o[((uint64_t)(i >> 4) << B12) + (i & 15)] = sm[swz(i)];
+  }
+}
+
 inline uint32_t inv_pow2(uint32_t log) { return minv(1u << log); }
 
 }  // namespace
@@ -248,7 +383,7 @@ TwiddleView DeviceTables::view(uint32_t domain_log, bool inverse) const {
 }
 
 cudaError_t build_twiddle_tower(DeviceTables& t, uint32_t root_log, cudaStream_t stream) {
-  k_build_tower<<<1024, 256, 0, stream>>>(PointTable{t.points}, root_log, t.tw, t.itw);
+  k_build_tower<<<1024, 256, 0, stream>>>(PointTable{t.points}, root_log, t.tw, t.itw); note_launch();
   t.tower_log = root_log;
   return cudaGetLastError();
 }
@@ -264,6 +399,7 @@ static cudaError_t launch_low(const DeviceTables& t, bool inverse, uint32_t doma
     k_fft_low<true><<<grid, LOW_THREADS, smem, stream>>>(src, src_stride, src_valid_log, dst, dst_stride, b, tv, scale);
   else
     k_fft_low<false><<<grid, LOW_THREADS, smem, stream>>>(src, src_stride, src_valid_log, dst, dst_stride, b, tv, scale);
+  note_launch();
   return cudaGetLastError();
 }
 
@@ -276,13 +412,61 @@ static cudaError_t launch_high(const HighParams& p, uint32_t n_cols, cudaStream_
     attr_set = true;
   }
   dim3 grid((1u << p.b) / HIGH_T, n_cols);
-  k_fft_high<<<grid, HIGH_THREADS, smem, stream>>>(p);
+  k_fft_high<<<grid, HIGH_THREADS, smem, stream>>>(p); note_launch();
+  return cudaGetLastError();
+}
+
+
+// ---- radix-16 path launchers ----------------------------------------------
+// The radix-16 kernels read and write 16-byte vectors: columns must start 16-byte aligned.
+static bool aligned16(const void* p, uint64_t stride) { return ((uintptr_t)p & 15) == 0 && (stride & 3) == 0; }
+static bool use16(uint32_t log_in, uint32_t log_out, const void* a, uint64_t sa, const void* b, uint64_t sb_) {
+  return log_in >= 16 && log_out <= 22 && aligned16(a, sa) && aligned16(b, sb_);
+}
+
+static cudaError_t launch_low12(const DeviceTables& t, bool inverse, uint32_t domain_log, uint32_t n_cols,
+                                const uint32_t* src, uint64_t ss, uint32_t* dst, uint64_t ds, uint32_t scale,
+                                cudaStream_t stream) {
+  dim3 grid(1u << (domain_log - B12), n_cols);
+  TwiddleView tv = t.view(domain_log, inverse);
+  if (inverse) k_fft_low12<true><<<grid, 256, 0, stream>>>(src, ss, dst, ds, tv, scale);
+  else k_fft_low12<false><<<grid, 256, 0, stream>>>(src, ss, dst, ds, tv, scale);
+  note_launch();
+  return cudaGetLastError();
+}
+
+static cudaError_t launch_high16(const High16Params& p, uint32_t n_cols, cudaStream_t stream) {
+  uint32_t rows = p.do_forward ? std::max(p.rows_in, p.rows_out) : p.rows_in;
+  size_t smem = (size_t)64 << rows;
+  static bool attr_set = false;
+  if (!attr_set) {
+    cudaFuncSetAttribute(k_fft_high16, cudaFuncAttributeMaxDynamicSharedMemorySize, 64 * 1024);
+    attr_set = true;
+  }
+  dim3 grid(1u << (B12 - 4), n_cols);
+  k_fft_high16<<<grid, 1u << rows, smem, stream>>>(p);
+  note_launch();
   return cudaGetLastError();
 }
 
 cudaError_t fft_columns(const DeviceTables& t, bool inverse, uint32_t log_size, uint32_t n_cols, uint32_t* cols,
                         uint64_t stride, cudaStream_t stream) {
   if (n_cols == 0) return cudaSuccess;
+  if (use16(log_size, log_size, cols, stride, cols, stride)) {
+    High16Params p{};
+    p.src = cols; p.ss = stride; p.rows_in = log_size - B12;
+    if (inverse) {
+      cudaError_t e = launch_low12(t, true, log_size, n_cols, cols, stride, cols, stride, 0, stream);
+      if (e != cudaSuccess) return e;
+      p.do_inverse = 1; p.itv = t.view(log_size, true); p.scale = inv_pow2(log_size); p.coef = cols; p.cs = stride;
+      return launch_high16(p, n_cols, stream);
+    }
+    p.do_forward = 1; p.ftv = t.view(log_size, false); p.rows_out = p.rows_in; p.fwd_layers = p.rows_in;
+    p.out = cols; p.os = stride;
+    cudaError_t e = launch_high16(p, n_cols, stream);
+    if (e != cudaSuccess) return e;
+    return launch_low12(t, false, log_size, n_cols, cols, stride, cols, stride, 0, stream);
+  }
   const uint32_t b = std::min(log_size, LOW_BITS);
   const uint32_t scale = inverse ? inv_pow2(log_size) : 0;
   if (log_size <= b)
@@ -308,6 +492,16 @@ cudaError_t extend(const DeviceTables& t, uint32_t log_size, uint32_t log_blowup
                    cudaStream_t stream) {
   if (n_cols == 0) return cudaSuccess;
   const uint32_t out_log = log_size + log_blowup;
+  if (use16(log_size, out_log, coeffs, co_stride, lde, lde_stride)) {
+    High16Params p{};
+    p.src = coeffs; p.ss = co_stride; p.rows_in = log_size - B12;
+    p.do_forward = 1; p.ftv = t.view(out_log, false); p.rows_out = out_log - B12;
+    p.dup = log_blowup == 1; p.fwd_layers = p.dup ? p.rows_in : p.rows_out;
+    p.out = lde; p.os = lde_stride;
+    cudaError_t e = launch_high16(p, n_cols, stream);
+    if (e != cudaSuccess) return e;
+    return launch_low12(t, false, out_log, n_cols, lde, lde_stride, lde, lde_stride, 0, stream);
+  }
   const uint32_t b = std::min(out_log, LOW_BITS);
   if (out_log <= b)  // single low pass with zero extension
     return launch_low(t, false, out_log, n_cols, coeffs, co_stride, log_size, lde, lde_stride, 0, stream);
@@ -340,8 +534,21 @@ cudaError_t interpolate_extend(const DeviceTables& t, uint32_t log_size, uint32_
                                const uint32_t* evals, uint64_t ev_stride, uint32_t* coeffs, uint64_t co_stride,
                                uint32_t* lde, uint64_t lde_stride, cudaStream_t stream) {
   if (n_cols == 0) return cudaSuccess;
-  const uint32_t b = std::min(log_size, LOW_BITS);
   const uint32_t out_log = log_size + log_blowup;
+  if (use16(log_size, out_log, evals, ev_stride, lde, lde_stride) && aligned16(coeffs, co_stride)) {
+    cudaError_t e = launch_low12(t, true, log_size, n_cols, evals, ev_stride, coeffs, co_stride, 0, stream);
+    if (e != cudaSuccess) return e;
+    High16Params p{};
+    p.src = coeffs; p.ss = co_stride; p.rows_in = log_size - B12;
+    p.do_inverse = 1; p.itv = t.view(log_size, true); p.scale = inv_pow2(log_size); p.coef = coeffs; p.cs = co_stride;
+    p.do_forward = 1; p.ftv = t.view(out_log, false); p.rows_out = out_log - B12;
+    p.dup = log_blowup == 1; p.fwd_layers = p.dup ? p.rows_in : p.rows_out;
+    p.out = lde; p.os = lde_stride;
+    e = launch_high16(p, n_cols, stream);
+    if (e != cudaSuccess) return e;
+    return launch_low12(t, false, out_log, n_cols, lde, lde_stride, lde, lde_stride, 0, stream);
+  }
+  const uint32_t b = std::min(log_size, LOW_BITS);
   if (log_size <= b || out_log > LOW_BITS + 12) {
     // Small domains (or unsupported fused sizes): separate transforms.
     if (coeffs != evals) {

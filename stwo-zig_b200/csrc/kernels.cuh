@@ -14,6 +14,11 @@
 
 namespace sb {
 
+// Launch counter behind stwo_b200_telemetry_snapshot (the Metal backend's dispatch
+// telemetry, src/backends/metal/telemetry.zig:49-336).
+void note_launch();
+uint64_t launch_count();
+
 // Per-device read-only tables.
 struct DeviceTables {
   PointM* points = nullptr;    // point table (circle.cuh)

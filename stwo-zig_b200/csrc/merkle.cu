@@ -37,24 +37,25 @@ __device__ __forceinline__ void store_hash(uint8_t* layers, uint64_t node, const
   d[1] = make_uint4(h[4], h[5], h[6], h[7]);
 }
 
-__device__ __forceinline__ void node_hash(const uint32_t seed[8], const uint32_t* l, const uint32_t* r, uint32_t h[8]) {
+__device__ __forceinline__ void node_hash(const uint32_t seed[8], const uint32_t* l, const uint32_t* r, uint32_t h[8],
+                                          uint32_t one) {
   uint32_t m[16];
 #pragma unroll
   for (int i = 0; i < 8; ++i) { m[i] = l[i]; m[8 + i] = r[i]; }
 #pragma unroll
   for (int i = 0; i < 8; ++i) h[i] = seed[i];
-  b2s_compress(h, m, 128, true);
+  b2s_compress(h, m, 128, true, one);
 }
 
 // Folds `count` hashes in shared memory (sm[i*8 .. i*8+8)) `levels` times;
 // level j's nodes are written to the layer of log size (top_log - j).
 __device__ void fold_levels(uint32_t* sm, uint32_t count, uint32_t levels, uint8_t* layers, uint32_t max_log,
-                            uint32_t child_log, uint64_t first_child, const uint32_t seed[8]) {
+                            uint32_t child_log, uint64_t first_child, const uint32_t seed[8], uint32_t one) {
   for (uint32_t j = 1; j <= levels; ++j) {
     uint32_t n = count >> j;
     uint32_t h[8];
     bool active = threadIdx.x < n;
-    if (active) node_hash(seed, sm + (2 * threadIdx.x) * 8, sm + (2 * threadIdx.x + 1) * 8, h);
+    if (active) node_hash(seed, sm + (2 * threadIdx.x) * 8, sm + (2 * threadIdx.x + 1) * 8, h, one);
     __syncthreads();
     if (active) {
 #pragma unroll
@@ -69,7 +70,8 @@ __device__ void fold_levels(uint32_t* sm, uint32_t count, uint32_t levels, uint8
 
 __global__ void __launch_bounds__(LEAF_THREADS) k_merkle_leaves(uint32_t log_size, uint32_t n_cols,
                                                                  const uint32_t* __restrict__ cols, uint64_t stride,
-                                                                 uint8_t* layers, Seeds seeds, uint32_t levels) {
+                                                                 uint8_t* layers, Seeds seeds, uint32_t levels,
+                                                                 uint32_t one) {
   __shared__ uint32_t sm[LEAF_THREADS * 8];
   const uint64_t row = (uint64_t)blockIdx.x * LEAF_THREADS + threadIdx.x;
   const uint64_t n_rows = 1ull << log_size;
@@ -89,7 +91,7 @@ __global__ void __launch_bounds__(LEAF_THREADS) k_merkle_leaves(uint32_t log_siz
       }
       const bool last = blk + 1 == n_blocks;
       const uint32_t t = last ? total : 64 + 64 * (blk + 1);
-      b2s_compress(h, m, t, last);
+      b2s_compress(h, m, t, last, one);
     }
     store_hash(layers, row, h);
 #pragma unroll
@@ -97,13 +99,13 @@ __global__ void __launch_bounds__(LEAF_THREADS) k_merkle_leaves(uint32_t log_siz
   }
   __syncthreads();
   uint32_t count = n_rows < LEAF_THREADS ? (uint32_t)n_rows : LEAF_THREADS;
-  fold_levels(sm, count, levels, layers, log_size, log_size, (uint64_t)blockIdx.x * LEAF_THREADS, seeds.node);
+  fold_levels(sm, count, levels, layers, log_size, log_size, (uint64_t)blockIdx.x * LEAF_THREADS, seeds.node, one);
 }
 
 // Children layer of log size child_log -> `levels` parent levels; each CTA folds
 // 2 * NODE_THREADS children (or the whole layer when smaller).
 __global__ void __launch_bounds__(NODE_THREADS) k_merkle_nodes(uint8_t* layers, uint32_t max_log, uint32_t child_log,
-                                                                uint32_t levels, Seeds seeds) {
+                                                                uint32_t levels, Seeds seeds, uint32_t one) {
   __shared__ uint32_t sm[2 * NODE_THREADS * 8];
   const uint64_t n_children = 1ull << child_log;
   const uint32_t per_cta = n_children < 2 * NODE_THREADS ? (uint32_t)n_children : 2 * NODE_THREADS;
@@ -114,7 +116,7 @@ __global__ void __launch_bounds__(NODE_THREADS) k_merkle_nodes(uint8_t* layers, 
     sm[i * 4 + 0] = v.x; sm[i * 4 + 1] = v.y; sm[i * 4 + 2] = v.z; sm[i * 4 + 3] = v.w;
   }
   __syncthreads();
-  fold_levels(sm, per_cta, levels, layers, max_log, child_log, first, seeds.node);
+  fold_levels(sm, per_cta, levels, layers, max_log, child_log, first, seeds.node, one);
 }
 
 __global__ void k_empty_root(uint8_t* layers, Seeds seeds) {
@@ -133,13 +135,13 @@ cudaError_t merkle_commit(uint32_t log_size, uint32_t n_cols, const uint32_t* co
                           uint8_t* layers, cudaStream_t stream) {
   static const Seeds seeds = make_seeds();
   if (n_cols == 0) {
-    k_empty_root<<<1, 1, 0, stream>>>(layers, seeds);
+    k_empty_root<<<1, 1, 0, stream>>>(layers, seeds); note_launch();
     return cudaGetLastError();
   }
   const uint64_t n_rows = 1ull << log_size;
   uint32_t leaf_levels = log_size < LEAF_LEVELS ? log_size : LEAF_LEVELS;
   uint32_t grid = (uint32_t)((n_rows + LEAF_THREADS - 1) / LEAF_THREADS);
-  k_merkle_leaves<<<grid, LEAF_THREADS, 0, stream>>>(log_size, n_cols, cols, stride, layers, seeds, leaf_levels);
+  k_merkle_leaves<<<grid, LEAF_THREADS, 0, stream>>>(log_size, n_cols, cols, stride, layers, seeds, leaf_levels, 1u); note_launch();
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return e;
   uint32_t child_log = log_size - leaf_levels;
@@ -148,7 +150,7 @@ cudaError_t merkle_commit(uint32_t log_size, uint32_t n_cols, const uint32_t* co
     uint64_t n_children = 1ull << child_log;
     uint32_t per_cta = n_children < 2 * NODE_THREADS ? (uint32_t)n_children : 2 * NODE_THREADS;
     uint32_t blocks = (uint32_t)(n_children / per_cta);
-    k_merkle_nodes<<<blocks, NODE_THREADS, 0, stream>>>(layers, log_size, child_log, levels, seeds);
+    k_merkle_nodes<<<blocks, NODE_THREADS, 0, stream>>>(layers, log_size, child_log, levels, seeds, 1u); note_launch();
     e = cudaGetLastError();
     if (e != cudaSuccess) return e;
     child_log -= levels;
@@ -175,7 +177,7 @@ __device__ __forceinline__ uint32_t ctz128(uint32_t a, uint32_t b, uint32_t c, u
 struct PowPrefix { uint32_t w[8]; };
 
 __global__ void __launch_bounds__(256) k_pow(PowPrefix pre, uint32_t n_bits, uint64_t max_nonce,
-                                             unsigned long long* found, uint32_t* status) {
+                                             unsigned long long* found, uint32_t* status, uint32_t one) {
   const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
   uint64_t nonce = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
   uint32_t iter = 0;
@@ -189,13 +191,13 @@ __global__ void __launch_bounds__(256) k_pow(PowPrefix pre, uint32_t n_bits, uin
     m[8] = (uint32_t)nonce; m[9] = (uint32_t)(nonce >> 32);
 #pragma unroll
     for (int i = 10; i < 16; ++i) m[i] = 0;
-    b2s_compress(h, m, 40, true);
+    b2s_compress(h, m, 40, true, one);
     if (ctz128(h[0], h[1], h[2], h[3]) >= n_bits) {
       atomicMin(found, (unsigned long long)nonce);
       return;
     }
     nonce += stride;
-    if ((++iter & 15) == 0) best = *((volatile unsigned long long*)found);
+    if ((++iter & 3) == 0) best = *((volatile unsigned long long*)found);
   }
   if (nonce >= max_nonce && threadIdx.x == 0 && blockIdx.x == 0) {
     // Reached the search bound: the host reports a timeout unless a nonce was found.
@@ -218,7 +220,7 @@ cudaError_t pow_grind(const uint32_t prefix_words[8], uint32_t n_bits, uint64_t 
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
   k_pow<<<sms * 8, 256, 0, stream>>>(pre, n_bits, max_nonce, reinterpret_cast<unsigned long long*>(result_dev),
-                                     result_dev + 2);
+                                     result_dev + 2, 1u); note_launch();
   return cudaGetLastError();
 }
 

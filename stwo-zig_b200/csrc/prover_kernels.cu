@@ -285,7 +285,7 @@ inline uint32_t grid_for(uint64_t n, uint32_t threads, uint32_t cap = 148 * 32) 
 
 cudaError_t wide_fib_trace(uint32_t log_n, uint32_t W, int kind, uint64_t seed, uint32_t* out, uint64_t stride,
                            cudaStream_t stream) {
-  k_wide_fib_trace<<<grid_for(1ull << log_n, 256), 256, 0, stream>>>(log_n, W, kind, seed, out, stride);
+  k_wide_fib_trace<<<grid_for(1ull << log_n, 256), 256, 0, stream>>>(log_n, W, kind, seed, out, stride); note_launch();
   return cudaGetLastError();
 }
 
@@ -298,7 +298,7 @@ cudaError_t wide_fib_composition(uint32_t log_n, uint32_t W, const uint32_t* eva
     if (e != cudaSuccess) return e;
   }
   k_composition<<<grid_for(2ull << log_n, 256), 256, smem, stream>>>(log_n, W, eval, stride, coeffs_dev, den_inv0,
-                                                                     den_inv1, out, out_stride);
+                                                                     den_inv1, out, out_stride); note_launch();
   return cudaGetLastError();
 }
 
@@ -320,10 +320,10 @@ cudaError_t eval_at_point(const DeviceTables&, uint32_t log_size, uint32_t n_col
   uint32_t chunk_bits = log_size < OODS_CHUNK_BITS ? log_size : OODS_CHUNK_BITS;
   uint32_t n_chunks = 1u << (log_size - chunk_bits);
   dim3 grid(n_chunks, n_cols);
-  k_oods_chunks<<<grid, OODS_THREADS, 0, stream>>>(F, coeffs, stride, partial, n_chunks);
+  k_oods_chunks<<<grid, OODS_THREADS, 0, stream>>>(F, coeffs, stride, partial, n_chunks); note_launch();
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return e;
-  k_oods_sum<<<(n_cols + 127) / 128, 128, 0, stream>>>(partial, n_chunks, n_cols, out);
+  k_oods_sum<<<(n_cols + 127) / 128, 128, 0, stream>>>(partial, n_chunks, n_cols, out); note_launch();
   return cudaGetLastError();
 }
 
@@ -337,7 +337,7 @@ cudaError_t accumulate_quotients(const DeviceTables& t, uint32_t log_size, uint3
     attr = true;
   }
   k_quotients<<<grid_for(1ull << log_size, 256), 256, smem, stream>>>(PointTable{t.points}, log_size, n_batches,
-                                                                      batches, col_ptrs, coeff_c, out, out_stride);
+                                                                      batches, col_ptrs, coeff_c, out, out_stride); note_launch();
   return cudaGetLastError();
 }
 
@@ -346,7 +346,7 @@ cudaError_t fold_circle_into_line(const DeviceTables& t, uint32_t src_log, const
                                   cudaStream_t stream) {
   TwiddleView itv = t.view(src_log, true);
   k_fold_circle<<<grid_for(1ull << (src_log - 1), 256), 256, 0, stream>>>(itv, src_log - 1, src, src_stride, alpha,
-                                                                          qsq(alpha), dst, dst_stride, accumulate);
+                                                                          qsq(alpha), dst, dst_stride, accumulate); note_launch();
   return cudaGetLastError();
 }
 
@@ -356,19 +356,19 @@ cudaError_t fold_line(const DeviceTables& t, uint32_t src_log, const uint32_t* s
   // the circle domain of log src_log + 1.
   TwiddleView itv = t.view(src_log + 1, true);
   k_fold_line<<<grid_for(1ull << (src_log - 1), 256), 256, 0, stream>>>(itv, src_log - 1, src, src_stride, alpha, dst,
-                                                                        dst_stride);
+                                                                        dst_stride); note_launch();
   return cudaGetLastError();
 }
 
 cudaError_t gather_words(const GatherItem* items, uint32_t n, uint32_t* out, cudaStream_t stream) {
   if (n == 0) return cudaSuccess;
-  k_gather_words<<<(n + 255) / 256, 256, 0, stream>>>(items, n, out);
+  k_gather_words<<<(n + 255) / 256, 256, 0, stream>>>(items, n, out); note_launch();
   return cudaGetLastError();
 }
 
 cudaError_t gather_hashes(const HashGatherItem* items, uint32_t n, uint8_t* out, cudaStream_t stream) {
   if (n == 0) return cudaSuccess;
-  k_gather_hashes<<<(n + 255) / 256, 256, 0, stream>>>(items, n, out);
+  k_gather_hashes<<<(n + 255) / 256, 256, 0, stream>>>(items, n, out); note_launch();
   return cudaGetLastError();
 }
 

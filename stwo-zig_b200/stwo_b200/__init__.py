@@ -66,7 +66,8 @@ _SIGS = {
                                        ctypes.POINTER(ctypes.c_size_t), ctypes.POINTER(StageTimesC)],
     "stwo_b200_prove_wide_fibonacci_batch": [_vp, ctypes.POINTER(RequestC), ctypes.c_size_t,
                                              ctypes.POINTER(_vp), ctypes.POINTER(ctypes.c_size_t),
-                                             ctypes.POINTER(ctypes.c_size_t), ctypes.POINTER(_i32), _u32],
+                                             ctypes.POINTER(ctypes.c_size_t), ctypes.POINTER(_i32), _u32,
+                                             ctypes.POINTER(StageTimesC)],
     "stwo_b200_interpolate_columns": [_vp, _u32, _u32, _vp, _u64, _vp],
     "stwo_b200_evaluate_columns": [_vp, _u32, _u32, _vp, _u64, _vp],
     "stwo_b200_interpolate_and_extend": [_vp, _u32, _u32, _u32, _vp, _u64, _vp, _u64, _vp, _u64, _vp],
@@ -79,6 +80,7 @@ _SIGS = {
     "stwo_b200_wide_fib_trace": [_vp, _u32, _u32, _u32, _u64, _vp, _u64, _vp],
     "stwo_b200_wide_fib_composition": [_vp, _u32, _u32, _vp, _u64, _vp, _u32, _u32, _vp, _u64, _vp],
     "stwo_b200_pow_grind": [_vp, ctypes.c_char_p, _u32, ctypes.POINTER(_u64)],
+    "stwo_b200_telemetry_snapshot": [ctypes.POINTER(_u64)],
 }
 for _name, _args in _SIGS.items():
     _fn = getattr(_lib, _name)
@@ -105,6 +107,13 @@ def _check(status: int) -> None:
 
 def lib():
     return _lib
+
+
+def kernel_launches() -> int:
+    """Kernels this library has launched in the process (telemetry counter)."""
+    v = _u64(0)
+    _check(_lib.stwo_b200_telemetry_snapshot(ctypes.byref(v)))
+    return v.value
 
 
 # ---------------------------------------------------------------------------
@@ -175,6 +184,7 @@ class Context:
         _check(_lib.stwo_b200_context_create(device, ctypes.byref(h)))
         self._h = h
         self.device = device
+        self._cap = 1 << 21
 
     def close(self) -> None:
         if self._h:
@@ -201,7 +211,8 @@ class Context:
                 req.trace_device = trace.data_ptr()
             else:
                 import numpy as np
-                keep = np.ascontiguousarray(trace, dtype=np.uint32)
+                keep = trace if (isinstance(trace, np.ndarray) and trace.dtype == np.uint32
+                                 and trace.flags.c_contiguous) else np.ascontiguousarray(trace, dtype=np.uint32)
                 req.trace_host = keep.ctypes.data
             keep = (keep, trace)
         req.trace_kind = trace_kind
@@ -215,19 +226,26 @@ class Context:
                              with_times: bool = False):
         """Proves the wide-Fibonacci AIR; returns the JSON wire proof bytes (and stage times)."""
         req, keep = self._request(statement, config, trace, trace_kind, trace_seed, channel_seed)
-        cap = 1 << 24
+        cap = self._cap
         buf = ctypes.create_string_buffer(cap)
         n = ctypes.c_size_t(0)
         times = StageTimesC()
-        _check(_lib.stwo_b200_prove_wide_fibonacci(self._h, ctypes.byref(req), buf, cap, ctypes.byref(n),
-                                                   ctypes.byref(times)))
+        rc = _lib.stwo_b200_prove_wide_fibonacci(self._h, ctypes.byref(req), buf, cap, ctypes.byref(n),
+                                                 ctypes.byref(times))
+        if rc == E_BUFFER_TOO_SMALL:
+            self._cap = cap = max(2 * cap, n.value)
+            buf = ctypes.create_string_buffer(cap)
+            rc = _lib.stwo_b200_prove_wide_fibonacci(self._h, ctypes.byref(req), buf, cap, ctypes.byref(n),
+                                                     ctypes.byref(times))
+        _check(rc)
         del keep
         proof = buf.raw[: n.value]
         if with_times:
             return proof, {name: getattr(times, name) for name, _ in StageTimesC._fields_}
         return proof
 
-    def prove_wide_fibonacci_batch(self, requests: list[dict], max_in_flight: int = 4) -> list[bytes]:
+    def prove_wide_fibonacci_batch(self, requests: list[dict], max_in_flight: int = 4, with_times: bool = False,
+                                   proof_cap: int = 1 << 21):
         """requests: dicts with statement, config and optional trace / trace_kind / trace_seed / channel_seed."""
         n = len(requests)
         arr = (RequestC * n)()
@@ -237,15 +255,20 @@ class Context:
                                       r.get("trace_seed", 0), r.get("channel_seed"))
             arr[i] = req
             keeps.append(keep)
-        cap = 1 << 24
+        cap = proof_cap
         bufs = [ctypes.create_string_buffer(cap) for _ in range(n)]
         outs = (_vp * n)(*[ctypes.cast(b, _vp) for b in bufs])
         caps = (ctypes.c_size_t * n)(*([cap] * n))
         lens = (ctypes.c_size_t * n)()
         statuses = (_i32 * n)()
-        _check(_lib.stwo_b200_prove_wide_fibonacci_batch(self._h, arr, n, outs, caps, lens, statuses, max_in_flight))
+        times = (StageTimesC * n)()
+        _check(_lib.stwo_b200_prove_wide_fibonacci_batch(self._h, arr, n, outs, caps, lens, statuses, max_in_flight,
+                                                         times))
         del keeps
-        return [bufs[i].raw[: lens[i]] for i in range(n)]
+        proofs = [bufs[i].raw[: lens[i]] for i in range(n)]
+        if with_times:
+            return proofs, [{k: getattr(times[i], k) for k, _ in StageTimesC._fields_} for i in range(n)]
+        return proofs
 
     # ---- backend-contract operations (device tensors) ------------------------
     def interpolate(self, cols, log_size: int, n_cols: int, stride: int, stream=None) -> None:

@@ -25,7 +25,7 @@ def rand_cols(rng, n_cols, log):
     return rng.integers(0, P, size=(n_cols, 1 << log), dtype=np.uint32)
 
 
-@pytest.mark.parametrize("log", [1, 2, 3, 4, 7, 11, 12, 13, 16, 20])
+@pytest.mark.parametrize("log", [1, 2, 3, 4, 7, 11, 12, 13, 15, 16, 17, 18, 19, 20, 21, 22])
 def test_interpolate_evaluate(ctx, log):
     rng = np.random.default_rng(log)
     n_cols = 3
@@ -39,7 +39,8 @@ def test_interpolate_evaluate(ctx, log):
     assert np.array_equal(host(d).reshape(n_cols, -1), cols)
 
 
-@pytest.mark.parametrize("log,blowup", [(1, 1), (3, 1), (10, 1), (11, 1), (12, 1), (15, 1), (20, 1), (12, 2), (5, 3)])
+@pytest.mark.parametrize("log,blowup", [(1, 1), (3, 1), (10, 1), (11, 1), (12, 1), (15, 1), (16, 1), (17, 1),
+                                        (19, 1), (20, 1), (21, 1), (12, 2), (16, 2), (18, 3), (5, 3)])
 def test_interpolate_and_extend(ctx, log, blowup):
     import torch
     rng = np.random.default_rng(100 + log)
