@@ -300,64 +300,145 @@ struct High16Params {
   uint32_t* out; uint64_t os;
 };
 
-// One window stage over the tile: threads [0, 2^rows * ... ) own 16 rows each.
-template <bool INV>
-__device__ __forceinline__ void high_stage(uint32_t* sm, const TwiddleView& tv, uint32_t rows, uint32_t w0,
-                                           uint32_t nl) {
+// Tile of the high pass: 2^rows rows x 16 adjacent low indices; tile element
+// i = (m << 4) | t is transform index (m << 12) + g*16 + t. A window stage gives
+// thread (q, t) the 16 rows spread(q, W0) + (k << W0).
+//
+// SRC: 0 = shared memory, 1 = global source rows (rows beyond the source are
+// duplicates when DUP, zeros otherwise); DST: 0 = shared memory, 1 = global
+// output, 2 = scale, store coefficients to global and to shared memory (also at
+// row + 2^rows_src when DUP).
+struct HighIo {
+  const uint32_t* src; uint32_t src_rows;  // source rows (log)
+  uint32_t* out;                           // global destination tile base (column + g*16)
+  uint32_t scale;
+  int dup;
+};
+
+template <bool INV, int W0, int NL, int SRC, int DST>
+__device__ __noinline__ void high_stage(uint32_t* sm, const TwiddleView tv, uint32_t rows, const HighIo io) {
   const uint32_t th = threadIdx.x;
   if (th < (1u << rows)) {
     const uint32_t t = th & 15, q = th >> 4;
-    const uint32_t mb = spread(q, w0);
+    const uint32_t mb = spread(q, W0);
     const uint32_t a = swz((mb << 4) | t);
     uint32_t x[16];
+    if (SRC == 0) {
 #pragma unroll
-    for (int k = 0; k < 16; ++k) x[k] = sm[a ^ swz((uint32_t)k << (w0 + 4))];
-    radix16_dyn<INV>(x, tv, B12, w0, mb, nl);
+      for (int k = 0; k < 16; ++k) x[k] = sm[a ^ swz((uint32_t)k << (W0 + 4))];
+    } else {
+      const uint32_t src_n = 1u << io.src_rows;
 #pragma unroll
-    for (int k = 0; k < 16; ++k) sm[a ^ swz((uint32_t)k << (w0 + 4))] = x[k];
+      for (int k = 0; k < 16; ++k) {
+        uint32_t m = mb + ((uint32_t)k << W0);
+        uint32_t v = 0;
+        if (m < src_n) v = __ldg(io.src + ((uint64_t)m << B12) + t);
+        else if (io.dup) v = __ldg(io.src + ((uint64_t)(m - src_n) << B12) + t);
+        x[k] = v;
+      }
+    }
+    radix16<INV, 0, NL>(x, tv, B12, W0, mb);
+    if (DST == 0) {
+#pragma unroll
+      for (int k = 0; k < 16; ++k) sm[a ^ swz((uint32_t)k << (W0 + 4))] = x[k];
+    } else if (DST == 1) {
+#pragma unroll
+      for (int k = 0; k < 16; ++k) io.out[((uint64_t)(mb + ((uint32_t)k << W0)) << B12) + t] = x[k];
+    } else {
+      const uint32_t dup_off = swz((1u << rows) << 4);
+#pragma unroll
+      for (int k = 0; k < 16; ++k) {
+        uint32_t v = io.scale ? mmul(x[k], io.scale) : x[k];
+        io.out[((uint64_t)(mb + ((uint32_t)k << W0)) << B12) + t] = v;
+        uint32_t pos = a ^ swz((uint32_t)k << (W0 + 4));
+        sm[pos] = v;
+        if (io.dup) sm[pos ^ dup_off] = v;
+      }
+    }
   }
   __syncthreads();
 }
 
-// Grid (256 tiles of 16 adjacent low indices, n_cols); blockDim = 2^rows_max threads.
+template <bool INV, int W0, int NL>
+__device__ __forceinline__ void high_stage_io(uint32_t* sm, const TwiddleView& tv, uint32_t rows, const HighIo& io,
+                                              int src, int dst) {
+  if (src == 0 && dst == 0) high_stage<INV, W0, NL, 0, 0>(sm, tv, rows, io);
+  else if (src == 0 && dst == 1) high_stage<INV, W0, NL, 0, 1>(sm, tv, rows, io);
+  else if (src == 0 && dst == 2) high_stage<INV, W0, NL, 0, 2>(sm, tv, rows, io);
+  else if (src == 1 && dst == 0) high_stage<INV, W0, NL, 1, 0>(sm, tv, rows, io);
+  else if (src == 1 && dst == 1) high_stage<INV, W0, NL, 1, 1>(sm, tv, rows, io);
+  else high_stage<INV, W0, NL, 1, 2>(sm, tv, rows, io);
+}
+
+// Runtime (w0, nl) -> compiled stage. Windows used: w0 in [0, 6], nl = 4 except
+// the short stage at w0 = 0.
+template <bool INV>
+__device__ void high_stage_dyn(uint32_t* sm, const TwiddleView& tv, uint32_t rows, const HighIo& io, uint32_t w0,
+                               uint32_t nl, int src, int dst) {
+  if (nl == 4) {
+    switch (w0) {
+      case 0: high_stage_io<INV, 0, 4>(sm, tv, rows, io, src, dst); break;
+      case 1: high_stage_io<INV, 1, 4>(sm, tv, rows, io, src, dst); break;
+      case 2: high_stage_io<INV, 2, 4>(sm, tv, rows, io, src, dst); break;
+      case 3: high_stage_io<INV, 3, 4>(sm, tv, rows, io, src, dst); break;
+      case 4: high_stage_io<INV, 4, 4>(sm, tv, rows, io, src, dst); break;
+      case 5: high_stage_io<INV, 5, 4>(sm, tv, rows, io, src, dst); break;
+      default: high_stage_io<INV, 6, 4>(sm, tv, rows, io, src, dst); break;
+    }
+  } else if (nl == 3) {
+    high_stage_io<INV, 0, 3>(sm, tv, rows, io, src, dst);
+  } else if (nl == 2) {
+    high_stage_io<INV, 0, 2>(sm, tv, rows, io, src, dst);
+  } else {
+    high_stage_io<INV, 0, 1>(sm, tv, rows, io, src, dst);
+  }
+}
+
+// Grid (256 tiles of 16 adjacent low indices, n_cols); blockDim = 2^max(rows) threads.
+// Phases: inverse layers [12, 12 + rows_in) then 1/n scale and coefficient store;
+// forward layers of the extended tile. Every stage keeps its 16 elements in
+// registers; only the first stage reads global memory and only the last writes it.
 __global__ void __launch_bounds__(1024) k_fft_high16(High16Params p) {
   extern __shared__ uint32_t sm[];
-  const uint32_t g = blockIdx.x, col = blockIdx.y, th = threadIdx.x, nt = blockDim.x;
-  const uint32_t n_in = 16u << p.rows_in;
-  const uint32_t* s = p.src + col * p.ss + g * 16;
-  for (uint32_t i = th; i < n_in; i += nt) sm[swz(i)] = __ldg(s + ((uint64_t)(i >> 4) << B12) + (i & 15));
-  __syncthreads();
+  const uint32_t g = blockIdx.x, col = blockIdx.y;
+  HighIo io;
+  io.src = p.src + col * p.ss + g * 16;
+  io.src_rows = p.rows_in;
+  io.scale = p.scale;
+  io.dup = p.dup;
   if (p.do_inverse) {
     const uint32_t RL = p.rows_in, rem = RL & 3;
+    const uint32_t n_st = (RL >> 2) + (rem ? 1 : 0);
+    io.out = p.coef + col * p.cs + g * 16;
     uint32_t w0 = 0;
-    if (rem) { high_stage<true>(sm, p.itv, RL, 0, rem); w0 = rem; }
-    for (; w0 < RL; w0 += 4) high_stage<true>(sm, p.itv, RL, w0, 4);
-    for (uint32_t i = th; i < n_in; i += nt) {
-      uint32_t v = sm[swz(i)];
-      if (p.scale) { v = mmul(v, p.scale); sm[swz(i)] = v; }
-      if (p.coef) p.coef[col * p.cs + g * 16 + ((uint64_t)(i >> 4) << B12) + (i & 15)] = v;
+    for (uint32_t st = 0; st < n_st; ++st) {
+      const uint32_t nl = (st == 0 && rem) ? rem : 4;
+      const int src = st == 0 ? 1 : 0;
+      const int dst = st + 1 == n_st ? 2 : 0;
+      // a pure inverse transform (no forward phase) needs no shared copy at the end
+      high_stage_dyn<true>(sm, p.itv, RL, io, w0, nl, src, dst);
+      w0 += nl;
     }
-    __syncthreads();
   }
-  uint32_t rows_now = p.rows_in;
   if (p.do_forward) {
-    const uint32_t n_out = 16u << p.rows_out;
-    if (p.dup) {
-      for (uint32_t i = th; i < n_in; i += nt) sm[swz(i + n_in)] = sm[swz(i)];
-    } else {
-      for (uint32_t i = n_in + th; i < n_out; i += nt) sm[swz(i)] = 0;
-    }
-    __syncthreads();
     const uint32_t RL = p.fwd_layers, rem = RL & 3;
+    const uint32_t n_st = (RL >> 2) + (rem ? 1 : 0);
+    io.out = p.out + col * p.os + g * 16;
+    if (p.do_inverse && !p.dup && p.rows_out > p.rows_in) {
+      // zero extension after an inverse phase: rows beyond the coefficients are zero
+      for (uint32_t i = (16u << p.rows_in) + threadIdx.x; i < (16u << p.rows_out); i += blockDim.x) sm[swz(i)] = 0;
+      __syncthreads();
+    }
     int w0 = (int)RL - 4;
-    for (; w0 >= (int)rem; w0 -= 4) high_stage<false>(sm, p.ftv, p.rows_out, (uint32_t)w0, 4);
-    if (rem) high_stage<false>(sm, p.ftv, p.rows_out, 0, rem);
-    rows_now = p.rows_out;
-  }
-  if (p.out) {
-    const uint32_t n_now = 16u << rows_now;
-    uint32_t* o = p.out + col * p.os + g * 16;
-    for (uint32_t i = th; i < n_now; i += nt) o[((uint64_t)(i >> 4) << B12) + (i & 15)] = sm[swz(i)];
+    for (uint32_t st = 0; st < n_st; ++st) {
+      const bool short_st = rem && st + 1 == n_st;
+      const uint32_t nl = short_st ? rem : 4;
+      const uint32_t ww = short_st ? 0 : (uint32_t)w0;
+      const int src = (st == 0 && !p.do_inverse) ? 1 : 0;
+      const int dst = st + 1 == n_st ? 1 : 0;
+      high_stage_dyn<false>(sm, p.ftv, p.rows_out, io, ww, nl, src, dst);
+      w0 -= 4;
+    }
   }
 }
 
