@@ -148,6 +148,20 @@ int32_t stwo_b200_eval_at_point(stwo_b200_context* ctx, uint32_t log_size, uint3
                                 uint64_t stride, stwo_b200_qm31 px, stwo_b200_qm31 py, stwo_b200_qm31* out_dev,
                                 void* stream);
 
+/* Same result as stwo_b200_eval_at_point, but it allocates nothing: no reference counterpart (the
+ * reference evaluates on the host). For callers that cannot allocate device memory when they need
+ * this value, e.g. a serving loop bound to an admitted device-memory budget, an embedder whose arena
+ * owns all device memory, or code where CUDA allocation calls are not allowed. The per-chunk partial
+ * sums live in one fixed device array of STWO_B200_NOALLOC_EVAL_SCRATCH 16-byte entries (1 MiB, kept
+ * on every GPU that loads the library until exit): n_cols * max(1, 2^(log_size-12)) must not exceed
+ * it, else STWO_B200_E_INVALID. All calls on a device share the array, so calls whose work overlaps
+ * on the GPU race: serialize them. The first call on each device looks up the array's address; make
+ * it before any stream capture. */
+#define STWO_B200_NOALLOC_EVAL_SCRATCH 65536
+int32_t stwo_b200_eval_at_point_noalloc(stwo_b200_context* ctx, uint32_t log_size, uint32_t n_cols,
+                                        const uint32_t* coeffs, uint64_t stride, stwo_b200_qm31 px,
+                                        stwo_b200_qm31 py, stwo_b200_qm31* out_dev, void* stream);
+
 /* ---- MerkleOps (src/backend/merkle_ops.zig:20-56) ------------------------------------------------ */
 
 /* Blake2s lifted Merkle commitment of n_cols columns of 2^log_size rows ("leaf"/"node" prefixed

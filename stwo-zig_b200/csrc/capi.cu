@@ -6,11 +6,8 @@
 #include <vector>
 
 #include "../../include/stwo_b200.h"
+#include "context.hpp"
 #include "prover.hpp"
-
-struct stwo_b200_context {
-  sb::Context ctx;
-};
 
 namespace sb {
 static std::atomic<uint64_t> g_launches(0);
@@ -26,6 +23,13 @@ int32_t set_error(int32_t code, const std::string& msg) {
   g_last_error = msg;
   return code;
 }
+}  // namespace
+
+namespace sb {
+int32_t set_last_error(int32_t code, const std::string& msg) { return set_error(code, msg); }
+}  // namespace sb
+
+namespace {
 
 #define CK_CTX(c)                                                      \
   do {                                                                 \

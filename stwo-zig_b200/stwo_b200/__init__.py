@@ -73,6 +73,7 @@ _SIGS = {
     "stwo_b200_interpolate_and_extend": [_vp, _u32, _u32, _u32, _vp, _u64, _vp, _u64, _vp, _u64, _vp],
     "stwo_b200_extend_columns": [_vp, _u32, _u32, _u32, _vp, _u64, _vp, _u64, _vp],
     "stwo_b200_eval_at_point": [_vp, _u32, _u32, _vp, _u64, QM31C, QM31C, _vp, _vp],
+    "stwo_b200_eval_at_point_noalloc": [_vp, _u32, _u32, _vp, _u64, QM31C, QM31C, _vp, _vp],
     "stwo_b200_merkle_commit": [_vp, _u32, _u32, _vp, _u64, _vp, _vp, _vp],
     "stwo_b200_fold_circle_into_line": [_vp, _u32, _vp, _u64, QM31C, _vp, _u64, _i32, _vp],
     "stwo_b200_fold_line": [_vp, _u32, _vp, _u64, QM31C, _vp, _u64, _vp],
@@ -304,6 +305,13 @@ class Context:
     def eval_at_point(self, coeffs, log_size: int, n_cols: int, stride: int, px, py, out, stream=None) -> None:
         _check(_lib.stwo_b200_eval_at_point(self._h, log_size, n_cols, _ptr(coeffs), stride, _qm(px), _qm(py),
                                             _ptr(out), _stream(stream)))
+
+    def eval_at_point_noalloc(self, coeffs, log_size: int, n_cols: int, stride: int, px, py, out,
+                              stream=None) -> None:
+        """eval_at_point without any device allocation: partial sums go to the library's fixed
+        scratch array (shared by all calls on the device; serialize calls that would overlap)."""
+        _check(_lib.stwo_b200_eval_at_point_noalloc(self._h, log_size, n_cols, _ptr(coeffs), stride, _qm(px),
+                                                    _qm(py), _ptr(out), _stream(stream)))
 
     def accumulate_quotients(self, log_size: int, col_ptrs, c, px, py, sum_a, sum_b, out, n_cols: int,
                              stream=None) -> None:
