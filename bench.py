@@ -30,7 +30,7 @@ sys.path.insert(0, os.path.join(ROOT, "stwo-zig_b200"))
 
 METRIC = "proofs/s & p99 ms: batched vs single-proof on 1 B200, wide-Fib 2^20x100, exact"
 LOG_N, WIDTH = 20, 100
-IN_FLIGHT = 4
+IN_FLIGHT = 8
 
 
 def parse():

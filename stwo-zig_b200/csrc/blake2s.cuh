@@ -29,13 +29,18 @@ struct B2sIv {
 // Additions can be issued on the FMA pipe as IMAD x*one+y with a runtime `one`
 // (the XOR/rotate half of G keeps the ALU pipe busy; splitting the adds off
 // balances the two pipes). On the host `one` is ignored.
+SB_HD uint32_t b2s_fadd(uint32_t a, uint32_t b, uint32_t one) {
 #if defined(__CUDA_ARCH__)
-__device__ __forceinline__ uint32_t fadd(uint32_t a, uint32_t b, uint32_t one) {
   uint32_t r;
   asm("mad.lo.u32 %0, %1, %2, %3;" : "=r"(r) : "r"(a), "r"(one), "r"(b));
   return r;
+#else
+  (void)one;
+  return a + b;
+#endif
 }
-#define SB_ADD(a, b) fadd((a), (b), one)
+#if defined(__CUDA_ARCH__)
+#define SB_ADD(a, b) b2s_fadd((a), (b), one)
 #else
 #define SB_ADD(a, b) ((a) + (b))
 #endif

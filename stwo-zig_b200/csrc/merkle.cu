@@ -21,6 +21,7 @@ namespace {
 constexpr uint32_t LEAF_THREADS = 256;  // leaves per CTA
 constexpr uint32_t LEAF_LEVELS = 8;     // node levels folded inside a leaf CTA
 constexpr uint32_t NODE_THREADS = 256;  // parents per CTA at the first level
+constexpr uint32_t NODE_FOLD_LOG = 12;  // layers up to 2^12 nodes fold inside CTAs
 
 struct Seeds { uint32_t leaf[8], node[8]; };
 
@@ -119,6 +120,20 @@ __global__ void __launch_bounds__(NODE_THREADS) k_merkle_nodes(uint8_t* layers, 
   fold_levels(sm, per_cta, levels, layers, max_log, child_log, first, seeds.node, one);
 }
 
+// One parent layer, one thread per parent (used while layers are large, so every
+// compression has a thread of its own).
+__global__ void __launch_bounds__(256) k_merkle_layer(uint8_t* layers, uint32_t max_log, uint32_t parent_log,
+                                                     Seeds seeds, uint32_t one) {
+  const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= (1ull << parent_log)) return;
+  const uint4* c = reinterpret_cast<const uint4*>(layers + (merkle_layer_offset(max_log, parent_log + 1) + 2 * i) * 32);
+  uint4 a = c[0], b = c[1], d = c[2], e = c[3];
+  uint32_t l[8] = {a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w}, r[8] = {d.x, d.y, d.z, d.w, e.x, e.y, e.z, e.w};
+  uint32_t h[8];
+  node_hash(seeds.node, l, r, h, one);
+  store_hash(layers, merkle_layer_offset(max_log, parent_log) + i, h);
+}
+
 __global__ void k_empty_root(uint8_t* layers, Seeds seeds) {
   // No columns: the single leaf hashes the prefix block alone, as the final block.
   uint32_t h[8];
@@ -139,12 +154,22 @@ cudaError_t merkle_commit(uint32_t log_size, uint32_t n_cols, const uint32_t* co
     return cudaGetLastError();
   }
   const uint64_t n_rows = 1ull << log_size;
-  uint32_t leaf_levels = log_size < LEAF_LEVELS ? log_size : LEAF_LEVELS;
+  // A tree that fits one CTA is folded to its root in the leaf launch; larger
+  // trees keep the leaf CTAs short (no fold) and fold layer by layer.
+  uint32_t leaf_levels = log_size <= LEAF_LEVELS ? log_size : 0;
   uint32_t grid = (uint32_t)((n_rows + LEAF_THREADS - 1) / LEAF_THREADS);
   k_merkle_leaves<<<grid, LEAF_THREADS, 0, stream>>>(log_size, n_cols, cols, stride, layers, seeds, leaf_levels, 1u); note_launch();
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return e;
   uint32_t child_log = log_size - leaf_levels;
+  while (child_log > NODE_FOLD_LOG) {
+    uint32_t parent_log = child_log - 1;
+    uint32_t blocks = (uint32_t)(((1ull << parent_log) + 255) / 256);
+    k_merkle_layer<<<blocks, 256, 0, stream>>>(layers, log_size, parent_log, seeds, 1u); note_launch();
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    child_log = parent_log;
+  }
   while (child_log > 0) {
     uint32_t levels = child_log < 9 ? child_log : 9;
     uint64_t n_children = 1ull << child_log;
