@@ -99,10 +99,25 @@ cudaError_t fold_circle_into_line(const DeviceTables& t, uint32_t src_log, const
 cudaError_t fold_line(const DeviceTables& t, uint32_t src_log, const uint32_t* src, uint64_t src_stride,
                       QM31 alpha, uint32_t* dst, uint64_t dst_stride, cudaStream_t stream);
 
+// FRI fold (circle -> line when `circle`, else line -> line with the source line
+// domain halfOdds(src_log)) fused with the commitment of the folded layer: when
+// `layers` is non-null the folded values are hashed as leaves (4 words each) and
+// the whole tree of 2^(src_log-1) leaves is built.
+cudaError_t fri_fold_commit(const DeviceTables& t, bool circle, uint32_t src_log, const uint32_t* src,
+                            uint64_t src_stride, QM31 alpha, uint32_t* dst, uint64_t dst_stride, uint8_t* layers,
+                            cudaStream_t stream);
+
 // ---- Proof of work (src/core/channel/blake2s.zig:135-240) ------------------
 // result[0..1] = lowest valid nonce (u64), result[2] = status (0 ok, 1 gave up).
 cudaError_t pow_grind(const uint32_t prefix_words[8], uint32_t n_bits, uint64_t max_nonce,
                       uint32_t* result_dev, cudaStream_t stream);
+
+// Bounded rounds of the same search (the form the prover uses, so the grind
+// never holds every SM slot for the whole search): result_dev[0..1] must start
+// at ~0; round r covers nonces [base, base + pow_round_nonces(sm_count)).
+uint64_t pow_round_nonces(int sm_count);
+cudaError_t pow_round(const uint32_t prefix_words[8], uint32_t n_bits, uint64_t base, uint32_t* result_dev,
+                      int sm_count, cudaStream_t stream);
 
 // ---- Trace generation (src/examples/wide_fibonacci/trace.zig:34-162) -------
 cudaError_t wide_fib_trace(uint32_t log_n, uint32_t W, int kind, uint64_t seed, uint32_t* out,

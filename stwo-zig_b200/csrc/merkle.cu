@@ -134,6 +134,51 @@ __global__ void __launch_bounds__(256) k_merkle_layer(uint8_t* layers, uint32_t 
   store_hash(layers, merkle_layer_offset(max_log, parent_log) + i, h);
 }
 
+// FRI fold fused with the next layer's commitment (src/core/fri/folding.zig:352-384,
+// 558-602; src/prover/fri.zig:377-592): thread i folds pair (2i, 2i+1) of the source
+// into line value i, stores its 4 coordinates and, when `layers` is set, hashes it
+// as leaf i of the next layer's tree (4 words, one compression) and folds `levels`
+// node levels inside the CTA.
+__device__ __forceinline__ void fri_ibfly(QM31& f0, QM31& f1, uint32_t it) {
+  QM31 a = f0;
+  f0 = qadd(a, f1);
+  f1 = qmulm(qsub(a, f1), it);
+}
+
+template <bool CIRCLE>
+__global__ void __launch_bounds__(LEAF_THREADS) k_fri_fold_commit(TwiddleView itv, uint32_t dst_log,
+                                                                   const uint32_t* __restrict__ src, uint64_t ss,
+                                                                   QM31 alpha, uint32_t* dst, uint64_t ds,
+                                                                   uint8_t* layers, Seeds seeds, uint32_t levels,
+                                                                   uint32_t one) {
+  __shared__ uint32_t sm[LEAF_THREADS * 8];
+  const uint64_t n = 1ull << dst_log;
+  const uint64_t i = (uint64_t)blockIdx.x * LEAF_THREADS + threadIdx.x;
+  if (i < n) {
+    uint2 w0 = *reinterpret_cast<const uint2*>(src + 2 * i);
+    uint2 w1 = *reinterpret_cast<const uint2*>(src + ss + 2 * i);
+    uint2 w2 = *reinterpret_cast<const uint2*>(src + 2 * ss + 2 * i);
+    uint2 w3 = *reinterpret_cast<const uint2*>(src + 3 * ss + 2 * i);
+    QM31 f0 = qmake(w0.x, w1.x, w2.x, w3.x), f1 = qmake(w0.y, w1.y, w2.y, w3.y);
+    fri_ibfly(f0, f1, CIRCLE ? itv.circ((uint32_t)i) : itv.line(1, (uint32_t)i));
+    QM31 r = CIRCLE ? qadd(qmul(alpha, f1), f0) : qadd(f0, qmul(alpha, f1));
+    dst[i] = r.c0.a; dst[ds + i] = r.c0.b; dst[2 * ds + i] = r.c1.a; dst[3 * ds + i] = r.c1.b;
+    if (layers) {
+      uint32_t h[8], m[16] = {r.c0.a, r.c0.b, r.c1.a, r.c1.b, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
+#pragma unroll
+      for (int k = 0; k < 8; ++k) h[k] = seeds.leaf[k];
+      b2s_compress(h, m, 80, true, one);
+      store_hash(layers, i, h);
+#pragma unroll
+      for (int k = 0; k < 8; ++k) sm[threadIdx.x * 8 + k] = h[k];
+    }
+  }
+  if (!layers) return;
+  __syncthreads();
+  uint32_t count = n < LEAF_THREADS ? (uint32_t)n : LEAF_THREADS;
+  fold_levels(sm, count, levels, layers, dst_log, dst_log, (uint64_t)blockIdx.x * LEAF_THREADS, seeds.node, one);
+}
+
 __global__ void k_empty_root(uint8_t* layers, Seeds seeds) {
   // No columns: the single leaf hashes the prefix block alone, as the final block.
   uint32_t h[8];
@@ -146,26 +191,19 @@ __global__ void k_empty_root(uint8_t* layers, Seeds seeds) {
 
 }  // namespace
 
-cudaError_t merkle_commit(uint32_t log_size, uint32_t n_cols, const uint32_t* cols, uint64_t stride,
-                          uint8_t* layers, cudaStream_t stream) {
+static const Seeds& seeds_once() {
   static const Seeds seeds = make_seeds();
-  if (n_cols == 0) {
-    k_empty_root<<<1, 1, 0, stream>>>(layers, seeds); note_launch();
-    return cudaGetLastError();
-  }
-  const uint64_t n_rows = 1ull << log_size;
-  // A tree that fits one CTA is folded to its root in the leaf launch; larger
-  // trees keep the leaf CTAs short (no fold) and fold layer by layer.
-  uint32_t leaf_levels = log_size <= LEAF_LEVELS ? log_size : 0;
-  uint32_t grid = (uint32_t)((n_rows + LEAF_THREADS - 1) / LEAF_THREADS);
-  k_merkle_leaves<<<grid, LEAF_THREADS, 0, stream>>>(log_size, n_cols, cols, stride, layers, seeds, leaf_levels, 1u); note_launch();
-  cudaError_t e = cudaGetLastError();
-  if (e != cudaSuccess) return e;
-  uint32_t child_log = log_size - leaf_levels;
+  return seeds;
+}
+
+// Folds the node layers above child layer `child_log` of a tree with 2^max_log leaves.
+static cudaError_t merkle_finish(uint8_t* layers, uint32_t max_log, uint32_t child_log, cudaStream_t stream) {
+  const Seeds& seeds = seeds_once();
+  cudaError_t e = cudaSuccess;
   while (child_log > NODE_FOLD_LOG) {
     uint32_t parent_log = child_log - 1;
     uint32_t blocks = (uint32_t)(((1ull << parent_log) + 255) / 256);
-    k_merkle_layer<<<blocks, 256, 0, stream>>>(layers, log_size, parent_log, seeds, 1u); note_launch();
+    k_merkle_layer<<<blocks, 256, 0, stream>>>(layers, max_log, parent_log, seeds, 1u); note_launch();
     e = cudaGetLastError();
     if (e != cudaSuccess) return e;
     child_log = parent_log;
@@ -175,12 +213,53 @@ cudaError_t merkle_commit(uint32_t log_size, uint32_t n_cols, const uint32_t* co
     uint64_t n_children = 1ull << child_log;
     uint32_t per_cta = n_children < 2 * NODE_THREADS ? (uint32_t)n_children : 2 * NODE_THREADS;
     uint32_t blocks = (uint32_t)(n_children / per_cta);
-    k_merkle_nodes<<<blocks, NODE_THREADS, 0, stream>>>(layers, log_size, child_log, levels, seeds, 1u); note_launch();
+    k_merkle_nodes<<<blocks, NODE_THREADS, 0, stream>>>(layers, max_log, child_log, levels, seeds, 1u); note_launch();
     e = cudaGetLastError();
     if (e != cudaSuccess) return e;
     child_log -= levels;
   }
   return cudaSuccess;
+}
+
+cudaError_t fri_fold_commit(const DeviceTables& t, bool circle, uint32_t src_log, const uint32_t* src,
+                            uint64_t src_stride, QM31 alpha, uint32_t* dst, uint64_t dst_stride, uint8_t* layers,
+                            cudaStream_t stream) {
+  const Seeds& seeds = seeds_once();
+  const uint32_t dst_log = src_log - 1;
+  const uint64_t n = 1ull << dst_log;
+  const uint32_t grid = (uint32_t)((n + LEAF_THREADS - 1) / LEAF_THREADS);
+  // One compression per leaf: the CTA also folds 8 node levels (node work equals
+  // leaf work here, and it saves the launches of the large layers).
+  const uint32_t levels = layers ? (dst_log < LEAF_LEVELS ? dst_log : LEAF_LEVELS) : 0;
+  if (circle)
+    k_fri_fold_commit<true><<<grid, LEAF_THREADS, 0, stream>>>(t.view(src_log, true), dst_log, src, src_stride, alpha,
+                                                               dst, dst_stride, layers, seeds, levels, 1u);
+  else
+    k_fri_fold_commit<false><<<grid, LEAF_THREADS, 0, stream>>>(t.view(src_log + 1, true), dst_log, src, src_stride,
+                                                                alpha, dst, dst_stride, layers, seeds, levels, 1u);
+  note_launch();
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess || !layers) return e;
+  return merkle_finish(layers, dst_log, dst_log - levels, stream);
+}
+
+cudaError_t merkle_commit(uint32_t log_size, uint32_t n_cols, const uint32_t* cols, uint64_t stride,
+                          uint8_t* layers, cudaStream_t stream) {
+  const Seeds& seeds = seeds_once();
+  if (n_cols == 0) {
+    k_empty_root<<<1, 1, 0, stream>>>(layers, seeds); note_launch();
+    return cudaGetLastError();
+  }
+  const uint64_t n_rows = 1ull << log_size;
+  // A tree that fits one CTA is folded to its root in the leaf launch. Trees of
+  // 4-word leaves (FRI-style, one compression each) also fold 8 levels per CTA;
+  // wider leaves keep the leaf CTAs short and fold layer by layer.
+  uint32_t leaf_levels = log_size <= LEAF_LEVELS ? log_size : (n_cols <= 4 ? LEAF_LEVELS : 0);
+  uint32_t grid = (uint32_t)((n_rows + LEAF_THREADS - 1) / LEAF_THREADS);
+  k_merkle_leaves<<<grid, LEAF_THREADS, 0, stream>>>(log_size, n_cols, cols, stride, layers, seeds, leaf_levels, 1u); note_launch();
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  return merkle_finish(layers, log_size, log_size - leaf_levels, stream);
 }
 
 // ---------------------------------------------------------------------------
@@ -230,7 +309,45 @@ __global__ void __launch_bounds__(256) k_pow(PowPrefix pre, uint32_t n_bits, uin
   }
 }
 
+// One bounded round of the search: nonces [base, base + grid*256*per_thread).
+// Rounds are enqueued in nonce order on one stream; a round starts by leaving
+// at once when an earlier round already found a smaller nonce, and each thread
+// stops at its first valid nonce or once the best known nonce is below its own.
+__global__ void __launch_bounds__(256) k_pow_round(PowPrefix pre, uint32_t n_bits, uint64_t base,
+                                                   uint32_t per_thread, unsigned long long* found, uint32_t one) {
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  uint64_t nonce = base + (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  unsigned long long best = *((volatile unsigned long long*)found);
+  for (uint32_t k = 0; k < per_thread && nonce < best; ++k, nonce += stride) {
+    uint32_t h[8];
+    b2s_init(h);
+    uint32_t m[16];
+#pragma unroll
+    for (int i = 0; i < 8; ++i) m[i] = pre.w[i];
+    m[8] = (uint32_t)nonce; m[9] = (uint32_t)(nonce >> 32);
+#pragma unroll
+    for (int i = 10; i < 16; ++i) m[i] = 0;
+    b2s_compress(h, m, 40, true, one);
+    if (ctz128(h[0], h[1], h[2], h[3]) >= n_bits) {
+      atomicMin(found, (unsigned long long)nonce);
+      return;
+    }
+    if ((k & 3) == 3) best = *((volatile unsigned long long*)found);
+  }
+}
+
 }  // namespace
+
+uint64_t pow_round_nonces(int sm_count) { return (uint64_t)sm_count * 4 * 256 * 112; }
+
+cudaError_t pow_round(const uint32_t prefix_words[8], uint32_t n_bits, uint64_t base, uint32_t* result_dev,
+                      int sm_count, cudaStream_t stream) {
+  PowPrefix pre;
+  for (int i = 0; i < 8; ++i) pre.w[i] = prefix_words[i];
+  k_pow_round<<<sm_count * 4, 256, 0, stream>>>(pre, n_bits, base, 112,
+                                               reinterpret_cast<unsigned long long*>(result_dev), 1u); note_launch();
+  return cudaGetLastError();
+}
 
 cudaError_t pow_grind(const uint32_t prefix_words[8], uint32_t n_bits, uint64_t max_nonce, uint32_t* result_dev,
                       cudaStream_t stream) {

@@ -443,18 +443,21 @@ int32_t WideFibProver::prove(const ProveRequest& req, std::string& out, StageTim
     fri_roots.push_back(r);
     ch.mix_root(r.data());
     QM31 alpha = ch.draw_secure_felt();
-    SB_CK(fold_circle_into_line(T, l.L, b.quot, l.NL, alpha, b.line[0], 1ull << (l.L - 1), false, s));
+    // Each fold writes the next line layer and, unless it is the last layer,
+    // commits it in the same launch sequence.
+    SB_CK(fri_fold_commit(T, true, l.L, b.quot, l.NL, alpha, b.line[0], 1ull << (l.L - 1),
+                          l.n_inner > 0 ? b.line_tree[0] : nullptr, s));
     for (uint32_t k = 0; k < l.n_inner; ++k) {
       uint32_t lg = l.L - 1 - k;
       size_t sz = 1ull << lg;
-      SB_CK(merkle_commit(lg, 4, b.line[k], sz, b.line_tree[k], s));
       SB_CK(cudaMemcpyAsync(pin, b.line_tree[k] + (2 * sz - 2) * 32, 32, cudaMemcpyDeviceToHost, s));
       SB_CK(sync());
       std::memcpy(r.data(), pin, 32);
       fri_roots.push_back(r);
       ch.mix_root(r.data());
       QM31 a = ch.draw_secure_felt();
-      SB_CK(fold_line(T, lg, b.line[k], sz, a, b.line[k + 1], sz / 2, s));
+      SB_CK(fri_fold_commit(T, false, lg, b.line[k], sz, a, b.line[k + 1], sz / 2,
+                            k + 1 < l.n_inner ? b.line_tree[k + 1] : nullptr, s));
     }
   }
   // Last layer: line IFFT of 2^last_log values (src/backend/line_evaluation.zig:97-145).
@@ -512,11 +515,18 @@ int32_t WideFibProver::prove(const ProveRequest& req, std::string& out, StageTim
     }
     uint32_t pw[8];
     std::memcpy(pw, prefix, 32);
-    uint64_t max_nonce = cfg.pow_bits >= 48 ? ~0ull : (1ull << (cfg.pow_bits + 16));
-    SB_CK(pow_grind(pw, cfg.pow_bits, max_nonce, b.pow_result, s));
-    SB_CK(cudaMemcpyAsync(pin, b.pow_result, 12, cudaMemcpyDeviceToHost, s));
-    SB_CK(sync());
-    std::memcpy(&nonce, pin, 8);
+    // Rounds of ~17M nonces, four per check; the search bound is 2^(bits+16) nonces.
+    const uint64_t max_nonce = cfg.pow_bits >= 48 ? ~0ull : (1ull << (cfg.pow_bits + 16));
+    const uint64_t per_round = pow_round_nonces(ctx_->sm_count);
+    SB_CK(cudaMemsetAsync(b.pow_result, 0xff, 8, s));
+    nonce = ~0ull;
+    for (uint64_t base = 0; base < max_nonce && nonce == ~0ull;) {
+      for (int r = 0; r < 4 && base < max_nonce; ++r, base += per_round)
+        SB_CK(pow_round(pw, cfg.pow_bits, base, b.pow_result, ctx_->sm_count, s));
+      SB_CK(cudaMemcpyAsync(pin, b.pow_result, 8, cudaMemcpyDeviceToHost, s));
+      SB_CK(sync());
+      std::memcpy(&nonce, pin, 8);
+    }
     if (nonce == ~0ull) return fail(E_TIMEOUT, "proof-of-work search bound reached");
   }
   ch.mix_u64(nonce);
