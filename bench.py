@@ -300,7 +300,7 @@ def main():
 
     # ---- INT32 rate of the proof-of-work grind (Blake2s, one compression per nonce)
     digest = bytes(range(32))
-    pow_bits = 24
+    pow_bits = 26
     ctx.pow_grind(digest, pow_bits)
     ev0.record(stream)
     nonce = ctx.pow_grind(digest, pow_bits)
@@ -327,10 +327,15 @@ def main():
                      "traffic": FFT_TRAFFIC_BYTES.get((args.log_n, args.width)),
                      "algorithmic_bytes": fft_bytes, "ms": fft_ms},
         "roofline_int32": {"kernel": "k_pow (Blake2s, 1 compression per nonce)", "hashes_per_s": hashes_per_s,
-                           "nonces": nonce + 1, "ms": pow_ms},
+                           "nonces": nonce + 1, "ms": pow_ms, "unit": "thread instructions/s",
+                           "achieved": hashes_per_s * POW_INSTR_PER_NONCE,
+                           "peak": 148 * 128 * 1e6 * (clocks.summary().get("sm_mhz") or 1965.0),
+                           "peak_source": "148 SMs x 128 lanes issue x sampled SM clock (nominal)"},
         "gpu_launches": launches,
         "clocks": clocks.summary(),
     }
+    ri = out["roofline_int32"]
+    ri["frac"] = ri["achieved"] / ri["peak"]
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         dt, ref = cpu_oracle_prove(args.log_n, args.width, args.preset, seeds[0])
         out["cpu_baseline"] = {"value": 1.0 / dt, "unit": "proofs/s", "cores": os.cpu_count() or 1, "kind": "port",
@@ -344,8 +349,13 @@ def main():
         dist.destroy_process_group()
 
 
-# DRAM bytes per launch-chain of the FFT pass, from ncu (profiles/fft_pass_*.md); None until captured.
-FFT_TRAFFIC_BYTES: dict = {}
+# DRAM bytes (read + write) of one FFT pass (the 3-kernel interpolate+extend chain) from one ncu
+# capture of 40 columns (profiles/fft_pass_20x40.md: 1531.5 MB), scaled to 100 columns; traffic is
+# linear in the column count.
+FFT_TRAFFIC_BYTES: dict = {(20, 100): 1531.5e6 * 100 / 40}
+# Thread instructions per nonce of the grind (profiles/pow_round_secure.md: 550.2 M warp
+# instructions x 32 / 16,973,824 nonces).
+POW_INSTR_PER_NONCE = 1037
 
 if __name__ == "__main__":
     main()

@@ -307,18 +307,16 @@ int32_t stwo_b200_pow_grind(stwo_b200_context* ctx, const uint8_t prefix_digest[
   CK_CTX(ctx);
   if (!prefix_digest || !nonce_out || n_bits > 64) return set_error(STWO_B200_E_INVALID, "bad pow arguments");
   if (n_bits == 0) { *nonce_out = 0; return STWO_B200_OK; }
+  std::lock_guard<std::mutex> g(ctx->ctx.small_mu);
   cudaStream_t s = ctx->ctx.stream;
-  void* res = nullptr;
-  cudaError_t e = cudaMallocAsync(&res, 16, s);
-  if (e != cudaSuccess) return cuda_status(e, "pow result");
+  uint32_t* res = ctx->ctx.small;
   uint32_t w[8];
   std::memcpy(w, prefix_digest, 32);
   uint64_t max_nonce = n_bits >= 48 ? ~0ull : (1ull << (n_bits + 16));
-  e = sb::pow_grind(w, n_bits, max_nonce, static_cast<uint32_t*>(res), s);
+  cudaError_t e = sb::pow_grind(w, n_bits, max_nonce, res, s);
   uint32_t host[3] = {0, 0, 0};
   if (e == cudaSuccess) e = cudaMemcpyAsync(host, res, 12, cudaMemcpyDeviceToHost, s);
   if (e == cudaSuccess) e = cudaStreamSynchronize(s);
-  cudaFreeAsync(res, s);
   if (e != cudaSuccess) return cuda_status(e, "pow_grind");
   uint64_t nonce = (uint64_t)host[0] | ((uint64_t)host[1] << 32);
   if (nonce == ~0ull) return set_error(STWO_B200_E_TIMEOUT, "proof-of-work search bound reached");

@@ -217,6 +217,7 @@ Context::~Context() {
   if (tables.points) cudaFree(tables.points);
   if (tables.tw) cudaFree(tables.tw);
   if (tables.itw) cudaFree(tables.itw);
+  if (small) cudaFree(small);
   if (stream) cudaStreamDestroy(stream);
 }
 
@@ -227,6 +228,14 @@ int32_t Context::init(int dev, uint32_t tower_log) {
   if (cudaSetDevice(dev) != cudaSuccess) return E_CUDA;
   cudaDeviceGetAttribute(&sm_count, cudaDevAttrMultiProcessorCount, dev);
   if (cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking) != cudaSuccess) return E_CUDA;
+  // Keep freed stream-ordered allocations cached in this process's default pool
+  // instead of returning them to the driver at every synchronization.
+  cudaMemPool_t pool;
+  if (cudaDeviceGetDefaultMemPool(&pool, dev) == cudaSuccess) {
+    uint64_t threshold = UINT64_MAX;
+    cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &threshold);
+  }
+  if (cudaMalloc(&small, 256) != cudaSuccess) return E_OOM;
   std::vector<PointM> pts = build_point_table();
   if (cudaMalloc(&tables.points, pts.size() * sizeof(PointM)) != cudaSuccess) return E_OOM;
   if (cudaMemcpy(tables.points, pts.data(), pts.size() * sizeof(PointM), cudaMemcpyHostToDevice) != cudaSuccess)

@@ -82,6 +82,8 @@ struct Context {
   std::mutex mu;
   std::vector<WideFibProver*> pool;  // idle provers
   cudaStream_t stream = nullptr;
+  uint32_t* small = nullptr;  // 256 bytes of device scratch for single-value results (PoW nonce)
+  std::mutex small_mu;
   ~Context();
   int32_t init(int device, uint32_t tower_log);
   WideFibProver* acquire();
