@@ -7,6 +7,7 @@ import numpy as np
 import pytest
 
 import oracle
+import verifier
 
 pytestmark = pytest.mark.gpu
 GOLDEN = os.path.join(os.path.dirname(__file__), "golden")
@@ -97,3 +98,12 @@ def test_repeat_determinism(ctx):
     a = ctx.prove_wide_fibonacci(sb.Statement(14, 32), g, trace_kind=1, trace_seed=1)
     b = ctx.prove_wide_fibonacci(sb.Statement(14, 32), g, trace_kind=1, trace_seed=1)
     assert a == b
+
+
+@pytest.mark.parametrize("log_n,W,preset", [(12, 100, "secure"), (16, 64, "functional")])
+def test_gpu_proofs_verify(ctx, log_n, W, preset):
+    import stwo_b200 as sb
+    _, g = cfg_pair(preset)
+    p = ctx.prove_wide_fibonacci(sb.Statement(log_n, W), g, trace_kind=sb.TRACE_SEEDED, trace_seed=42,
+                                 channel_seed=9)
+    assert verifier.verify_wide_fib(p, log_n, W, channel_seed=9)

@@ -8,6 +8,7 @@ import numpy as np
 import pytest
 
 import oracle
+import verifier
 
 GOLDEN = os.path.join(os.path.dirname(__file__), "golden")
 KATS = json.load(open(os.path.join(GOLDEN, "kats.json")))
@@ -102,3 +103,38 @@ def test_corrupted_trace_is_rejected():
     t[3, 5] ^= 1
     with pytest.raises(RuntimeError):
         oracle.prove_wide_fib(5, 8, oracle.config("smoke"), trace=t)
+
+
+def test_verifier_accepts_stored_reference_proof():
+    # The reference's own 2^10 x 8 functional proof, bytes from its benchmark bundle.
+    entry = next(e for e in STORED if "proof_hex" in e)
+    assert verifier.verify_wide_fib(bytes.fromhex(entry["proof_hex"]), entry["log_n_rows"], entry["sequence_len"])
+
+
+@pytest.mark.parametrize("preset,log_n,W,over", [("smoke", 5, 8, {}), ("secure", 8, 20, {}),
+                                                 ("functional", 9, 10, dict(log_blowup_factor=2, n_queries=5,
+                                                                            log_last_layer_degree_bound=1))])
+def test_verifier_accepts_oracle_proofs(preset, log_n, W, over):
+    p = oracle.prove_wide_fib(log_n, W, oracle.config(preset, **over), trace_kind=1, trace_seed=11, channel_seed=5)
+    assert verifier.verify_wide_fib(p, log_n, W, channel_seed=5)
+    with pytest.raises(verifier.VerificationError):
+        verifier.verify_wide_fib(p, log_n, W, channel_seed=6)
+
+
+@pytest.mark.parametrize("path", [
+    ("queried_values", 1, 3, 0), ("queried_values", 2, 7, 1), ("decommitments", 1, "hash_witness", 2, 5),
+    ("sampled_values", 1, 4, 0, 2), ("fri_proof", "first_layer", "fri_witness", 0, 1),
+    ("fri_proof", "inner_layers", 2, "decommitment", "hash_witness", 0, 0), ("fri_proof", "last_layer_poly", 0, 0),
+    ("commitments", 1, 0), ("proof_of_work",)])
+def test_verifier_rejects_tampering(path):
+    entry = next(e for e in STORED if "proof_hex" in e)
+    good = bytes.fromhex(entry["proof_hex"])
+    d = json.loads(good)
+    node = d
+    for k in path[:-1]:
+        node = node[k]
+    node[path[-1]] = (node[path[-1]] + 1) % (256 if path[0] in ("commitments", "decommitments") or
+                                             "hash_witness" in path else 2**31 - 1)
+    bad = json.dumps(d, separators=(",", ":")).encode()
+    with pytest.raises(verifier.VerificationError):
+        verifier.verify_wide_fib(bad, entry["log_n_rows"], entry["sequence_len"])
