@@ -350,11 +350,11 @@ def main():
 
 
 # DRAM bytes (read + write) of one FFT pass (the 3-kernel interpolate+extend chain) from one ncu
-# capture of 40 columns (profiles/fft_pass_20x40.md: 1531.5 MB), scaled to 100 columns; traffic is
-# linear in the column count.
+# capture of 2^20 rows x 40 columns (dram__bytes_read.sum + dram__bytes_write.sum = 1531.5 MB),
+# scaled to 100 columns; traffic is linear in the column count.
 FFT_TRAFFIC_BYTES: dict = {(20, 100): 1531.5e6 * 100 / 40}
-# Thread instructions per nonce of the grind (profiles/pow_round_secure.md: 550.2 M warp
-# instructions x 32 / 16,973,824 nonces).
+# Thread instructions per nonce of the grind (one ncu capture of a 26-bit round:
+# 550.2 M warp instructions x 32 / 16,973,824 nonces).
 POW_INSTR_PER_NONCE = 1037
 
 if __name__ == "__main__":

@@ -1,8 +1,8 @@
 /*
  * stwo_b200: C ABI of the B200 (sm_100a) backend for the stwo-zig circle-STARK
  * prover. A Zig backend type (or any FFI caller) binds these functions the way
- * src/backends/cuda/ffi.zig binds the stwo-cuda prototypes; INTEGRATION.md
- * shows the binding.
+ * src/backends/cuda/ffi.zig binds the stwo-cuda prototypes (an `extern fn`
+ * per entry point, slices passed as pointer + length).
  *
  * Conventions
  *  - Every function returns int32_t status: 0 = STWO_B200_OK, negative = error.
