@@ -10,6 +10,9 @@ goes through the C ABI with pinned host traces (host-to-device copy of every
 trace and device-to-host of every proof inside the timed region).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+    python bench.py --workload mixed48      # 48 mixed-shape proofs in one submission
+    python bench.py --workload serve [--rates 25,50,100,200] [--requests 64]
+                                            # Poisson arrivals into the serving loop
 
 N > 1 runs under torchrun as independent replicas (proofs do not shard): each
 rank proves its own K proofs; value = N*K / max over ranks of the timed region.
@@ -44,6 +47,10 @@ def parse():
     ap.add_argument("--preset", default="secure")
     ap.add_argument("--in-flight", type=int, default=IN_FLIGHT)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--workload", default="headline", choices=["headline", "mixed48", "serve"])
+    ap.add_argument("--rates", default="25,50,100,200")
+    ap.add_argument("--requests", type=int, default=64)
+    ap.add_argument("--slots", type=int, default=8)
     return ap.parse_args()
 
 
@@ -182,6 +189,13 @@ def main():
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
     ctx = sb.Context(local)
+    if args.workload != "headline":
+        if rank == 0:
+            (run_mixed48 if args.workload == "mixed48" else run_serve)(args, ctx)
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+        return
     cfg = sb.PcsConfig.preset(args.preset)
     st = sb.Statement(args.log_n, args.width)
     n_words = args.width << args.log_n
@@ -347,6 +361,129 @@ def main():
     if world > 1:
         import torch.distributed as dist
         dist.destroy_process_group()
+
+
+def mixed_statements(master_seed: int, count: int, log_lo: int, log_hi: int):
+    """Statements drawn from one master seed: log_n_rows uniform in [log_lo, log_hi], sequence_len
+    uniform in {16, 32, 100}, a trace seed and a channel seed each, and a Poisson gap (1/s units)."""
+    import numpy as np
+    rng = np.random.default_rng(master_seed)
+    out = []
+    for _ in range(count):
+        out.append(dict(log_n=int(rng.integers(log_lo, log_hi + 1)), W=int(rng.choice([16, 32, 100])),
+                        trace_seed=int(rng.integers(1, 2**62)), channel_seed=int(rng.integers(0, 2**62)),
+                        u=float(rng.exponential(1.0))))
+    return out
+
+
+def run_mixed48(args, ctx):
+    """48 independent proofs (log_n_rows 14..20, sequence_len {16, 32, 100}) in one submission, against
+    the same 48 proved one at a time; every batched proof must equal its single run."""
+    import torch
+    import stwo_b200 as sb
+    cfg = sb.PcsConfig.preset(args.preset)
+    stmts = mixed_statements(2026, 48, 14, 20)
+    reqs = [dict(statement=sb.Statement(r["log_n"], r["W"]), config=cfg, trace_kind=sb.TRACE_SEEDED,
+                 trace_seed=r["trace_seed"], channel_seed=r["channel_seed"]) for r in stmts]
+    ctx.prove_wide_fibonacci_batch(reqs[:16], max_in_flight=args.in_flight)  # warm-up: every workspace size
+    torch.cuda.synchronize()
+    launches0 = sb.kernel_launches()
+    with ClockSampler(0) as clocks:
+        t0 = time.perf_counter()
+        batch, times = ctx.prove_wide_fibonacci_batch(reqs, max_in_flight=args.in_flight, with_times=True)
+        batched_s = time.perf_counter() - t0
+    launches = sb.kernel_launches() - launches0
+    lat, single = [], []
+    t0 = time.perf_counter()
+    for r in reqs:
+        a = time.perf_counter()
+        single.append(ctx.prove_wide_fibonacci(r["statement"], cfg, trace_kind=sb.TRACE_SEEDED,
+                                               trace_seed=r["trace_seed"], channel_seed=r["channel_seed"]))
+        lat.append(1e3 * (time.perf_counter() - a))
+    single_s = time.perf_counter() - t0
+    identical = all(x == y for x, y in zip(batch, single))
+    cells = sum(r["W"] << r["log_n"] for r in stmts)
+    out = {"metric": "proofs/s, 48 mixed wide-Fibonacci proofs in one submission", "workload": "mixed48",
+           "value": 48 / batched_s, "unit": "proofs/s", "n_gpus": 1, "higher_is_better": True,
+           "dtype": "u32", "data": "synthetic: seeded traces, master seed 2026",
+           "config": {"workload": "48 wide-Fibonacci proofs, log_n_rows uniform 14..20, sequence_len in "
+                                  "{16, 32, 100}, own trace and channel seeds", "protocol": args.preset,
+                      "in_flight": args.in_flight, "trace_cells": cells},
+           "batched": {"proofs_per_s": 48 / batched_s, "wall_ms": 1e3 * batched_s,
+                       "p50_ms": pct([t["total"] for t in times], 50), "p99_ms": pct([t["total"] for t in times], 99)},
+           "single": {"proofs_per_s": 48 / single_s, "wall_ms": 1e3 * single_s, "p50_ms": pct(lat, 50),
+                      "p99_ms": pct(lat, 99)},
+           "batched_over_single": single_s / batched_s, "byte_identical_to_single": identical,
+           "gpu_launches": launches, "clocks": clocks.summary()}
+    print(json.dumps(out), flush=True)
+
+
+def run_serve(args, ctx):
+    """Poisson arrivals (seeded) of wide-Fibonacci requests (log_n_rows 12..22, sequence_len
+    {16, 32, 100}) into the serving loop at each rate; latency = submit to proof bytes. The same
+    requests proved one at a time give the single-proof throughput they are compared with."""
+    import torch
+    import stwo_b200 as sb
+    cfg = sb.PcsConfig.preset(args.preset)
+    rates = [float(x) for x in args.rates.split(",")]
+    results = []
+    stmts = mixed_statements(4242, args.requests, 12, 22)
+    # single-proof path over the same requests
+    for r in stmts[:4]:
+        ctx.prove_wide_fibonacci(sb.Statement(r["log_n"], r["W"]), cfg, trace_kind=sb.TRACE_SEEDED,
+                                 trace_seed=r["trace_seed"], channel_seed=r["channel_seed"])
+    t0 = time.perf_counter()
+    alone = []
+    for r in stmts:
+        alone.append(ctx.prove_wide_fibonacci(sb.Statement(r["log_n"], r["W"]), cfg, trace_kind=sb.TRACE_SEEDED,
+                                              trace_seed=r["trace_seed"], channel_seed=r["channel_seed"]))
+    single_s = time.perf_counter() - t0
+    for rate in rates:
+        with sb.Server(ctx, slots=args.slots, profile=2) as srv:
+            for r in stmts[:args.slots]:  # warm the stream-ordered pool
+                srv.wait(srv.submit(sb.Statement(r["log_n"], r["W"]), cfg, trace_kind=sb.TRACE_SEEDED,
+                                    trace_seed=r["trace_seed"], channel_seed=r["channel_seed"]))
+            tickets, submit_t = [None] * len(stmts), [0.0] * len(stmts)
+
+            def producer():
+                start = time.perf_counter()
+                at = 0.0
+                for i, r in enumerate(stmts):
+                    at += r["u"] / rate
+                    delay = start + at - time.perf_counter()
+                    if delay > 0:
+                        time.sleep(delay)
+                    submit_t[i] = time.perf_counter()
+                    tickets[i] = srv.submit(sb.Statement(r["log_n"], r["W"]), cfg, trace_kind=sb.TRACE_SEEDED,
+                                            trace_seed=r["trace_seed"], channel_seed=r["channel_seed"])
+            th = threading.Thread(target=producer)
+            t_begin = time.perf_counter()
+            th.start()
+            lat, done_t, same = [], [], True
+            for i in range(len(stmts)):
+                while tickets[i] is None:
+                    time.sleep(0.0005)
+                proof, st = srv.wait(tickets[i])
+                done_t.append(time.perf_counter())
+                lat.append(st["queued_ms"] + st["run_ms"])
+                same &= proof == alone[i]
+            th.join()
+            snap = srv.snapshot()
+        span = max(done_t) - t_begin
+        results.append({"rate_req_s": rate, "proofs_per_s": len(stmts) / span, "p50_ms": pct(lat, 50),
+                        "p99_ms": pct(lat, 99), "peak_in_flight": snap["peak_in_flight"],
+                        "peak_workspace_gb": snap["peak_workspace_bytes"] / 1e9, "identical_to_single": same})
+    best = max(x["proofs_per_s"] for x in results)
+    out = {"metric": "proofs/s and p50/p99 ms, serving loop under Poisson arrivals", "workload": "serve",
+           "value": best, "unit": "proofs/s", "n_gpus": 1, "higher_is_better": True, "dtype": "u32",
+           "data": "synthetic: seeded traces, master seed 4242",
+           "config": {"workload": f"{len(stmts)} wide-Fibonacci requests, log_n_rows uniform 12..22, sequence_len "
+                                  "in {16, 32, 100}, Poisson arrivals", "protocol": args.preset,
+                      "slots": args.slots, "profile": "extreme"},
+           "rates": results,
+           "single": {"proofs_per_s": len(stmts) / single_s, "wall_ms": 1e3 * single_s},
+           "serving_over_single": best / (len(stmts) / single_s)}
+    print(json.dumps(out), flush=True)
 
 
 # DRAM bytes (read + write) of one FFT pass (the 3-kernel interpolate+extend chain) from one ncu

@@ -41,6 +41,8 @@ extern "C" {
 #define STWO_B200_E_BUFFER_TOO_SMALL (-6)
 #define STWO_B200_E_FALLBACK (-7)
 #define STWO_B200_E_NO_DEVICE (-8)
+#define STWO_B200_E_DIVISION_BY_ZERO (-9) /* Error.DivisionByZero / ZeroDenominator of the reference */
+#define STWO_B200_E_REJECTED (-10)         /* admission refused (CommittedCellBudgetExceeded, memory budget) */
 
 typedef struct stwo_b200_context stwo_b200_context;
 
@@ -115,6 +117,51 @@ int32_t stwo_b200_prove_wide_fibonacci_batch(stwo_b200_context* ctx, const stwo_
                                              size_t n, uint8_t* const* proof_outs, const size_t* proof_caps,
                                              size_t* proof_lens, int32_t* statuses, uint32_t max_in_flight,
                                              stwo_b200_stage_times* times);
+
+/* ---- Serving loop ------------------------------------------------------------------------------- */
+
+/* Continuous batching of wide-Fibonacci proofs on one device: `slots` proofs in flight (each a host
+ * thread and a stream), admitted first-in first-out as a slot is free and the in-flight device
+ * workspace stays within memory_budget bytes (0 = 80% of the device memory free at creation). Each
+ * request must also pass the reference's resource-profile admission (profile 0 standard, 1 large,
+ * 2 extreme; 16 accounted bytes per committed cell, src/prover/native/resource_admission.zig:5-19,
+ * :147-161), else submit returns STWO_B200_E_REJECTED. Proof bytes equal those of
+ * stwo_b200_prove_wide_fibonacci for the same request. The reference has no serving loop; the
+ * admission limits are its resource profiles. */
+typedef struct stwo_b200_server stwo_b200_server;
+#define STWO_B200_SERVER_PERSISTENT_WORKSPACES 1u /* slots keep their workspace between proofs (counted
+                                                  * against the budget while held) instead of taking it
+                                                  * from the stream-ordered pool per proof */
+typedef struct {
+  uint32_t slots;
+  uint32_t profile;
+  uint64_t memory_budget;
+  uint32_t flags;
+} stwo_b200_server_config;
+typedef struct {
+  uint64_t accounted_bytes; /* 16 B per committed cell */
+  uint64_t workspace_bytes; /* device workspace the proof used */
+  double queued_ms;         /* submit -> admitted (host steady clock) */
+  double run_ms;            /* admitted -> proof bytes */
+  uint32_t slot;
+  stwo_b200_stage_times stages;
+} stwo_b200_request_stats;
+typedef struct {
+  uint64_t submitted, completed, failed, rejected;
+  uint64_t peak_in_flight, peak_workspace_bytes, budget_bytes;
+} stwo_b200_server_snapshot;
+
+int32_t stwo_b200_server_create(stwo_b200_context* ctx, const stwo_b200_server_config* cfg,
+                                stwo_b200_server** out);
+/* Queues a request and returns at once; host/device trace buffers must stay valid until wait returns. */
+int32_t stwo_b200_server_submit(stwo_b200_server* server, const stwo_b200_wide_fib_request* req, uint64_t* ticket);
+/* Blocks until the request is done and returns its status; STWO_B200_E_BUFFER_TOO_SMALL sets
+ * *proof_len and keeps the result for another call. */
+int32_t stwo_b200_server_wait(stwo_b200_server* server, uint64_t ticket, uint8_t* proof_out, size_t proof_cap,
+                              size_t* proof_len, stwo_b200_request_stats* stats);
+int32_t stwo_b200_server_snapshot_get(stwo_b200_server* server, stwo_b200_server_snapshot* out);
+/* Finishes every queued and running request, then releases the slots. */
+int32_t stwo_b200_server_destroy(stwo_b200_server* server);
 
 /* ---- PolyOps (src/backend/poly_ops.zig:12-24) --------------------------------------------------- */
 
@@ -211,6 +258,45 @@ int32_t stwo_b200_wide_fib_composition(stwo_b200_context* ctx, uint32_t log_n_ro
                                        const uint32_t* eval, uint64_t stride, const stwo_b200_qm31* coeffs_dev,
                                        uint32_t den_inv0, uint32_t den_inv1, uint32_t* out, uint64_t out_stride,
                                        void* stream);
+
+/* ---- FieldOps (src/backend/field_ops.zig:9-15) -------------------------------------------------- */
+
+/* Montgomery batch inverse of n elements of `degree` 1 (M31), 2 (CM31) or 4 (QM31); an element is
+ * `degree` coordinate columns (column k at base + k * stride). dst may alias src. Synchronous: returns
+ * STWO_B200_E_DIVISION_BY_ZERO when an element is zero, as batchInverse does (dst is then
+ * unspecified). Replaces batchInverse (src/core/fields/mod.zig:164-200). */
+int32_t stwo_b200_batch_inverse(stwo_b200_context* ctx, uint32_t degree, uint64_t n, const uint32_t* src,
+                                uint64_t src_stride, uint32_t* dst, uint64_t dst_stride, void* stream);
+
+/* ---- LogUp interaction columns ------------------------------------------------------------------- */
+
+/* One use of a relation at every row: denominator = sum_j alphas[j] * word_j(row) - z, numerator =
+ * multiplicity(row) (1 when NULL), negated when `negate`. words[j] is a device M31 column of
+ * 2^log_rows rows, or NULL for the constant constants[j] (relation_combine / relation_multiplicity,
+ * src/backends/metal/shaders/core/relation.metal:54-90). */
+#define STWO_B200_LOGUP_MAX_WORDS 8
+#define STWO_B200_LOGUP_MAX_USES 32
+typedef struct {
+  uint32_t n_words;
+  uint32_t negate;
+  const uint32_t* words[STWO_B200_LOGUP_MAX_WORDS];
+  uint32_t constants[STWO_B200_LOGUP_MAX_WORDS];
+  const uint32_t* multiplicity;
+} stwo_b200_logup_use;
+
+/* Interaction columns of n_uses uses (host array), `batch` (1 or 2) uses per column: a column of two
+ * uses is (n_a d_b + n_b d_a) / (d_a d_b). Column c (4 coordinate columns at out + (4c + k) * out_stride)
+ * holds per row the running sum of the row's fractions over columns 0..c; the last column is then the
+ * cumulative sum over rows: order 1 visits rows in coset order (scan index s -> circle index s/2 or
+ * N-1-s/2, stored at its bit reverse) and subtracts total (s+1)/N (relation.metal:160-237, law of
+ * src/tests/metal/backend/commitment_test.zig:73-154); order 0 sums in storage order without shift
+ * (cumulativeColumn, src/frontends/riscv/air/logup.zig:83-105). claimed_host receives the total.
+ * alphas: host array of max n_words QM31. Synchronous; STWO_B200_E_DIVISION_BY_ZERO when a
+ * denominator is zero. */
+int32_t stwo_b200_logup_interaction(stwo_b200_context* ctx, uint32_t log_rows, uint32_t n_uses,
+                                    const stwo_b200_logup_use* uses, const stwo_b200_qm31* alphas,
+                                    stwo_b200_qm31 z, uint32_t batch, uint32_t order, uint32_t* out,
+                                    uint64_t out_stride, stwo_b200_qm31* claimed_host, void* stream);
 
 /* ---- Channel proof of work ---------------------------------------------------------------------- */
 

@@ -1032,6 +1032,28 @@ std::string prove_wide_fib(const ProveParams& pp, const uint32_t* trace) {
 // ---------------------------------------------------------------------------
 // C entry points.
 // ---------------------------------------------------------------------------
+// Montgomery batch inversion, batchInverseClassic (src/core/fields/mod.zig:178-200): prefix products,
+// one inversion of the total, backward pass. Returns -2 (DivisionByZero) when an element is zero.
+template <class F, class Mul, class Inv, class IsZero>
+int batch_inverse_classic(std::vector<F>& col, Mul mul, Inv inv, IsZero is_zero) {
+  size_t n = col.size();
+  if (n == 0) return 0;
+  std::vector<F> dst(n);
+  dst[0] = col[0];
+  for (size_t i = 1; i < n; ++i) dst[i] = mul(dst[i - 1], col[i]);
+  if (is_zero(dst[n - 1])) return -2;
+  F cur = inv(dst[n - 1]);
+  for (size_t i = n; i-- > 1;) {
+    dst[i] = mul(dst[i - 1], cur);
+    cur = mul(cur, col[i]);
+  }
+  dst[0] = cur;
+  col.swap(dst);
+  return 0;
+}
+
+QM31 qinv_oracle(QM31 x) { return qinv(x); }
+
 extern "C" {
 
 int oracle_gen_trace(uint32_t log_n_rows, uint32_t sequence_len, int trace_kind, uint64_t seed, uint32_t* out) {
@@ -1157,6 +1179,107 @@ int oracle_blake2s(const uint8_t* data, size_t len, uint8_t out[32]) {
 int oracle_pow_grind(const uint8_t digest[32], uint32_t n_bits, int n_threads, uint64_t* nonce) {
   Hash d; std::memcpy(d.data(), digest, 32);
   *nonce = pow_grind(d, n_bits, n_threads);
+  return 0;
+}
+
+int oracle_batch_inverse(uint32_t degree, uint64_t n, const uint32_t* src, uint32_t* dst) {
+  if (degree == 1) {
+    std::vector<uint32_t> v(src, src + n);
+    int r = batch_inverse_classic(v, mmul, minv, [](uint32_t a) { return a == 0; });
+    if (r == 0) std::copy(v.begin(), v.end(), dst);
+    return r;
+  }
+  if (degree == 2) {
+    std::vector<CM31> v(n);
+    for (uint64_t i = 0; i < n; ++i) v[i] = {src[i], src[n + i]};
+    int r = batch_inverse_classic(v, cmul, cinv, czero);
+    if (r == 0)
+      for (uint64_t i = 0; i < n; ++i) { dst[i] = v[i].a; dst[n + i] = v[i].b; }
+    return r;
+  }
+  if (degree == 4) {
+    std::vector<QM31> v(n);
+    for (uint64_t i = 0; i < n; ++i) v[i] = qfrom(src[i], src[n + i], src[2 * n + i], src[3 * n + i]);
+    int r = batch_inverse_classic(v, qmul, qinv_oracle, qiszero);
+    if (r == 0)
+      for (uint64_t i = 0; i < n; ++i) {
+        uint32_t w[4]; qstore(v[i], w);
+        for (int k = 0; k < 4; ++k) dst[k * n + i] = w[k];
+      }
+    return r;
+  }
+  return -1;
+}
+
+// LogUp interaction columns. Fractions per use: relation_combine / relation_multiplicity
+// (src/backends/metal/shaders/core/relation.metal:54-90): denominator = sum_j alpha_j word_j - z,
+// numerator = +/- multiplicity; a column of two uses is (n_a d_b + n_b d_a) / (d_a d_b)
+// (relation.metal:77-90). Column c holds the running sum over columns 0..c of the row's fractions
+// (stwo_zig_relation_fused, relation.metal:131-158). The last column is then summed over rows:
+// order 1 in coset order with the total/N shift, the scalar law of
+// src/tests/metal/backend/commitment_test.zig:140-152; order 0 in storage order without shift
+// (cumulativeColumn, src/frontends/riscv/air/logup.zig:83-105).
+int oracle_logup_interaction(uint32_t log_rows, uint32_t n_uses, const oracle_logup_use* uses,
+                             const uint32_t* alphas, const uint32_t z_in[4], uint32_t batch, uint32_t order,
+                             uint32_t* out, uint32_t claimed_out[4]) {
+  if (log_rows > 24 || n_uses == 0 || (batch != 1 && batch != 2) || order > 1) return -1;
+  const size_t rows = (size_t)1 << log_rows;
+  const uint32_t n_cols = (n_uses + batch - 1) / batch;
+  const QM31 z = qload(z_in);
+  auto den = [&](const oracle_logup_use& u, size_t r) {
+    QM31 acc = qneg(z);
+    for (uint32_t j = 0; j < u.n_words; ++j) {
+      uint32_t w = u.words[j] ? u.words[j][r] : u.constants[j];
+      acc = qadd(acc, qmulm(qload(alphas + 4 * j), w));
+    }
+    return acc;
+  };
+  auto num = [&](const oracle_logup_use& u, size_t r) {
+    uint32_t m = u.multiplicity ? u.multiplicity[r] : 1u;
+    return u.negate ? mneg(m) : m;
+  };
+  std::vector<QM31> last(rows);
+  for (size_t r = 0; r < rows; ++r) {
+    QM31 acc = qzero();
+    for (uint32_t c = 0; c < n_cols; ++c) {
+      uint32_t u0 = c * batch;
+      QM31 n, d;
+      if (batch == 2 && u0 + 1 < n_uses) {
+        QM31 da = den(uses[u0], r), db = den(uses[u0 + 1], r);
+        n = qadd(qmulm(da, num(uses[u0 + 1], r)), qmulm(db, num(uses[u0], r)));
+        d = qmul(da, db);
+      } else {
+        n = qbase(num(uses[u0], r));
+        d = den(uses[u0], r);
+      }
+      if (qiszero(d)) return -2;
+      acc = qadd(acc, qmul(n, qinv(d)));
+      uint32_t w[4]; qstore(acc, w);
+      for (int k = 0; k < 4; ++k) out[(4 * (size_t)c + k) * rows + r] = w[k];
+    }
+    last[r] = acc;
+  }
+  QM31 total = qzero();
+  for (size_t r = 0; r < rows; ++r) total = qadd(total, last[r]);
+  uint32_t* lc = out + 4 * (size_t)(n_cols - 1) * rows;
+  QM31 acc = qzero();
+  if (order == 0) {
+    for (size_t r = 0; r < rows; ++r) {
+      acc = qadd(acc, last[r]);
+      uint32_t w[4]; qstore(acc, w);
+      for (int k = 0; k < 4; ++k) lc[k * rows + r] = w[k];
+    }
+  } else {
+    QM31 shift = qmulm(total, minv((uint32_t)(rows % P)));
+    for (size_t s = 0; s < rows; ++s) {
+      size_t ci = (s & 1) == 0 ? s / 2 : rows - 1 - s / 2;
+      size_t r = bit_reverse_index(ci, log_rows);
+      acc = qadd(acc, qsub(last[r], shift));
+      uint32_t w[4]; qstore(acc, w);
+      for (int k = 0; k < 4; ++k) lc[k * rows + r] = w[k];
+    }
+  }
+  qstore(total, claimed_out);
   return 0;
 }
 

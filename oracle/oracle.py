@@ -181,3 +181,65 @@ def pow_grind(digest: bytes, n_bits: int, n_threads: int = 0) -> int:
     nonce = ctypes.c_uint64(0)
     assert lib().oracle_pow_grind(digest, n_bits, n_threads or (os.cpu_count() or 1), ctypes.byref(nonce)) == 0
     return nonce.value
+
+
+class DivisionByZero(ArithmeticError):
+    """The reference's Error.DivisionByZero / error.ZeroDenominator."""
+
+
+def batch_inverse(values: np.ndarray) -> np.ndarray:
+    """values: (n,) M31, or (degree, n) coordinate planes with degree 2 (CM31) or 4 (QM31)."""
+    v = np.ascontiguousarray(values, dtype=np.uint32)
+    degree, n = (1, v.size) if v.ndim == 1 else (v.shape[0], v.shape[1])
+    out = np.empty_like(v)
+    r = lib().oracle_batch_inverse(degree, n, _u32p(v), _u32p(out))
+    if r == -2:
+        raise DivisionByZero("batch_inverse: zero element")
+    assert r == 0
+    return out
+
+
+class LogupUse(ctypes.Structure):
+    _fields_ = [
+        ("n_words", ctypes.c_uint32),
+        ("negate", ctypes.c_uint32),
+        ("words", ctypes.POINTER(ctypes.c_uint32) * 8),
+        ("constants", ctypes.c_uint32 * 8),
+        ("multiplicity", ctypes.POINTER(ctypes.c_uint32)),
+    ]
+
+
+def logup_interaction(log_rows: int, uses: list[dict], alphas, z, batch: int = 1, order: int = 1):
+    """uses: dicts with "words" (each a uint32 column of 2^log_rows or an int constant), optional
+    "multiplicity" (uint32 column) and "negate". Returns (columns (n_cols, 4, rows), claimed (4,))."""
+    keep, structs = [], (LogupUse * len(uses))()
+    for u, d in zip(structs, uses):
+        u.n_words = len(d["words"])
+        u.negate = int(bool(d.get("negate", False)))
+        for j, w in enumerate(d["words"]):
+            if isinstance(w, (int, np.integer)):
+                u.constants[j] = int(w)
+            else:
+                a = np.ascontiguousarray(w, dtype=np.uint32)
+                keep.append(a)
+                u.words[j] = _u32p(a)
+        if d.get("multiplicity") is not None:
+            m = np.ascontiguousarray(d["multiplicity"], dtype=np.uint32)
+            keep.append(m)
+            u.multiplicity = _u32p(m)
+    n_cols = (len(uses) + batch - 1) // batch
+    rows = 1 << log_rows
+    out = np.empty((n_cols, 4, rows), dtype=np.uint32)
+    claimed = np.empty(4, dtype=np.uint32)
+    al = np.ascontiguousarray(np.array(alphas, dtype=np.uint32).reshape(-1, 4))
+    zz = np.array(z, dtype=np.uint32)
+    lib().oracle_logup_interaction.argtypes = [
+        ctypes.c_uint32, ctypes.c_uint32, ctypes.POINTER(LogupUse), ctypes.POINTER(ctypes.c_uint32),
+        ctypes.POINTER(ctypes.c_uint32), ctypes.c_uint32, ctypes.c_uint32, ctypes.POINTER(ctypes.c_uint32),
+        ctypes.POINTER(ctypes.c_uint32)]
+    r = lib().oracle_logup_interaction(log_rows, len(uses), structs, _u32p(al), _u32p(zz), batch, order,
+                                       _u32p(out), _u32p(claimed))
+    if r == -2:
+        raise DivisionByZero("logup_interaction: zero denominator")
+    assert r == 0
+    return out, claimed

@@ -61,6 +61,24 @@ int oracle_eval_at_point(uint32_t log_size, const uint32_t* coeffs, const uint32
 int oracle_blake2s(const uint8_t* data, size_t len, uint8_t out[32]);
 int oracle_pow_grind(const uint8_t digest[32], uint32_t n_bits, int n_threads, uint64_t* nonce);
 
+/* Batch inverse of n elements of degree 1, 2 or 4 (degree coordinate planes of n words).
+ * Returns -2 when an element is zero. */
+int oracle_batch_inverse(uint32_t degree, uint64_t n, const uint32_t* src, uint32_t* dst);
+
+/* One LogUp use (host columns of 2^log_rows words; NULL word = constant, NULL multiplicity = 1). */
+typedef struct {
+  uint32_t n_words;
+  uint32_t negate;
+  const uint32_t* words[8];
+  uint32_t constants[8];
+  const uint32_t* multiplicity;
+} oracle_logup_use;
+/* Interaction columns (4 planes per column, 2^log_rows words each) and the claimed sum.
+ * alphas: n_words x 4 words. Returns -2 on a zero denominator. */
+int oracle_logup_interaction(uint32_t log_rows, uint32_t n_uses, const oracle_logup_use* uses,
+                             const uint32_t* alphas, const uint32_t z[4], uint32_t batch, uint32_t order,
+                             uint32_t* out, uint32_t claimed[4]);
+
 #ifdef __cplusplus
 }
 #endif

@@ -1,4 +1,5 @@
 // C ABI of libstwo_b200 (declarations and reference citations: include/stwo_b200.h).
+#include <algorithm>
 #include <atomic>
 #include <cstring>
 #include <string>
@@ -8,6 +9,7 @@
 #include "../../include/stwo_b200.h"
 #include "context.hpp"
 #include "prover.hpp"
+#include "server.hpp"
 
 namespace sb {
 static std::atomic<uint64_t> g_launches(0);
@@ -321,6 +323,155 @@ int32_t stwo_b200_pow_grind(stwo_b200_context* ctx, const uint8_t prefix_digest[
   uint64_t nonce = (uint64_t)host[0] | ((uint64_t)host[1] << 32);
   if (nonce == ~0ull) return set_error(STWO_B200_E_TIMEOUT, "proof-of-work search bound reached");
   *nonce_out = nonce;
+  return STWO_B200_OK;
+}
+
+struct stwo_b200_server {
+  sb::Server* server;
+  stwo_b200_context* ctx;
+};
+
+int32_t stwo_b200_server_create(stwo_b200_context* ctx, const stwo_b200_server_config* cfg,
+                                stwo_b200_server** out) {
+  CK_CTX(ctx);
+  if (!cfg || !out || cfg->profile > 2 || cfg->slots > 64 || cfg->flags > 1)
+    return set_error(STWO_B200_E_INVALID, "bad server config");
+  uint64_t budget = cfg->memory_budget;
+  if (budget == 0) {
+    size_t free_b = 0, total_b = 0;
+    cudaError_t e = cudaMemGetInfo(&free_b, &total_b);
+    if (e != cudaSuccess) return cuda_status(e, "cudaMemGetInfo");
+    budget = free_b / 10 * 8;
+  }
+  auto* s = new stwo_b200_server{new sb::Server(&ctx->ctx, cfg->slots ? cfg->slots : 8, budget, cfg->profile, cfg->flags),
+                                ctx};
+  int32_t rc = s->server->start();
+  if (rc != STWO_B200_OK) {
+    delete s->server;
+    delete s;
+    return set_error(rc, "server start failed");
+  }
+  *out = s;
+  return STWO_B200_OK;
+}
+
+int32_t stwo_b200_server_submit(stwo_b200_server* server, const stwo_b200_wide_fib_request* req, uint64_t* ticket) {
+  if (!server || !req || !ticket) return set_error(STWO_B200_E_INVALID, "null server argument");
+  std::string err;
+  int32_t rc = server->server->submit(to_request(*req), ticket, &err);
+  return rc == STWO_B200_OK ? rc : set_error(rc, err);
+}
+
+int32_t stwo_b200_server_wait(stwo_b200_server* server, uint64_t ticket, uint8_t* proof_out, size_t proof_cap,
+                              size_t* proof_len, stwo_b200_request_stats* stats) {
+  if (!server) return set_error(STWO_B200_E_INVALID, "null server");
+  std::string err;
+  sb::RequestStats st;
+  int32_t rc = server->server->wait(ticket, proof_out, proof_cap, proof_len, &st, &err);
+  if (stats) {
+    stats->accounted_bytes = st.accounted_bytes;
+    stats->workspace_bytes = st.workspace_bytes;
+    stats->queued_ms = st.queued_ms;
+    stats->run_ms = st.run_ms;
+    stats->slot = st.slot;
+    static_assert(sizeof(stats->stages) == sizeof(st.stages), "stage times layout");
+    std::memcpy(&stats->stages, &st.stages, sizeof(st.stages));
+  }
+  return rc == STWO_B200_OK ? rc : set_error(rc, err);
+}
+
+int32_t stwo_b200_server_snapshot_get(stwo_b200_server* server, stwo_b200_server_snapshot* out) {
+  if (!server || !out) return set_error(STWO_B200_E_INVALID, "null server argument");
+  sb::ServerSnapshot s = server->server->snapshot();
+  out->submitted = s.submitted;
+  out->completed = s.completed;
+  out->failed = s.failed;
+  out->rejected = s.rejected;
+  out->peak_in_flight = s.peak_in_flight;
+  out->peak_workspace_bytes = s.peak_workspace_bytes;
+  out->budget_bytes = s.budget_bytes;
+  return STWO_B200_OK;
+}
+
+int32_t stwo_b200_server_destroy(stwo_b200_server* server) {
+  if (!server) return STWO_B200_OK;
+  cudaSetDevice(server->ctx->ctx.device);
+  delete server->server;
+  delete server;
+  return STWO_B200_OK;
+}
+
+int32_t stwo_b200_batch_inverse(stwo_b200_context* ctx, uint32_t degree, uint64_t n, const uint32_t* src,
+                                uint64_t src_stride, uint32_t* dst, uint64_t dst_stride, void* stream) {
+  CK_CTX(ctx);
+  if ((degree != 1 && degree != 2 && degree != 4) || (n && (!src || !dst)) || n > (1ull << 32) ||
+      (degree > 1 && (src_stride < n || dst_stride < n)))
+    return set_error(STWO_B200_E_INVALID, "bad batch_inverse arguments");
+  if (n == 0) return STWO_B200_OK;
+  std::lock_guard<std::mutex> g(ctx->ctx.small_mu);
+  uint32_t* flag = ctx->ctx.small;
+  cudaStream_t s = st(stream);
+  cudaError_t e = cudaMemsetAsync(flag, 0, 4, s);
+  if (e == cudaSuccess) e = sb::batch_inverse(degree, n, src, src_stride, dst, dst_stride, flag, s);
+  uint32_t host = 0;
+  if (e == cudaSuccess) e = cudaMemcpyAsync(&host, flag, 4, cudaMemcpyDeviceToHost, s);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  if (e != cudaSuccess) return cuda_status(e, "batch_inverse");
+  if (host) return set_error(STWO_B200_E_DIVISION_BY_ZERO, "batch_inverse: zero element");
+  return STWO_B200_OK;
+}
+
+int32_t stwo_b200_logup_interaction(stwo_b200_context* ctx, uint32_t log_rows, uint32_t n_uses,
+                                    const stwo_b200_logup_use* uses, const stwo_b200_qm31* alphas,
+                                    stwo_b200_qm31 z, uint32_t batch, uint32_t order, uint32_t* out,
+                                    uint64_t out_stride, stwo_b200_qm31* claimed_host, void* stream) {
+  CK_CTX(ctx);
+  if (log_rows > 28 || n_uses == 0 || n_uses > STWO_B200_LOGUP_MAX_USES || !uses || !out || !claimed_host ||
+      (batch != 1 && batch != 2) || order > 1 || out_stride < (1ull << log_rows))
+    return set_error(STWO_B200_E_INVALID, "bad logup_interaction arguments");
+  sb::LogupParams p{};
+  p.log_rows = log_rows;
+  p.n_uses = n_uses;
+  p.batch = batch;
+  p.order = order;
+  p.z = q(z);
+  uint32_t max_words = 0;
+  for (uint32_t u = 0; u < n_uses; ++u) {
+    const stwo_b200_logup_use& in = uses[u];
+    if (in.n_words == 0 || in.n_words > STWO_B200_LOGUP_MAX_WORDS)
+      return set_error(STWO_B200_E_INVALID, "logup use with 0 or more than 8 words");
+    max_words = std::max(max_words, in.n_words);
+    sb::LogupUse& o = p.uses[u];
+    o.n_words = in.n_words;
+    o.negate = in.negate != 0;
+    for (uint32_t j = 0; j < in.n_words; ++j) {
+      o.words[j] = in.words[j];
+      o.constants[j] = in.constants[j];
+      if (!in.words[j] && in.constants[j] >= sb::P) return set_error(STWO_B200_E_INVALID, "non-canonical constant");
+    }
+    o.multiplicity = in.multiplicity;
+  }
+  if (!alphas) return set_error(STWO_B200_E_INVALID, "null alphas");
+  for (uint32_t j = 0; j < max_words; ++j) p.alphas[j] = q(alphas[j]);
+  cudaStream_t s = st(stream);
+  size_t nscratch = sb::logup_scratch_count(log_rows) + 1;  // block sums + claimed
+  void* scratch = nullptr;
+  cudaError_t e = cudaMallocAsync(&scratch, nscratch * sizeof(sb::QM31), s);
+  if (e != cudaSuccess) return cuda_status(e, "logup scratch");
+  sb::QM31* claimed_dev = static_cast<sb::QM31*>(scratch);
+  std::lock_guard<std::mutex> g(ctx->ctx.small_mu);
+  uint32_t* flag = ctx->ctx.small;
+  e = cudaMemsetAsync(flag, 0, 4, s);
+  if (e == cudaSuccess) e = sb::logup_interaction(p, out, out_stride, claimed_dev, claimed_dev + 1, flag, s);
+  uint32_t host[5] = {0, 0, 0, 0, 0};
+  if (e == cudaSuccess) e = cudaMemcpyAsync(host, claimed_dev, 16, cudaMemcpyDeviceToHost, s);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(host + 4, flag, 4, cudaMemcpyDeviceToHost, s);
+  cudaError_t e2 = cudaFreeAsync(scratch, s);
+  if (e == cudaSuccess) e = e2;
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  if (e != cudaSuccess) return cuda_status(e, "logup_interaction");
+  if (host[4]) return set_error(STWO_B200_E_DIVISION_BY_ZERO, "logup_interaction: zero denominator");
+  *claimed_host = stwo_b200_qm31{host[0], host[1], host[2], host[3]};
   return STWO_B200_OK;
 }
 

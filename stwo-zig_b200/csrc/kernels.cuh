@@ -135,11 +135,43 @@ struct HashGatherItem {
 };
 cudaError_t gather_hashes(const HashGatherItem* items, uint32_t n, uint8_t* out, cudaStream_t stream);
 
-// ---- LogUp fraction / prefix scan (a20) ------------------------------------
-// out (4 coord columns): cumulative sum in coset order of 1/(z - sum_j alpha^j v_j)
-// (the reference's scalar law), see logup.cu.
-cudaError_t logup_cumsum(uint32_t log_size, uint32_t n_vals, const uint32_t* vals, uint64_t stride,
-                         const uint32_t* mult, QM31 z, QM31 alpha, uint32_t* out, uint64_t out_stride,
-                         QM31* scratch, cudaStream_t stream);
+// ---- Batch inversion (src/core/fields/mod.zig:164-200) ---------------------
+// Montgomery batch inverse of n elements of `degree` (1 M31, 2 CM31, 4 QM31)
+// coordinate columns. Sets *zero_flag (device) to 1 when an element is zero.
+// dst may alias src.
+cudaError_t batch_inverse(uint32_t degree, uint64_t n, const uint32_t* src, uint64_t src_stride, uint32_t* dst,
+                          uint64_t dst_stride, uint32_t* zero_flag, cudaStream_t stream);
+
+// ---- LogUp interaction columns (a20) ---------------------------------------
+// One use of a relation: denominator = sum_j alphas[j] * word_j(row) - z,
+// numerator = +/- multiplicity(row) (relation_combine / relation_multiplicity,
+// src/backends/metal/shaders/core/relation.metal:54-90).
+constexpr uint32_t LOGUP_MAX_WORDS = 8;
+constexpr uint32_t LOGUP_MAX_USES = 32;
+struct LogupUse {
+  uint32_t n_words;
+  uint32_t negate;
+  const uint32_t* words[LOGUP_MAX_WORDS];  // nullptr: constants[j]
+  uint32_t constants[LOGUP_MAX_WORDS];
+  const uint32_t* multiplicity;            // nullptr: 1
+};
+struct LogupParams {
+  uint32_t log_rows;
+  uint32_t n_uses;
+  uint32_t batch;  // uses per interaction column: 1, or 2 (pairs n1 d2 + n2 d1 over d1 d2)
+  uint32_t order;  // 0: cumulative sum in storage order; 1: coset order minus total/N per step
+  QM31 alphas[LOGUP_MAX_WORDS];
+  QM31 z;
+  LogupUse uses[LOGUP_MAX_USES];
+};
+SB_HD uint32_t logup_n_cols(uint32_t n_uses, uint32_t batch) { return (n_uses + batch - 1) / batch; }
+// Scratch entries (QM31) logup_interaction needs for 2^log_rows rows.
+size_t logup_scratch_count(uint32_t log_rows);
+// out: n_cols interaction columns of 4 coordinate columns each (column c, coordinate k at
+// out + (4c + k) * out_stride). Column c holds, per row, the running sum over columns 0..c of
+// the row's fractions; the last column is then scanned over rows. claimed (device QM31) gets
+// the total. *zero_flag (device) is set to 1 when a denominator is zero.
+cudaError_t logup_interaction(const LogupParams& p, uint32_t* out, uint64_t out_stride, QM31* claimed,
+                              QM31* scratch, uint32_t* zero_flag, cudaStream_t stream);
 
 }  // namespace sb

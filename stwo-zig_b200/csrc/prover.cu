@@ -286,10 +286,37 @@ void WideFibProver::release() {
   ws_log_n_ = ws_W_ = ws_B_ = 0;
 }
 
+size_t WideFibProver::workspace_bytes(uint32_t log_n, uint32_t W, uint32_t B) {
+  return layout_bytes(layout_for(log_n, W, B, 0)) + (1 << 20);
+}
+
+void WideFibProver::set_transient(bool on) {
+  if (on && !transient_ && arena_) {
+    cudaFree(arena_);
+    arena_ = nullptr;
+    arena_size_ = 0;
+    ws_log_n_ = ws_W_ = ws_B_ = 0;
+  }
+  transient_ = on;
+}
+
 int32_t WideFibProver::ensure_workspace(uint32_t log_n, uint32_t W, uint32_t B) {
+  if (!pinned_) {
+    pinned_size_ = GATHER_SCRATCH + (1 << 20);
+    if (cudaMallocHost(&pinned_, pinned_size_) != cudaSuccess) { pinned_ = nullptr; return fail(E_OOM, "pinned staging allocation failed"); }
+  }
+  size_t need = workspace_bytes(log_n, W, B);
+  if (transient_) {
+    if (cudaMallocAsync(&arena_, need, stream_) != cudaSuccess) {
+      arena_ = nullptr;
+      cudaGetLastError();
+      return fail(E_OOM, "device workspace allocation failed");
+    }
+    arena_size_ = need;
+    ws_log_n_ = log_n; ws_W_ = W; ws_B_ = B;
+    return OK;
+  }
   if (arena_ && ws_log_n_ == log_n && ws_W_ == W && ws_B_ == B) return OK;
-  Layout l = layout_for(log_n, W, B, 0);
-  size_t need = layout_bytes(l) + (1 << 20);
   if (arena_ && arena_size_ >= need) {
     ws_log_n_ = log_n; ws_W_ = W; ws_B_ = B;
     return OK;
@@ -297,10 +324,6 @@ int32_t WideFibProver::ensure_workspace(uint32_t log_n, uint32_t W, uint32_t B) 
   if (arena_) { cudaFree(arena_); arena_ = nullptr; }
   if (cudaMalloc(&arena_, need) != cudaSuccess) { arena_ = nullptr; cudaGetLastError(); return fail(E_OOM, "device workspace allocation failed"); }
   arena_size_ = need;
-  if (!pinned_) {
-    pinned_size_ = GATHER_SCRATCH + (1 << 20);
-    if (cudaMallocHost(&pinned_, pinned_size_) != cudaSuccess) { pinned_ = nullptr; return fail(E_OOM, "pinned staging allocation failed"); }
-  }
   ws_log_n_ = log_n; ws_W_ = W; ws_B_ = B;
   return OK;
 }
@@ -316,6 +339,18 @@ int32_t WideFibProver::prove(const ProveRequest& req, std::string& out, StageTim
   cudaSetDevice(ctx_->device);
   int32_t rc = ensure_workspace(n, W, B);
   if (rc != OK) return rc;
+  // In transient mode the workspace goes back to the stream-ordered pool on every exit path.
+  struct TransientRelease {
+    WideFibProver* p;
+    ~TransientRelease() {
+      if (p->transient_ && p->arena_) {
+        cudaFreeAsync(p->arena_, p->stream_);
+        p->arena_ = nullptr;
+        p->arena_size_ = 0;
+        p->ws_log_n_ = p->ws_W_ = p->ws_B_ = 0;
+      }
+    }
+  } transient_release{this};
   Layout l = layout_for(n, W, B, cfg.log_last_layer_degree_bound);
   Arena arena{arena_, 0, arena_size_};
   Buffers b;
@@ -738,6 +773,8 @@ const char* status_string(int32_t code) {
     case E_BUFFER_TOO_SMALL: return "output buffer too small";
     case E_FALLBACK: return "operation not taken by the device";
     case E_NO_DEVICE: return "no CUDA device";
+    case E_DIVISION_BY_ZERO: return "division by zero";
+    case E_REJECTED: return "admission rejected";
     default: return "unknown status";
   }
 }

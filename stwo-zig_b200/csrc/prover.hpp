@@ -46,6 +46,8 @@ enum : int32_t {
   E_BUFFER_TOO_SMALL = -6,
   E_FALLBACK = -7,
   E_NO_DEVICE = -8,
+  E_DIVISION_BY_ZERO = -9,
+  E_REJECTED = -10,
 };
 
 struct Context;
@@ -57,6 +59,12 @@ class WideFibProver {
   ~WideFibProver();
   int32_t prove(const ProveRequest& req, std::string& proof_json, StageTimes* times);
   const std::string& error() const { return err_; }
+  // Device workspace one proof of this shape uses (bytes).
+  static size_t workspace_bytes(uint32_t log_n, uint32_t W, uint32_t B);
+  // Transient mode: the workspace is taken from the device's stream-ordered pool at the start of
+  // each proof and returned at its end, so the device memory a prover holds between proofs is
+  // only its pinned staging. Used by the serving loop, which admits by in-flight workspace bytes.
+  void set_transient(bool on);
 
  private:
   int32_t ensure_workspace(uint32_t log_n, uint32_t W, uint32_t B);
@@ -70,6 +78,7 @@ class WideFibProver {
   uint8_t* arena_ = nullptr;
   size_t arena_size_ = 0;
   uint32_t ws_log_n_ = 0, ws_W_ = 0, ws_B_ = 0;
+  bool transient_ = false;
   uint8_t* pinned_ = nullptr;
   size_t pinned_size_ = 0;
   cudaEvent_t ev_[12];

@@ -1,0 +1,172 @@
+// Serving loop (continuous batching) over WideFibProver slots; see server.hpp.
+#include "server.hpp"
+
+#include <algorithm>
+#include <cstring>
+
+namespace sb {
+
+bool profile_limits(uint32_t profile, ResourceLimits* out) {
+  // STANDARD/LARGE/EXTREME_MAX_COMMITTED_CELLS and _ACCOUNTED_BYTES, resource_admission.zig:14-19.
+  switch (profile) {
+    case 0: *out = {33554432ull, 536870912ull}; return true;
+    case 1: *out = {134217728ull, 2147483648ull}; return true;
+    case 2: *out = {419430400ull, 6710886400ull}; return true;
+    default: return false;
+  }
+}
+
+Server::Server(Context* ctx, uint32_t slots, uint64_t budget, uint32_t profile, uint32_t flags)
+    : ctx_(ctx), n_slots_(slots), budget_(budget), flags_(flags), held_(slots, 0) {
+  if (!profile_limits(profile, &limits_)) limits_ = {0, 0};
+  snap_.budget_bytes = budget;
+}
+
+int32_t Server::start() {
+  if (limits_.max_committed_cells == 0) return E_INVALID;
+  cudaSetDevice(ctx_->device);
+  for (uint32_t i = 0; i < n_slots_; ++i) {
+    cudaStream_t s;
+    if (cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking) != cudaSuccess) return E_CUDA;
+    WideFibProver* p = new WideFibProver(ctx_, s);
+    p->set_transient(!(flags_ & SERVER_PERSISTENT_WORKSPACES));
+    provers_.push_back(p);
+  }
+  for (uint32_t i = 0; i < n_slots_; ++i) threads_.emplace_back(&Server::worker, this, i);
+  return OK;
+}
+
+Server::~Server() {
+  {
+    std::lock_guard<std::mutex> g(mu_);
+    stopping_ = true;
+  }
+  cv_work_.notify_all();
+  for (auto& t : threads_) t.join();
+  for (auto* p : provers_) delete p;
+  for (auto& kv : table_) delete kv.second;
+}
+
+int32_t Server::submit(const ProveRequest& r, uint64_t* ticket, std::string* err) {
+  // admit(profile, log_rows, columns), resource_admission.zig: rows in [1, 22], cells and
+  // accounted bytes within the profile.
+  if (r.log_n_rows < 1 || r.log_n_rows > ADMISSION_MAX_LOG_ROWS || r.sequence_len < 2 || r.sequence_len > 1000 ||
+      r.config.log_blowup_factor < 1 || r.config.log_blowup_factor > 4) {
+    *err = "invalid proof shape";
+    return E_INVALID;
+  }
+  uint64_t cells = (uint64_t)r.sequence_len << r.log_n_rows;
+  uint64_t accounted = cells * ACCOUNTED_BYTES_PER_CELL;
+  std::lock_guard<std::mutex> g(mu_);
+  if (cells > limits_.max_committed_cells || accounted > limits_.max_accounted_bytes) {
+    ++snap_.rejected;
+    *err = "committed cell budget of the resource profile exceeded";
+    return E_REJECTED;
+  }
+  size_t ws = WideFibProver::workspace_bytes(r.log_n_rows, r.sequence_len, r.config.log_blowup_factor);
+  if (ws > budget_) {
+    ++snap_.rejected;
+    *err = "proof workspace exceeds the server's device memory budget";
+    return E_REJECTED;
+  }
+  Entry* e = new Entry();
+  e->req = r;
+  e->ticket = next_ticket_++;
+  e->workspace = ws;
+  e->stats.accounted_bytes = accounted;
+  e->stats.workspace_bytes = ws;
+  e->t_submit = std::chrono::steady_clock::now();
+  table_[e->ticket] = e;
+  queue_.push_back(e);
+  ++snap_.submitted;
+  *ticket = e->ticket;
+  cv_work_.notify_one();
+  return OK;
+}
+
+void Server::worker(uint32_t slot) {
+  cudaSetDevice(ctx_->device);
+  WideFibProver* prover = provers_[slot];
+  std::unique_lock<std::mutex> lk(mu_);
+  for (;;) {
+    // First in, first admitted: the head waits until its workspace fits the budget. Transient
+    // workspaces count while their proof runs; persistent ones count for as long as a slot holds
+    // them (a slot grows its workspace to the largest proof it has run).
+    const bool persistent = flags_ & SERVER_PERSISTENT_WORKSPACES;
+    auto extra = [&](const Entry* h) -> uint64_t {
+      if (!persistent) return h->workspace;
+      return h->workspace > held_[slot] ? h->workspace - held_[slot] : 0;
+    };
+    cv_work_.wait(lk, [&] {
+      return (stopping_ && queue_.empty()) || (!queue_.empty() && in_use_ + extra(queue_.front()) <= budget_);
+    });
+    if (queue_.empty()) return;
+    Entry* e = queue_.front();
+    queue_.pop_front();
+    const uint64_t added = extra(e);
+    in_use_ += added;
+    if (persistent) held_[slot] += added;
+    ++in_flight_;
+    snap_.peak_in_flight = std::max(snap_.peak_in_flight, in_flight_);
+    snap_.peak_workspace_bytes = std::max<uint64_t>(snap_.peak_workspace_bytes, in_use_);
+    e->t_start = std::chrono::steady_clock::now();
+    e->stats.slot = slot;
+    lk.unlock();
+    // Another head may fit beside this one.
+    cv_work_.notify_one();
+    std::string proof;
+    int32_t rc = prover->prove(e->req, proof, &e->stats.stages);
+    auto t_end = std::chrono::steady_clock::now();
+    lk.lock();
+    if (!persistent) in_use_ -= e->workspace;
+    --in_flight_;
+    e->status = rc;
+    if (rc == OK) {
+      e->proof.swap(proof);
+      ++snap_.completed;
+    } else {
+      e->error = prover->error();
+      ++snap_.failed;
+    }
+    e->stats.queued_ms = std::chrono::duration<double, std::milli>(e->t_start - e->t_submit).count();
+    e->stats.run_ms = std::chrono::duration<double, std::milli>(t_end - e->t_start).count();
+    e->done = true;
+    cv_done_.notify_all();
+    cv_work_.notify_all();
+  }
+}
+
+int32_t Server::wait(uint64_t ticket, uint8_t* out, size_t cap, size_t* len, RequestStats* stats, std::string* err) {
+  std::unique_lock<std::mutex> lk(mu_);
+  auto it = table_.find(ticket);
+  if (it == table_.end()) {
+    *err = "unknown ticket";
+    return E_INVALID;
+  }
+  Entry* e = it->second;
+  cv_done_.wait(lk, [&] { return e->done; });
+  if (stats) *stats = e->stats;
+  if (e->status != OK) {
+    *err = e->error;
+    int32_t rc = e->status;
+    table_.erase(it);
+    delete e;
+    return rc;
+  }
+  if (len) *len = e->proof.size();
+  if (!out || cap < e->proof.size()) {
+    *err = "proof buffer too small";
+    return E_BUFFER_TOO_SMALL;
+  }
+  std::memcpy(out, e->proof.data(), e->proof.size());
+  table_.erase(it);
+  delete e;
+  return OK;
+}
+
+ServerSnapshot Server::snapshot() {
+  std::lock_guard<std::mutex> g(mu_);
+  return snap_;
+}
+
+}  // namespace sb

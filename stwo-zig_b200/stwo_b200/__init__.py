@@ -32,6 +32,8 @@ E_CONSTRAINTS = -5
 E_BUFFER_TOO_SMALL = -6
 E_FALLBACK = -7
 E_NO_DEVICE = -8
+E_DIVISION_BY_ZERO = -9
+E_REJECTED = -10
 
 _u32 = ctypes.c_uint32
 _u64 = ctypes.c_uint64
@@ -54,9 +56,28 @@ class RequestC(ctypes.Structure):
                 ("channel_seed", _u64)]
 
 
+class LogupUseC(ctypes.Structure):
+    _fields_ = [("n_words", _u32), ("negate", _u32), ("words", _vp * 8), ("constants", _u32 * 8),
+                ("multiplicity", _vp)]
+
+
+class ServerConfigC(ctypes.Structure):
+    _fields_ = [("slots", _u32), ("profile", _u32), ("memory_budget", _u64), ("flags", _u32)]
+
+
+class ServerSnapshotC(ctypes.Structure):
+    _fields_ = [(n, _u64) for n in ("submitted", "completed", "failed", "rejected", "peak_in_flight",
+                                    "peak_workspace_bytes", "budget_bytes")]
+
+
 class StageTimesC(ctypes.Structure):
     _fields_ = [(n, ctypes.c_float) for n in ("upload", "trace", "main_commit", "composition", "composition_commit",
                                               "oods", "quotients", "fri", "pow", "decommit", "total")]
+
+
+class RequestStatsC(ctypes.Structure):
+    _fields_ = [("accounted_bytes", _u64), ("workspace_bytes", _u64), ("queued_ms", ctypes.c_double),
+                ("run_ms", ctypes.c_double), ("slot", _u32), ("stages", StageTimesC)]
 
 
 _SIGS = {
@@ -82,6 +103,15 @@ _SIGS = {
     "stwo_b200_wide_fib_composition": [_vp, _u32, _u32, _vp, _u64, _vp, _u32, _u32, _vp, _u64, _vp],
     "stwo_b200_pow_grind": [_vp, ctypes.c_char_p, _u32, ctypes.POINTER(_u64)],
     "stwo_b200_telemetry_snapshot": [ctypes.POINTER(_u64)],
+    "stwo_b200_server_create": [_vp, ctypes.POINTER(ServerConfigC), ctypes.POINTER(_vp)],
+    "stwo_b200_server_submit": [_vp, ctypes.POINTER(RequestC), ctypes.POINTER(_u64)],
+    "stwo_b200_server_wait": [_vp, _u64, _vp, ctypes.c_size_t, ctypes.POINTER(ctypes.c_size_t),
+                              ctypes.POINTER(RequestStatsC)],
+    "stwo_b200_server_snapshot_get": [_vp, ctypes.POINTER(ServerSnapshotC)],
+    "stwo_b200_server_destroy": [_vp],
+    "stwo_b200_batch_inverse": [_vp, _u32, _u64, _vp, _u64, _vp, _u64, _vp],
+    "stwo_b200_logup_interaction": [_vp, _u32, _u32, ctypes.POINTER(LogupUseC), ctypes.POINTER(QM31C), QM31C,
+                                    _u32, _u32, _vp, _u64, ctypes.POINTER(QM31C), _vp],
 }
 for _name, _args in _SIGS.items():
     _fn = getattr(_lib, _name)
@@ -330,7 +360,95 @@ class Context:
                                                    2 << log_n_rows, _ptr(coeffs), den0, den1, _ptr(out),
                                                    2 << log_n_rows, _stream(stream)))
 
+    def batch_inverse(self, src, dst, n: int, degree: int = 1, src_stride: int | None = None,
+                      dst_stride: int | None = None, stream=None) -> None:
+        """Montgomery batch inverse (batchInverse); raises StwoError(E_DIVISION_BY_ZERO) on a zero."""
+        _check(_lib.stwo_b200_batch_inverse(self._h, degree, n, _ptr(src), n if src_stride is None else src_stride,
+                                            _ptr(dst), n if dst_stride is None else dst_stride, _stream(stream)))
+
+    def logup_interaction(self, log_rows: int, uses: list[dict], alphas, z, out, batch: int = 1, order: int = 1,
+                          stream=None) -> tuple:
+        """LogUp interaction columns into `out` ((n_cols, 4, 2^log_rows) words); returns the claimed
+        sum. uses: dicts with "words" (device columns or int constants), optional "multiplicity"
+        (device column) and "negate"."""
+        arr = (LogupUseC * len(uses))()
+        for u, d in zip(arr, uses):
+            u.n_words = len(d["words"])
+            u.negate = int(bool(d.get("negate", False)))
+            for j, w in enumerate(d["words"][:8]):  # the library rejects more than 8 words
+                if isinstance(w, int):
+                    u.constants[j] = w
+                else:
+                    u.words[j] = _ptr(w)
+            u.multiplicity = _ptr(d.get("multiplicity"))
+        al = (QM31C * max(1, len(alphas)))(*[_qm(a) for a in alphas])
+        claimed = QM31C()
+        _check(_lib.stwo_b200_logup_interaction(self._h, log_rows, len(uses), arr, al, _qm(z), batch, order,
+                                                _ptr(out), 1 << log_rows, ctypes.byref(claimed), _stream(stream)))
+        return (claimed.a, claimed.b, claimed.c, claimed.d)
+
     def pow_grind(self, prefix_digest: bytes, n_bits: int) -> int:
         nonce = _u64(0)
         _check(_lib.stwo_b200_pow_grind(self._h, prefix_digest, n_bits, ctypes.byref(nonce)))
         return nonce.value
+
+
+class Server:
+    """Continuous-batching serving loop on one device (stwo_b200_server_*): `slots` proofs in
+    flight, admitted first-in first-out within `memory_budget` bytes of device workspace (0 = 80% of
+    free device memory) and the reference's resource profile (0 standard, 1 large, 2 extreme)."""
+
+    def __init__(self, ctx: Context, slots: int = 8, profile: int = 1, memory_budget: int = 0,
+                 persistent_workspaces: bool = False):
+        h = _vp()
+        cfg = ServerConfigC(slots, profile, memory_budget, int(persistent_workspaces))
+        _check(_lib.stwo_b200_server_create(ctx._h, ctypes.byref(cfg), ctypes.byref(h)))
+        self._h = h
+        self._ctx = ctx
+        self._keep: dict[int, object] = {}
+
+    def submit(self, statement: Statement, config: PcsConfig, trace=None, trace_kind: int = TRACE_REFERENCE,
+               trace_seed: int = 0, channel_seed: int | None = None) -> int:
+        req, keep = self._ctx._request(statement, config, trace, trace_kind, trace_seed, channel_seed)
+        ticket = _u64(0)
+        _check(_lib.stwo_b200_server_submit(self._h, ctypes.byref(req), ctypes.byref(ticket)))
+        self._keep[ticket.value] = keep
+        return ticket.value
+
+    def wait(self, ticket: int) -> tuple[bytes, dict]:
+        cap = 1 << 21
+        n = ctypes.c_size_t(0)
+        st = RequestStatsC()
+        buf = ctypes.create_string_buffer(cap)
+        rc = _lib.stwo_b200_server_wait(self._h, ticket, buf, cap, ctypes.byref(n), ctypes.byref(st))
+        if rc == E_BUFFER_TOO_SMALL:
+            buf = ctypes.create_string_buffer(n.value)
+            rc = _lib.stwo_b200_server_wait(self._h, ticket, buf, n.value, ctypes.byref(n), ctypes.byref(st))
+        self._keep.pop(ticket, None)
+        _check(rc)
+        stats = {name: getattr(st, name) for name, _ in RequestStatsC._fields_ if name != "stages"}
+        stats["stages"] = {name: getattr(st.stages, name) for name, _ in StageTimesC._fields_}
+        return buf.raw[: n.value], stats
+
+    def snapshot(self) -> dict:
+        s = ServerSnapshotC()
+        _check(_lib.stwo_b200_server_snapshot_get(self._h, ctypes.byref(s)))
+        return {name: getattr(s, name) for name, _ in ServerSnapshotC._fields_}
+
+    def close(self) -> None:
+        if self._h:
+            _lib.stwo_b200_server_destroy(self._h)
+            self._h = None
+            self._keep.clear()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

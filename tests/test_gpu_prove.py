@@ -107,3 +107,30 @@ def test_gpu_proofs_verify(ctx, log_n, W, preset):
     p = ctx.prove_wide_fibonacci(sb.Statement(log_n, W), g, trace_kind=sb.TRACE_SEEDED, trace_seed=42,
                                  channel_seed=9)
     assert verifier.verify_wide_fib(p, log_n, W, channel_seed=9)
+
+
+def mixed_requests(master_seed=2026, count=48):
+    """48 wide-Fibonacci statements: log_n_rows uniform in 14..20, sequence_len in {16, 32, 100},
+    each with its own trace seed and channel seed, all drawn from one master seed."""
+    import stwo_b200 as sb
+    rng = np.random.default_rng(master_seed)
+    _, g = cfg_pair("secure")
+    reqs = []
+    for i in range(count):
+        reqs.append(dict(statement=sb.Statement(int(rng.integers(14, 21)), int(rng.choice([16, 32, 100]))),
+                         config=g, trace_kind=sb.TRACE_SEEDED, trace_seed=int(rng.integers(1, 2**63)),
+                         channel_seed=int(rng.integers(0, 2**63))))
+    return reqs
+
+
+def test_mixed_batch_of_48_matches_single_runs(ctx):
+    reqs = mixed_requests()
+    batch = ctx.prove_wide_fibonacci_batch(reqs, max_in_flight=8)
+    for r, p in zip(reqs, batch):
+        single = ctx.prove_wide_fibonacci(r["statement"], r["config"], trace_kind=r["trace_kind"],
+                                          trace_seed=r["trace_seed"], channel_seed=r["channel_seed"])
+        assert p == single
+    # A few of them independently verified.
+    for r, p in list(zip(reqs, batch))[:3]:
+        assert verifier.verify_wide_fib(p, r["statement"].log_n_rows, r["statement"].sequence_len,
+                                        channel_seed=r["channel_seed"])

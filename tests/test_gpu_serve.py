@@ -1,0 +1,99 @@
+"""Serving loop: continuous batching, admission by resource profile and device memory budget."""
+import threading
+import time
+
+import numpy as np
+import pytest
+
+import oracle
+
+pytestmark = pytest.mark.gpu
+
+
+def _cfg(preset="secure"):
+    import stwo_b200 as sb
+    c = oracle.config(preset)
+    return sb.PcsConfig(c.pow_bits, sb.FriConfig(c.log_blowup_factor, c.log_last_layer_degree_bound, c.n_queries))
+
+
+def _stream(seed, count):
+    rng = np.random.default_rng(seed)
+    out = []
+    for _ in range(count):
+        out.append(dict(log_n=int(rng.integers(12, 21)), W=int(rng.choice([16, 32, 100])),
+                        trace_seed=int(rng.integers(1, 2**62)), channel_seed=int(rng.integers(0, 2**62)),
+                        gap_s=float(rng.exponential(1 / 200.0))))
+    return out
+
+
+def test_served_proofs_equal_their_single_runs(ctx):
+    import stwo_b200 as sb
+    g = _cfg()
+    reqs = _stream(7, 24)
+    tickets = [None] * len(reqs)
+    with sb.Server(ctx, slots=6, profile=2) as srv:
+        def producer():
+            for i, r in enumerate(reqs):
+                tickets[i] = srv.submit(sb.Statement(r["log_n"], r["W"]), g, trace_kind=sb.TRACE_SEEDED,
+                                        trace_seed=r["trace_seed"], channel_seed=r["channel_seed"])
+                time.sleep(r["gap_s"])
+        th = threading.Thread(target=producer)
+        th.start()
+        served = []
+        for i in range(len(reqs)):
+            while tickets[i] is None:
+                time.sleep(0.001)
+            served.append(srv.wait(tickets[i]))
+        th.join()
+        snap = srv.snapshot()
+    assert snap["completed"] == len(reqs) and snap["failed"] == 0
+    assert snap["peak_in_flight"] > 1  # requests overlapped on the device
+    for r, (proof, stats) in zip(reqs, served):
+        alone = ctx.prove_wide_fibonacci(sb.Statement(r["log_n"], r["W"]), g, trace_kind=sb.TRACE_SEEDED,
+                                         trace_seed=r["trace_seed"], channel_seed=r["channel_seed"])
+        assert proof == alone
+        assert stats["accounted_bytes"] == 16 * r["W"] << r["log_n"]
+
+
+def test_resource_profile_admission(ctx):
+    import stwo_b200 as sb
+    g = _cfg("functional")
+    cases = [(0, 18, 100, True), (0, 20, 100, False), (1, 20, 100, True), (1, 21, 100, False),
+             (1, 22, 100, False), (2, 22, 100, True), (2, 22, 101, False)]
+    for profile, log_n, W, ok in cases:
+        with sb.Server(ctx, slots=1, profile=profile) as srv:
+            if ok:
+                t = srv.submit(sb.Statement(log_n, W), g, trace_kind=sb.TRACE_SEEDED, trace_seed=1)
+                proof, _ = srv.wait(t)
+                assert len(proof) > 0
+            else:
+                with pytest.raises(sb.StwoError) as e:
+                    srv.submit(sb.Statement(log_n, W), g, trace_kind=sb.TRACE_SEEDED, trace_seed=1)
+                assert e.value.status == sb.E_REJECTED
+
+
+def test_memory_budget_limits_in_flight_work(ctx):
+    import stwo_b200 as sb
+    g = _cfg("functional")
+    with sb.Server(ctx, slots=2, profile=1) as probe:
+        _, st = probe.wait(probe.submit(sb.Statement(16, 32), g, trace_kind=sb.TRACE_SEEDED, trace_seed=1))
+    ws = st["workspace_bytes"]
+    with sb.Server(ctx, slots=4, profile=1, memory_budget=ws + ws // 2) as srv:
+        ts = [srv.submit(sb.Statement(16, 32), g, trace_kind=sb.TRACE_SEEDED, trace_seed=10 + i) for i in range(5)]
+        proofs = [srv.wait(t)[0] for t in ts]
+        with pytest.raises(sb.StwoError) as e:
+            srv.submit(sb.Statement(18, 32), g, trace_kind=sb.TRACE_SEEDED, trace_seed=1)
+        assert e.value.status == sb.E_REJECTED
+        snap = srv.snapshot()
+    assert snap["peak_in_flight"] == 1 and snap["peak_workspace_bytes"] <= ws + ws // 2
+    for i, p in enumerate(proofs):
+        assert p == ctx.prove_wide_fibonacci(sb.Statement(16, 32), g, trace_kind=sb.TRACE_SEEDED, trace_seed=10 + i)
+
+
+def test_close_finishes_queued_requests(ctx):
+    import stwo_b200 as sb
+    g = _cfg("functional")
+    srv = sb.Server(ctx, slots=2, profile=1)
+    for i in range(6):
+        srv.submit(sb.Statement(14, 16), g, trace_kind=sb.TRACE_SEEDED, trace_seed=i)
+    srv.close()  # drains without a wait per request

@@ -138,3 +138,83 @@ def test_verifier_rejects_tampering(path):
     bad = json.dumps(d, separators=(",", ":")).encode()
     with pytest.raises(verifier.VerificationError):
         verifier.verify_wide_fib(bad, entry["log_n_rows"], entry["sequence_len"])
+
+
+def _py_inverse(x):
+    return verifier.qinv(x)
+
+
+def test_batch_inverse_oracle():
+    rng = np.random.default_rng(3)
+    for degree in (1, 2, 4):
+        for n in (1, 2, 7, 64):
+            v = rng.integers(1, 2**31 - 1, size=(degree, n), dtype=np.uint32)
+            got = oracle.batch_inverse(v[0] if degree == 1 else v)
+            got = got.reshape(degree, n)
+            for i in range(n):
+                x = verifier.q(*[int(v[k, i]) for k in range(degree)])
+                assert verifier.qflat(verifier.qinv(x))[:degree] == [int(got[k, i]) for k in range(degree)]
+    with pytest.raises(oracle.DivisionByZero):
+        oracle.batch_inverse(np.array([5, 0, 7], dtype=np.uint32))
+
+
+def test_logup_scan_law_of_the_reference():
+    # src/tests/metal/backend/commitment_test.zig:73-154: 256 rows, one use (11, row + 1),
+    # alphas (3, 5), z = 7; fraction = 1 / (3*11 + 5*(row+1) - 7); shift = total / 256; scan in
+    # coset order (scan index s -> circle index s/2 or 255 - s/2, stored at its bit reverse).
+    rows, log = 256, 8
+    col = np.arange(1, rows + 1, dtype=np.uint32)
+    out, claimed = oracle.logup_interaction(log, [dict(words=[11, col])], [[3, 0, 0, 0], [5, 0, 0, 0]],
+                                            [7, 0, 0, 0], batch=1, order=1)
+    q = verifier.q
+    fr = [verifier.qinv(verifier.qsub(verifier.qadd(verifier.qmulm(q(3), 11), verifier.qmulm(q(5), r + 1)), q(7)))
+          for r in range(rows)]
+    total = q(0)
+    for f in fr:
+        total = verifier.qadd(total, f)
+    shift = verifier.qmulm(total, pow(rows, 2**31 - 3, 2**31 - 1))
+    acc, expected = q(0), [None] * rows
+    for s in range(rows):
+        ci = s // 2 if s % 2 == 0 else rows - 1 - s // 2
+        r = int(f"{ci:08b}"[::-1], 2)
+        acc = verifier.qadd(acc, verifier.qsub(fr[r], shift))
+        expected[r] = acc
+    assert list(claimed) == verifier.qflat(total)
+    for r in range(rows):
+        assert [int(out[0, k, r]) for k in range(4)] == verifier.qflat(expected[r])
+
+
+def test_logup_pairs_storage_order_law():
+    # cumulativeColumn (src/frontends/riscv/air/logup.zig:83-105): per row
+    # (n1 d2 + n2 d1) / (d1 d2), running sum in storage order, claimed = last value.
+    rng = np.random.default_rng(4)
+    log, rows = 5, 32
+    a = rng.integers(0, 256, size=rows, dtype=np.uint32)
+    b = rng.integers(0, 256, size=rows, dtype=np.uint32)
+    m = rng.integers(0, 9, size=rows, dtype=np.uint32)
+    alphas = [[1, 0, 0, 0], [12345, 6, 7, 8], [99, 1, 2, 3]]
+    z = [1000003, 5, 11, 2]
+    uses = [dict(words=[a, b]), dict(words=[4, a, b], multiplicity=m, negate=True)]
+    out, claimed = oracle.logup_interaction(log, uses, alphas, z, batch=2, order=0)
+    Q = [verifier.q(*x) for x in alphas]
+    zq = verifier.q(*z)
+
+    def den(ws, r):
+        acc = verifier.qsub(verifier.q(0), zq)
+        for j, w in enumerate(ws):
+            acc = verifier.qadd(acc, verifier.qmulm(Q[j], w if isinstance(w, int) else int(w[r])))
+        return acc
+    acc = verifier.q(0)
+    for r in range(rows):
+        d1, d2 = den([a, b], r), den([4, a, b], r)
+        n1, n2 = 1, (2**31 - 1 - int(m[r])) % (2**31 - 1)
+        num = verifier.qadd(verifier.qmulm(d2, n1), verifier.qmulm(d1, n2))
+        acc = verifier.qadd(acc, verifier.qmul(num, verifier.qinv(verifier.qmul(d1, d2))))
+        assert [int(out[0, k, r]) for k in range(4)] == verifier.qflat(acc)
+    assert list(claimed) == verifier.qflat(acc)
+
+
+def test_logup_zero_denominator():
+    col = np.arange(16, dtype=np.uint32)
+    with pytest.raises(oracle.DivisionByZero):
+        oracle.logup_interaction(4, [dict(words=[col])], [[1, 0, 0, 0]], [5, 0, 0, 0])
