@@ -13,6 +13,8 @@ trace and device-to-host of every proof inside the timed region).
     python bench.py --workload mixed48      # 48 mixed-shape proofs in one submission
     python bench.py --workload serve [--rates 25,50,100,200] [--requests 64]
                                             # Poisson arrivals into the serving loop
+    python bench.py --workload kernels128   # kernel-level ops: 128 columns 2^20 -> 2^21, Merkle,
+                                            # fold_circle_into_line 2^21 and fold_line to 2^4
 
 N > 1 runs under torchrun as independent replicas (proofs do not shard): each
 rank proves its own K proofs; value = N*K / max over ranks of the timed region.
@@ -47,7 +49,7 @@ def parse():
     ap.add_argument("--preset", default="secure")
     ap.add_argument("--in-flight", type=int, default=IN_FLIGHT)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", default="headline", choices=["headline", "mixed48", "serve"])
+    ap.add_argument("--workload", default="headline", choices=["headline", "mixed48", "serve", "kernels128"])
     ap.add_argument("--rates", default="25,50,100,200")
     ap.add_argument("--requests", type=int, default=64)
     ap.add_argument("--slots", type=int, default=8)
@@ -191,7 +193,7 @@ def main():
     ctx = sb.Context(local)
     if args.workload != "headline":
         if rank == 0:
-            (run_mixed48 if args.workload == "mixed48" else run_serve)(args, ctx)
+            {"mixed48": run_mixed48, "serve": run_serve, "kernels128": run_kernels128}[args.workload](args, ctx)
         if world > 1:
             import torch.distributed as dist
             dist.destroy_process_group()
@@ -206,13 +208,10 @@ def main():
             import torch.distributed as dist
             dist.barrier()
 
+    from stwo_b200 import replicas
+
     def max_over_ranks(x: float) -> float:
-        if world == 1:
-            return x
-        import torch.distributed as dist
-        t = torch.tensor([x], device=dev, dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+        return replicas.max_over_ranks(x, device=dev)
 
     # Device-resident traces, a distinct seed per proof (generated untimed by the library's kernel).
     seeds = [1_000_003 * (rank + 1) + i for i in range(K + W)]
@@ -340,7 +339,7 @@ def main():
                      "frac": fft_gbs / hbm_peak, "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)",
                      "traffic": FFT_TRAFFIC_BYTES.get((args.log_n, args.width)),
                      "algorithmic_bytes": fft_bytes, "ms": fft_ms},
-        "roofline_int32": {"kernel": "k_pow (Blake2s, 1 compression per nonce)", "hashes_per_s": hashes_per_s,
+        "roofline_int32": {"kernel": "k_pow_round (Blake2s, 1 compression per nonce)", "hashes_per_s": hashes_per_s,
                            "nonces": nonce + 1, "ms": pow_ms, "unit": "thread instructions/s",
                            "achieved": hashes_per_s * POW_INSTR_PER_NONCE,
                            "peak": 148 * 128 * 1e6 * (clocks.summary().get("sm_mhz") or 1965.0),
@@ -418,6 +417,91 @@ def run_mixed48(args, ctx):
     print(json.dumps(out), flush=True)
 
 
+def run_kernels128(args, ctx):
+    """The kernel-level case: 128 seeded uniform M31 columns of 2^20 interpolated on their canonic
+    coset and extended to 2^21, a Blake2s Merkle commit of the 2^21 x 128 evaluations, then
+    fold_circle_into_line of a seeded uniform QM31 evaluation of 2^21 and fold_line down to 2^4 with
+    seeded alphas. Each op is timed with CUDA events (inputs larger than L2); four sampled columns,
+    the folds and the Merkle root of 8 columns are checked against the oracle."""
+    import numpy as np
+    import torch
+    import stwo_b200 as sb
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
+    P = (1 << 31) - 1
+    n, cols = 20, 128
+    g = torch.Generator(device="cuda").manual_seed(128)
+    evals = torch.randint(0, P - 1, (cols << n,), dtype=torch.int32, device="cuda", generator=g)
+    coeffs = torch.empty_like(evals)
+    lde = torch.empty(cols << (n + 1), dtype=torch.int32, device="cuda")
+    layers = torch.empty(((4 << n) - 1) * 32, dtype=torch.uint8, device="cuda")
+    line = torch.randint(0, P, (4 << (n + 1),), dtype=torch.int32, device="cuda", generator=g)
+    rng = np.random.default_rng(128)
+    alphas = [rng.integers(0, P, size=4).tolist() for _ in range(n + 1)]
+    folds = [torch.empty(4 << k, dtype=torch.int32, device="cuda") for k in range(n + 1)]
+    stream = torch.cuda.current_stream()
+
+    def timed(fn, reps=5):
+        fn()
+        torch.cuda.synchronize()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        for _ in range(reps):
+            fn()
+        b.record(stream)
+        torch.cuda.synchronize()
+        return a.elapsed_time(b) / reps
+
+    def fri_chain():
+        ctx.fold_circle_into_line(line, folds[n], n + 1, alphas[0])
+        for k in range(n, 4, -1):
+            ctx.fold_line(folds[k], folds[k - 1], k, alphas[n + 1 - k])
+
+    fft_ms = timed(lambda: ctx.interpolate_and_extend(evals, coeffs, lde, n, 1, cols))
+    merkle_ms = timed(lambda: ctx.merkle_commit(lde, n + 1, cols, layers))
+    fri_ms = timed(fri_chain)
+    peaks = {}
+    try:
+        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except (OSError, ValueError):
+        pass
+    hbm = peaks.get("hbm_gbs", 6650.0)
+    fft_bytes = 16 * (cols << n)
+    fold_bytes = sum(48 << k for k in range(4, n + 1))  # 32 B in + 16 B out per output
+    leaf_comp = (1 << (n + 1)) * ((cols + 15) // 16)
+    node_comp = (1 << (n + 1)) - 1
+    # parity: 4 sampled columns, the FRI chain and an 8-column root against the oracle
+    ev = evals.cpu().numpy().view(np.uint32).reshape(cols, 1 << n)
+    co = coeffs.cpu().numpy().view(np.uint32).reshape(cols, 1 << n)
+    ld = lde.cpu().numpy().view(np.uint32).reshape(cols, 2 << n)
+    ok = True
+    for c in (0, 37, 90, 127):
+        oc = oracle.interpolate(ev[c])
+        ok &= bool(np.array_equal(co[c], oc)) and bool(np.array_equal(ld[c], oracle.extend(oc, 1)))
+    small = torch.empty(((4 << n) - 1) * 32, dtype=torch.uint8, device="cuda")
+    root8 = ctx.merkle_commit(lde, n + 1, 8, small)
+    ok &= root8 == oracle.merkle_root([ld[c] for c in range(8)])
+    src = line.cpu().numpy().view(np.uint32).reshape(4, 2 << n)
+    f = oracle.fold_circle_into_line(src, alphas[0])
+    for k in range(n, 4, -1):
+        f = oracle.fold_line(f, alphas[n + 1 - k], n)
+    ok &= bool(np.array_equal(folds[4].cpu().numpy().view(np.uint32).reshape(4, 16), f))
+    out = {"metric": "kernel-level ops, 128 columns of 2^20", "workload": "kernels128", "n_gpus": 1,
+           "value": fft_bytes / (fft_ms / 1e3) / 1e9, "unit": "GB/s", "higher_is_better": True, "dtype": "u32",
+           "data": "synthetic: seeded uniform M31 columns and QM31 evaluation",
+           "config": {"workload": "interpolate 128 x 2^20 + extend to 2^21, Merkle 2^21 x 128, fold_circle_into_line "
+                                  "2^21 + fold_line to 2^4", "l2": "inputs larger than L2"},
+           "fft": {"ms": fft_ms, "algorithmic_bytes": fft_bytes, "gbs": fft_bytes / (fft_ms / 1e3) / 1e9,
+                   "frac_hbm": fft_bytes / (fft_ms / 1e3) / 1e9 / hbm},
+           "merkle": {"ms": merkle_ms, "compressions": leaf_comp + node_comp,
+                      "g_compressions_per_s": (leaf_comp + node_comp) / (merkle_ms / 1e3) / 1e9,
+                      "read_gbs": 4 * (cols << (n + 1)) / (merkle_ms / 1e3) / 1e9},
+           "fri": {"ms": fri_ms, "algorithmic_bytes": fold_bytes, "gbs": fold_bytes / (fri_ms / 1e3) / 1e9,
+                   "launches": 1 + (n - 4)},
+           "hbm_peak_gbs": hbm, "bit_exact_vs_oracle": bool(ok)}
+    print(json.dumps(out), flush=True)
+
+
 def run_serve(args, ctx):
     """Poisson arrivals (seeded) of wide-Fibonacci requests (log_n_rows 12..22, sequence_len
     {16, 32, 100}) into the serving loop at each rate; latency = submit to proof bytes. The same
@@ -439,7 +523,7 @@ def run_serve(args, ctx):
                                               trace_seed=r["trace_seed"], channel_seed=r["channel_seed"]))
     single_s = time.perf_counter() - t0
     for rate in rates:
-        with sb.Server(ctx, slots=args.slots, profile=2) as srv:
+        with sb.Server(ctx, slots=args.slots, profile=2, persistent_workspaces=True) as srv:
             for r in stmts[:args.slots]:  # warm the stream-ordered pool
                 srv.wait(srv.submit(sb.Statement(r["log_n"], r["W"]), cfg, trace_kind=sb.TRACE_SEEDED,
                                     trace_seed=r["trace_seed"], channel_seed=r["channel_seed"]))
@@ -479,7 +563,7 @@ def run_serve(args, ctx):
            "data": "synthetic: seeded traces, master seed 4242",
            "config": {"workload": f"{len(stmts)} wide-Fibonacci requests, log_n_rows uniform 12..22, sequence_len "
                                   "in {16, 32, 100}, Poisson arrivals", "protocol": args.preset,
-                      "slots": args.slots, "profile": "extreme"},
+                      "slots": args.slots, "profile": "extreme", "workspaces": "persistent per slot"},
            "rates": results,
            "single": {"proofs_per_s": len(stmts) / single_s, "wall_ms": 1e3 * single_s},
            "serving_over_single": best / (len(stmts) / single_s)}

@@ -219,6 +219,17 @@ int32_t stwo_b200_eval_at_point_noalloc(stwo_b200_context* ctx, uint32_t log_siz
 int32_t stwo_b200_merkle_commit(stwo_b200_context* ctx, uint32_t log_size, uint32_t n_cols, const uint32_t* cols,
                                 uint64_t stride, uint8_t* layers_dev, uint8_t* root_host, void* stream);
 
+/* Lifted Blake2s Merkle commitment of columns of mixed log sizes (the interaction and preprocessed
+ * trees of AIRs with several component sizes). cols: host array of n_cols device column pointers,
+ * log_sizes: host array of their log sizes (each >= 1 unless all are 0; at most 2048 columns).
+ * Columns are hashed in the reference's leaf order, stably sorted by log size ascending, each at its
+ * lifted index ((pos >> (max_log - log + 1)) << 1) + (pos & 1) (src/prover/vcs_lifted/leaves.zig:
+ * 104-115, decommit.zig:88). layers_dev: 2^(max_log+1)-1 hashes, leaves first. Synchronous when
+ * root_host is set. Replaces commitMerkle for mixed-size column sets (merkle_ops.zig:20-56). */
+int32_t stwo_b200_merkle_commit_lifted(stwo_b200_context* ctx, uint32_t n_cols, const uint32_t* const* cols,
+                                       const uint32_t* log_sizes, uint8_t* layers_dev, uint8_t* root_host,
+                                       void* stream);
+
 /* ---- FriOps (src/backend/fri_ops.zig:19-37) ------------------------------------------------------ */
 
 /* dst = dst * alpha^2 + fold(src) when accumulate, else fold(src); src 4 coordinate columns of
@@ -297,6 +308,14 @@ int32_t stwo_b200_logup_interaction(stwo_b200_context* ctx, uint32_t log_rows, u
                                     const stwo_b200_logup_use* uses, const stwo_b200_qm31* alphas,
                                     stwo_b200_qm31 z, uint32_t batch, uint32_t order, uint32_t* out,
                                     uint64_t out_stride, stwo_b200_qm31* claimed_host, void* stream);
+
+/* XOR-lookup trace for a LogUp lookup AIR (no reference AIR; the table follows the reference's
+ * bitwise table, src/frontends/riscv/air/preprocessed/bitwise.zig:17-35): main_cols receives 3
+ * columns of 2^log_n rows (a, b seeded uniform u8 - SplitMix64 of seed ^ (0xD6E8FEB86659FD93 *
+ * (row + 1)), a = low byte, b = next byte - and a XOR b), table 3 columns of 65536 rows (row
+ * a * 256 + b holds a, b, a XOR b), multiplicity 65536 words: how often each table row occurs. */
+int32_t stwo_b200_xor_lookup_trace(stwo_b200_context* ctx, uint32_t log_n, uint64_t seed, uint32_t* main_cols,
+                                   uint32_t* table, uint32_t* multiplicity, void* stream);
 
 /* ---- Channel proof of work ---------------------------------------------------------------------- */
 

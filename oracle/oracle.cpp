@@ -1283,4 +1283,31 @@ int oracle_logup_interaction(uint32_t log_rows, uint32_t n_uses, const oracle_lo
   return 0;
 }
 
+// XOR-lookup trace (the device kernel k_xor_trace restated): SplitMix64 of
+// seed ^ (0xD6E8FEB86659FD93 * (row + 1)), a = low byte, b = next byte, c = a ^ b; the
+// table follows the reference's bitwise table layout (row a * 256 + b,
+// src/frontends/riscv/air/preprocessed/bitwise.zig:17-35); mult counts each (a, b).
+int oracle_xor_lookup_trace(uint32_t log_n, uint64_t seed, uint32_t* main_cols, uint32_t* table, uint32_t* mult) {
+  if (log_n > 26) return -1;
+  const uint64_t rows = 1ull << log_n;
+  std::fill(mult, mult + 65536, 0u);
+  for (uint64_t r = 0; r < rows; ++r) {
+    uint64_t z = (seed ^ (0xD6E8FEB86659FD93ull * (r + 1))) + 0x9E3779B97F4A7C15ull;
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+    z ^= z >> 31;
+    uint32_t a = (uint32_t)z & 255u, b = (uint32_t)(z >> 8) & 255u;
+    main_cols[r] = a;
+    main_cols[rows + r] = b;
+    main_cols[2 * rows + r] = a ^ b;
+    ++mult[a << 8 | b];
+  }
+  for (uint32_t i = 0; i < 65536; ++i) {
+    table[i] = i >> 8;
+    table[65536 + i] = i & 255u;
+    table[2 * 65536 + i] = (i >> 8) ^ (i & 255u);
+  }
+  return 0;
+}
+
 }  // extern "C"

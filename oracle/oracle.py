@@ -243,3 +243,14 @@ def logup_interaction(log_rows: int, uses: list[dict], alphas, z, batch: int = 1
         raise DivisionByZero("logup_interaction: zero denominator")
     assert r == 0
     return out, claimed
+
+
+def xor_lookup_trace(log_n: int, seed: int):
+    """(main (3, 2^log_n), table (3, 65536), multiplicity (65536,)) of the XOR-lookup trace."""
+    main = np.empty((3, 1 << log_n), dtype=np.uint32)
+    table = np.empty((3, 65536), dtype=np.uint32)
+    mult = np.empty(65536, dtype=np.uint32)
+    lib().oracle_xor_lookup_trace.argtypes = [ctypes.c_uint32, ctypes.c_uint64, ctypes.POINTER(ctypes.c_uint32),
+                                              ctypes.POINTER(ctypes.c_uint32), ctypes.POINTER(ctypes.c_uint32)]
+    assert lib().oracle_xor_lookup_trace(log_n, seed, _u32p(main), _u32p(table), _u32p(mult)) == 0
+    return main, table, mult

@@ -79,6 +79,9 @@ int oracle_logup_interaction(uint32_t log_rows, uint32_t n_uses, const oracle_lo
                              const uint32_t* alphas, const uint32_t z[4], uint32_t batch, uint32_t order,
                              uint32_t* out, uint32_t claimed[4]);
 
+/* XOR-lookup trace: main 3 x 2^log_n (a, b, a ^ b), table 3 x 65536, mult 65536. */
+int oracle_xor_lookup_trace(uint32_t log_n, uint64_t seed, uint32_t* main_cols, uint32_t* table, uint32_t* mult);
+
 #ifdef __cplusplus
 }
 #endif

@@ -238,6 +238,56 @@ int32_t stwo_b200_merkle_commit(stwo_b200_context* ctx, uint32_t log_size, uint3
   return STWO_B200_OK;
 }
 
+int32_t stwo_b200_merkle_commit_lifted(stwo_b200_context* ctx, uint32_t n_cols, const uint32_t* const* cols,
+                                       const uint32_t* log_sizes, uint8_t* layers_dev, uint8_t* root_host,
+                                       void* stream) {
+  CK_CTX(ctx);
+  if (!layers_dev || (n_cols && (!cols || !log_sizes)) || n_cols > 2048)
+    return set_error(STWO_B200_E_INVALID, "bad merkle_commit_lifted arguments");
+  uint32_t max_log = 0;
+  for (uint32_t c = 0; c < n_cols; ++c) {
+    if (log_sizes[c] > 28 || !cols[c]) return set_error(STWO_B200_E_INVALID, "bad lifted column");
+    max_log = std::max(max_log, log_sizes[c]);
+  }
+  for (uint32_t c = 0; c < n_cols; ++c)
+    if (log_sizes[c] == 0 && max_log > 0) return set_error(STWO_B200_E_INVALID, "lifted columns need log size >= 1");
+  // Leaf order: stably sorted by log size ascending.
+  std::vector<uint32_t> order(n_cols);
+  for (uint32_t c = 0; c < n_cols; ++c) order[c] = c;
+  std::stable_sort(order.begin(), order.end(), [&](uint32_t a, uint32_t b) { return log_sizes[a] < log_sizes[b]; });
+  std::vector<uint64_t> staged(n_cols + (n_cols + 1) / 2 + 1, 0);
+  uint32_t* logs = reinterpret_cast<uint32_t*>(staged.data() + n_cols);
+  for (uint32_t i = 0; i < n_cols; ++i) {
+    staged[i] = reinterpret_cast<uint64_t>(cols[order[i]]);
+    logs[i] = log_sizes[order[i]];
+  }
+  cudaStream_t s = st(stream);
+  void* dev = nullptr;
+  cudaError_t e = cudaSuccess;
+  if (n_cols) {
+    e = cudaMallocAsync(&dev, staged.size() * 8, s);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(dev, staged.data(), staged.size() * 8, cudaMemcpyHostToDevice, s);
+  }
+  if (e == cudaSuccess) {
+    auto* dptr = static_cast<const uint32_t* const*>(dev);
+    auto* dlog = dev ? reinterpret_cast<const uint32_t*>(static_cast<uint64_t*>(dev) + n_cols) : nullptr;
+    e = sb::merkle_commit_lifted(max_log, n_cols, dptr, dlog, layers_dev, s);
+  }
+  // The staging copy above came from pageable memory, so it has completed; the free is stream-ordered.
+  if (dev) {
+    cudaError_t e2 = cudaFreeAsync(dev, s);
+    if (e == cudaSuccess) e = e2;
+  }
+  if (e != cudaSuccess) return cuda_status(e, "merkle_commit_lifted");
+  if (root_host) {
+    const uint64_t leaves = n_cols ? (1ull << max_log) : 1;
+    e = cudaMemcpyAsync(root_host, layers_dev + (2 * leaves - 2) * 32, 32, cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    return cuda_status(e, "merkle root readback");
+  }
+  return STWO_B200_OK;
+}
+
 int32_t stwo_b200_fold_circle_into_line(stwo_b200_context* ctx, uint32_t src_log, const uint32_t* src,
                                         uint64_t src_stride, stwo_b200_qm31 alpha, uint32_t* dst,
                                         uint64_t dst_stride, int32_t accumulate, void* stream) {
@@ -314,13 +364,18 @@ int32_t stwo_b200_pow_grind(stwo_b200_context* ctx, const uint8_t prefix_digest[
   uint32_t* res = ctx->ctx.small;
   uint32_t w[8];
   std::memcpy(w, prefix_digest, 32);
-  uint64_t max_nonce = n_bits >= 48 ? ~0ull : (1ull << (n_bits + 16));
-  cudaError_t e = sb::pow_grind(w, n_bits, max_nonce, res, s);
-  uint32_t host[3] = {0, 0, 0};
-  if (e == cudaSuccess) e = cudaMemcpyAsync(host, res, 12, cudaMemcpyDeviceToHost, s);
-  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  // The prover's search: bounded rounds in nonce order, four per check, at most 2^(bits+16) nonces.
+  const uint64_t max_nonce = n_bits >= 48 ? ~0ull : (1ull << (n_bits + 16));
+  const uint64_t per_round = sb::pow_round_nonces(ctx->ctx.sm_count);
+  cudaError_t e = cudaMemsetAsync(res, 0xff, 8, s);
+  uint64_t nonce = ~0ull;
+  for (uint64_t base = 0; e == cudaSuccess && base < max_nonce && nonce == ~0ull;) {
+    for (int r = 0; r < 4 && base < max_nonce && e == cudaSuccess; ++r, base += per_round)
+      e = sb::pow_round(w, n_bits, base, res, ctx->ctx.sm_count, s);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(&nonce, res, 8, cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  }
   if (e != cudaSuccess) return cuda_status(e, "pow_grind");
-  uint64_t nonce = (uint64_t)host[0] | ((uint64_t)host[1] << 32);
   if (nonce == ~0ull) return set_error(STWO_B200_E_TIMEOUT, "proof-of-work search bound reached");
   *nonce_out = nonce;
   return STWO_B200_OK;
@@ -399,6 +454,14 @@ int32_t stwo_b200_server_destroy(stwo_b200_server* server) {
   delete server->server;
   delete server;
   return STWO_B200_OK;
+}
+
+int32_t stwo_b200_xor_lookup_trace(stwo_b200_context* ctx, uint32_t log_n, uint64_t seed, uint32_t* main_cols,
+                                   uint32_t* table, uint32_t* multiplicity, void* stream) {
+  CK_CTX(ctx);
+  if (log_n > 28 || !main_cols || !table || !multiplicity)
+    return set_error(STWO_B200_E_INVALID, "bad xor_lookup_trace arguments");
+  return cuda_status(sb::xor_lookup_trace(log_n, seed, main_cols, table, multiplicity, st(stream)), "xor_lookup_trace");
 }
 
 int32_t stwo_b200_batch_inverse(stwo_b200_context* ctx, uint32_t degree, uint64_t n, const uint32_t* src,

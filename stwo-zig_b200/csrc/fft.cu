@@ -487,11 +487,11 @@ static cudaError_t launch_low(const DeviceTables& t, bool inverse, uint32_t doma
 static cudaError_t launch_high(const HighParams& p, uint32_t n_cols, cudaStream_t stream) {
   uint32_t rows_log = std::max(p.src_log, p.do_forward ? p.out_log : p.src_log) - p.b;
   size_t smem = ((size_t)HIGH_T * 4) << rows_log;
-  static bool attr_set = false;
-  if (!attr_set) {
+  static const bool attr_set = [] {  // once per process (thread-safe static initialisation)
     cudaFuncSetAttribute(k_fft_high, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
-    attr_set = true;
-  }
+    return true;
+  }();
+  (void)attr_set;
   dim3 grid((1u << p.b) / HIGH_T, n_cols);
   k_fft_high<<<grid, HIGH_THREADS, smem, stream>>>(p); note_launch();
   return cudaGetLastError();
@@ -519,11 +519,11 @@ static cudaError_t launch_low12(const DeviceTables& t, bool inverse, uint32_t do
 static cudaError_t launch_high16(const High16Params& p, uint32_t n_cols, cudaStream_t stream) {
   uint32_t rows = p.do_forward ? std::max(p.rows_in, p.rows_out) : p.rows_in;
   size_t smem = (size_t)64 << rows;
-  static bool attr_set = false;
-  if (!attr_set) {
+  static const bool attr_set = [] {  // once per process (thread-safe static initialisation)
     cudaFuncSetAttribute(k_fft_high16, cudaFuncAttributeMaxDynamicSharedMemorySize, 64 * 1024);
-    attr_set = true;
-  }
+    return true;
+  }();
+  (void)attr_set;
   dim3 grid(1u << (B12 - 4), n_cols);
   k_fft_high16<<<grid, 1u << rows, smem, stream>>>(p);
   note_launch();

@@ -56,7 +56,8 @@ cudaError_t extend(const DeviceTables& t, uint32_t log_size, uint32_t log_blowup
 cudaError_t merkle_commit(uint32_t log_size, uint32_t n_cols, const uint32_t* cols, uint64_t stride,
                           uint8_t* layers, cudaStream_t stream);
 // Leaves of columns with mixed log sizes (lifted), columns in leaf order
-// (stably sorted by log size ascending), pointers and logs in device memory.
+// (stably sorted by log size ascending), pointers and logs in device memory;
+// at most 2048 columns, each of log size >= 1 unless max_log is 0.
 cudaError_t merkle_commit_lifted(uint32_t max_log, uint32_t n_cols, const uint32_t* const* col_ptrs,
                                  const uint32_t* col_logs, uint8_t* layers, cudaStream_t stream);
 SB_HD uint64_t merkle_layer_offset(uint32_t max_log, uint32_t layer_log) {
@@ -108,10 +109,6 @@ cudaError_t fri_fold_commit(const DeviceTables& t, bool circle, uint32_t src_log
                             cudaStream_t stream);
 
 // ---- Proof of work (src/core/channel/blake2s.zig:135-240) ------------------
-// result[0..1] = lowest valid nonce (u64), result[2] = status (0 ok, 1 gave up).
-cudaError_t pow_grind(const uint32_t prefix_words[8], uint32_t n_bits, uint64_t max_nonce,
-                      uint32_t* result_dev, cudaStream_t stream);
-
 // Bounded rounds of the same search (the form the prover uses, so the grind
 // never holds every SM slot for the whole search): result_dev[0..1] must start
 // at ~0; round r covers nonces [base, base + pow_round_nonces(sm_count)).
@@ -173,5 +170,11 @@ size_t logup_scratch_count(uint32_t log_rows);
 // the total. *zero_flag (device) is set to 1 when a denominator is zero.
 cudaError_t logup_interaction(const LogupParams& p, uint32_t* out, uint64_t out_stride, QM31* claimed,
                               QM31* scratch, uint32_t* zero_flag, cudaStream_t stream);
+
+// XOR-lookup trace of 2^log_n rows (3 columns a, b, a ^ b, stride 2^log_n; a, b seeded
+// uniform u8), the 2^16-row XOR table (3 columns, row a * 256 + b) and the table-row
+// multiplicities (65536 words).
+cudaError_t xor_lookup_trace(uint32_t log_n, uint64_t seed, uint32_t* main_cols, uint32_t* table, uint32_t* mult,
+                             cudaStream_t stream);
 
 }  // namespace sb

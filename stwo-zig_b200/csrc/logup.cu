@@ -16,6 +16,8 @@
 // the suffix-product trick), then a three-pass scan over 1024-position blocks:
 // block sums, a one-CTA scan of the block sums (which also writes the claimed
 // sum), and the finalising rescan that writes the last column in place.
+#include <algorithm>
+
 #include "kernels.cuh"
 
 namespace sb {
@@ -202,6 +204,38 @@ uint32_t scan_blocks(uint32_t log_rows) {
   return (uint32_t)((rows + SCAN_BLOCK - 1) / SCAN_BLOCK);
 }
 
+// XOR-lookup trace: seeded uniform u8 pairs, their XOR, the 2^16-row XOR table
+// in the layout of the reference's bitwise table (row a * 256 + b holds (a, b, a ^ b),
+// src/frontends/riscv/air/preprocessed/bitwise.zig:17-35) and the multiplicity of
+// every table row in the trace.
+__device__ __forceinline__ uint64_t xor_splitmix(uint64_t z) {
+  z += 0x9E3779B97F4A7C15ull;
+  z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+  z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+  return z ^ (z >> 31);
+}
+
+__global__ void k_xor_trace(uint32_t log_n, uint64_t seed, uint32_t* main_cols, uint32_t* mult) {
+  const uint64_t rows = 1ull << log_n;
+  for (uint64_t r = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; r < rows; r += (uint64_t)gridDim.x * blockDim.x) {
+    uint64_t x = xor_splitmix(seed ^ (0xD6E8FEB86659FD93ull * (r + 1)));
+    uint32_t a = (uint32_t)x & 255u, b = (uint32_t)(x >> 8) & 255u;
+    main_cols[r] = a;
+    main_cols[rows + r] = b;
+    main_cols[2 * rows + r] = a ^ b;
+    atomicAdd(mult + (a << 8 | b), 1u);
+  }
+}
+
+__global__ void k_xor_table(uint32_t* table) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= 65536) return;
+  const uint32_t a = i >> 8, b = i & 255u;
+  table[i] = a;
+  table[65536 + i] = b;
+  table[2 * 65536 + i] = a ^ b;
+}
+
 }  // namespace
 
 size_t logup_scratch_count(uint32_t log_rows) { return scan_blocks(log_rows); }
@@ -223,6 +257,20 @@ cudaError_t logup_interaction(const LogupParams& p, uint32_t* out, uint64_t out_
   k_logup_scan_blocks<<<1, LU_THREADS, 0, stream>>>(scratch, nb, claimed);
   note_launch();
   k_logup_finalize<<<nb, LU_THREADS, 0, stream>>>(last, out_stride, p.log_rows, p.order, scratch, claimed);
+  note_launch();
+  return cudaGetLastError();
+}
+
+cudaError_t xor_lookup_trace(uint32_t log_n, uint64_t seed, uint32_t* main_cols, uint32_t* table, uint32_t* mult,
+                             cudaStream_t stream) {
+  if (log_n > 28) return cudaErrorInvalidValue;
+  cudaError_t e = cudaMemsetAsync(mult, 0, 65536 * 4, stream);
+  if (e != cudaSuccess) return e;
+  const uint64_t rows = 1ull << log_n;
+  const uint32_t grid = (uint32_t)std::min<uint64_t>((rows + 255) / 256, 148 * 16);
+  k_xor_trace<<<grid, 256, 0, stream>>>(log_n, seed, main_cols, mult);
+  note_launch();
+  k_xor_table<<<256, 256, 0, stream>>>(table);
   note_launch();
   return cudaGetLastError();
 }

@@ -103,6 +103,61 @@ __global__ void __launch_bounds__(LEAF_THREADS) k_merkle_leaves(uint32_t log_siz
   fold_levels(sm, count, levels, layers, log_size, log_size, (uint64_t)blockIdx.x * LEAF_THREADS, seeds.node, one);
 }
 
+// Leaves over columns of mixed log sizes (the lifted tree, src/prover/vcs_lifted/
+// leaves.zig:104-115): leaf pos hashes, for every column in leaf order (stably
+// sorted by log size ascending), its value at ((pos >> (max_log - log + 1)) << 1)
+// + (pos & 1). Column pointers and log sizes are staged in shared memory.
+constexpr uint32_t LIFTED_MAX_COLS = 2048;
+
+__global__ void __launch_bounds__(LEAF_THREADS) k_merkle_leaves_lifted(uint32_t max_log, uint32_t n_cols,
+                                                                       const uint32_t* const* __restrict__ col_ptrs,
+                                                                       const uint32_t* __restrict__ col_logs,
+                                                                       uint8_t* layers, Seeds seeds, uint32_t levels,
+                                                                       uint32_t one) {
+  __shared__ uint32_t sm[LEAF_THREADS * 8];
+  __shared__ const uint32_t* sp[LIFTED_MAX_COLS];
+  __shared__ uint8_t ssh[LIFTED_MAX_COLS];  // max_log - log + 1, or 0 for full-size columns
+  for (uint32_t c = threadIdx.x; c < n_cols; c += blockDim.x) {
+    sp[c] = col_ptrs[c];
+    uint32_t lg = col_logs[c];
+    ssh[c] = lg == max_log ? 0 : (uint8_t)(max_log - lg + 1);
+  }
+  __syncthreads();
+  const uint64_t row = (uint64_t)blockIdx.x * LEAF_THREADS + threadIdx.x;
+  const uint64_t n_rows = 1ull << max_log;
+  uint32_t h[8];
+  if (row < n_rows) {
+#pragma unroll
+    for (int i = 0; i < 8; ++i) h[i] = seeds.leaf[i];
+    const uint32_t n_blocks = (n_cols + 15) / 16;
+    const uint32_t total = 64 + 4 * n_cols;
+    for (uint32_t blk = 0; blk < n_blocks; ++blk) {
+      uint32_t m[16];
+      const uint32_t c0 = blk * 16;
+#pragma unroll
+      for (int i = 0; i < 16; ++i) {
+        uint32_t c = c0 + i;
+        uint32_t v = 0;
+        if (c < n_cols) {
+          uint32_t sh = ssh[c];
+          uint64_t idx = sh == 0 ? row : (((row >> sh) << 1) | (row & 1));
+          v = __ldg(sp[c] + idx);
+        }
+        m[i] = v;
+      }
+      const bool last = blk + 1 == n_blocks;
+      const uint32_t t = last ? total : 64 + 64 * (blk + 1);
+      b2s_compress(h, m, t, last, one);
+    }
+    store_hash(layers, row, h);
+#pragma unroll
+    for (int i = 0; i < 8; ++i) sm[threadIdx.x * 8 + i] = h[i];
+  }
+  __syncthreads();
+  uint32_t count = n_rows < LEAF_THREADS ? (uint32_t)n_rows : LEAF_THREADS;
+  fold_levels(sm, count, levels, layers, max_log, max_log, (uint64_t)blockIdx.x * LEAF_THREADS, seeds.node, one);
+}
+
 // Children layer of log size child_log -> `levels` parent levels; each CTA folds
 // 2 * NODE_THREADS children (or the whole layer when smaller).
 __global__ void __launch_bounds__(NODE_THREADS) k_merkle_nodes(uint8_t* layers, uint32_t max_log, uint32_t child_log,
@@ -262,6 +317,24 @@ cudaError_t merkle_commit(uint32_t log_size, uint32_t n_cols, const uint32_t* co
   return merkle_finish(layers, log_size, log_size - leaf_levels, stream);
 }
 
+cudaError_t merkle_commit_lifted(uint32_t max_log, uint32_t n_cols, const uint32_t* const* col_ptrs,
+                                 const uint32_t* col_logs, uint8_t* layers, cudaStream_t stream) {
+  const Seeds& seeds = seeds_once();
+  if (n_cols == 0) {
+    k_empty_root<<<1, 1, 0, stream>>>(layers, seeds); note_launch();
+    return cudaGetLastError();
+  }
+  if (n_cols > LIFTED_MAX_COLS) return cudaErrorInvalidValue;
+  const uint64_t n_rows = 1ull << max_log;
+  uint32_t leaf_levels = max_log <= LEAF_LEVELS ? max_log : (n_cols <= 4 ? LEAF_LEVELS : 0);
+  uint32_t grid = (uint32_t)((n_rows + LEAF_THREADS - 1) / LEAF_THREADS);
+  k_merkle_leaves_lifted<<<grid, LEAF_THREADS, 0, stream>>>(max_log, n_cols, col_ptrs, col_logs, layers, seeds,
+                                                            leaf_levels, 1u); note_launch();
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  return merkle_finish(layers, max_log, max_log - leaf_levels, stream);
+}
+
 // ---------------------------------------------------------------------------
 // Proof of work: lowest nonce with ctz(Blake2s(prefix_digest || LE64 nonce)[0..16]) >= n_bits.
 // Thread k tests nonces k, k + stride, ... and stops once its next nonce is not
@@ -279,35 +352,6 @@ __device__ __forceinline__ uint32_t ctz128(uint32_t a, uint32_t b, uint32_t c, u
 }
 
 struct PowPrefix { uint32_t w[8]; };
-
-__global__ void __launch_bounds__(256) k_pow(PowPrefix pre, uint32_t n_bits, uint64_t max_nonce,
-                                             unsigned long long* found, uint32_t* status, uint32_t one) {
-  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
-  uint64_t nonce = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  uint32_t iter = 0;
-  unsigned long long best = *((volatile unsigned long long*)found);
-  while (nonce < max_nonce && nonce < best) {
-    uint32_t h[8];
-    b2s_init(h);
-    uint32_t m[16];
-#pragma unroll
-    for (int i = 0; i < 8; ++i) m[i] = pre.w[i];
-    m[8] = (uint32_t)nonce; m[9] = (uint32_t)(nonce >> 32);
-#pragma unroll
-    for (int i = 10; i < 16; ++i) m[i] = 0;
-    b2s_compress(h, m, 40, true, one);
-    if (ctz128(h[0], h[1], h[2], h[3]) >= n_bits) {
-      atomicMin(found, (unsigned long long)nonce);
-      return;
-    }
-    nonce += stride;
-    if ((++iter & 3) == 0) best = *((volatile unsigned long long*)found);
-  }
-  if (nonce >= max_nonce && threadIdx.x == 0 && blockIdx.x == 0) {
-    // Reached the search bound: the host reports a timeout unless a nonce was found.
-    atomicExch(status, 1u);
-  }
-}
 
 // One bounded round of the search: nonces [base, base + grid*256*per_thread).
 // Rounds are enqueued in nonce order on one stream; a round starts by leaving
@@ -344,25 +388,10 @@ cudaError_t pow_round(const uint32_t prefix_words[8], uint32_t n_bits, uint64_t 
                       int sm_count, cudaStream_t stream) {
   PowPrefix pre;
   for (int i = 0; i < 8; ++i) pre.w[i] = prefix_words[i];
-  k_pow_round<<<sm_count * 4, 256, 0, stream>>>(pre, n_bits, base, 112,
-                                               reinterpret_cast<unsigned long long*>(result_dev), 1u); note_launch();
-  return cudaGetLastError();
-}
-
-cudaError_t pow_grind(const uint32_t prefix_words[8], uint32_t n_bits, uint64_t max_nonce, uint32_t* result_dev,
-                      cudaStream_t stream) {
-  PowPrefix pre;
-  for (int i = 0; i < 8; ++i) pre.w[i] = prefix_words[i];
-  // result: [0..1] found nonce (init ~0), [2] status
-  cudaError_t e = cudaMemsetAsync(result_dev, 0xff, 8, stream);
-  if (e != cudaSuccess) return e;
-  e = cudaMemsetAsync(result_dev + 2, 0, 4, stream);
-  if (e != cudaSuccess) return e;
-  int dev = 0, sms = 148;
-  cudaGetDevice(&dev);
-  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  k_pow<<<sms * 8, 256, 0, stream>>>(pre, n_bits, max_nonce, reinterpret_cast<unsigned long long*>(result_dev),
-                                     result_dev + 2, 1u); note_launch();
+  // Eight waves of short CTAs (14 nonces per thread, ~0.1 ms each) rather than one
+  // wave of long ones, so that other streams' work gets SMs between them.
+  k_pow_round<<<sm_count * 4 * 8, 256, 0, stream>>>(pre, n_bits, base, 14,
+                                                   reinterpret_cast<unsigned long long*>(result_dev), 1u); note_launch();
   return cudaGetLastError();
 }
 

@@ -271,11 +271,18 @@ void Context::release(WideFibProver* p) {
 // ---------------------------------------------------------------------------
 WideFibProver::WideFibProver(Context* ctx, cudaStream_t stream) : ctx_(ctx), stream_(stream) {
   for (auto& e : ev_) cudaEventCreate(&e);
+  int least = 0, greatest = 0;
+  if (cudaDeviceGetStreamPriorityRange(&least, &greatest) != cudaSuccess ||
+      cudaStreamCreateWithPriority(&fast_, cudaStreamNonBlocking, greatest) != cudaSuccess) {
+    cudaGetLastError();
+    fast_ = nullptr;
+  }
 }
 
 WideFibProver::~WideFibProver() {
   release();
   for (auto& e : ev_) cudaEventDestroy(e);
+  if (fast_) cudaStreamDestroy(fast_);
   if (stream_) cudaStreamDestroy(stream_);
 }
 
@@ -339,10 +346,12 @@ int32_t WideFibProver::prove(const ProveRequest& req, std::string& out, StageTim
   cudaSetDevice(ctx_->device);
   int32_t rc = ensure_workspace(n, W, B);
   if (rc != OK) return rc;
-  // In transient mode the workspace goes back to the stream-ordered pool on every exit path.
+  // On every exit path: the high-priority stream is drained (an early error return may leave
+  // its work in flight), then in transient mode the workspace goes back to the stream-ordered pool.
   struct TransientRelease {
     WideFibProver* p;
     ~TransientRelease() {
+      if (p->fast_) cudaStreamSynchronize(p->fast_);
       if (p->transient_ && p->arena_) {
         cudaFreeAsync(p->arena_, p->stream_);
         p->arena_ = nullptr;
@@ -359,6 +368,8 @@ int32_t WideFibProver::prove(const ProveRequest& req, std::string& out, StageTim
   cudaStream_t s = stream_;
   uint8_t* pin = pinned_;
   auto sync = [&]() -> cudaError_t { return cudaStreamSynchronize(s); };
+  cudaStream_t fs = fast_ ? fast_ : s;
+  auto fsync = [&]() -> cudaError_t { return cudaStreamSynchronize(fs); };
 
   Channel ch;
   SB_CK(cudaEventRecord(ev_[0], s));
@@ -438,13 +449,13 @@ int32_t WideFibProver::prove(const ProveRequest& req, std::string& out, StageTim
 
   // OODS point and sampled values of every coefficient column.
   PointQ oods = random_secure_point(ch);
-  SB_CK(eval_at_point(T, n, W, b.coeffs, l.N, oods, nullptr, b.oods_partial, b.oods_out, s));
-  SB_CK(eval_at_point(T, n, 4, b.comp, l.NC, oods, nullptr, b.oods_partial, b.oods_out + W, s));
-  SB_CK(eval_at_point(T, n, 4, b.comp + l.N, l.NC, oods, nullptr, b.oods_partial, b.oods_out + W + 4, s));
+  SB_CK(eval_at_point(T, n, W, b.coeffs, l.N, oods, nullptr, b.oods_partial, b.oods_out, fs));
+  SB_CK(eval_at_point(T, n, 4, b.comp, l.NC, oods, nullptr, b.oods_partial, b.oods_out + W, fs));
+  SB_CK(eval_at_point(T, n, 4, b.comp + l.N, l.NC, oods, nullptr, b.oods_partial, b.oods_out + W + 4, fs));
   std::vector<QM31> sampled(W + 8);
-  SB_CK(cudaMemcpyAsync(pin, b.oods_out, (W + 8) * sizeof(QM31), cudaMemcpyDeviceToHost, s));
-  SB_CK(cudaEventRecord(ev_[6], s));
-  SB_CK(sync());
+  SB_CK(cudaMemcpyAsync(pin, b.oods_out, (W + 8) * sizeof(QM31), cudaMemcpyDeviceToHost, fs));
+  SB_CK(cudaEventRecord(ev_[6], fs));
+  SB_CK(fsync());
   std::memcpy(sampled.data(), pin, (W + 8) * sizeof(QM31));
   ch.mix_felts(sampled.data(), sampled.size());
   QM31 quot_coeff = ch.draw_secure_felt();
@@ -469,19 +480,19 @@ int32_t WideFibProver::prove(const ProveRequest& req, std::string& out, StageTim
     for (uint32_t i = 0; i < 8; ++i) hp[W + i] = b.comp_lde + (size_t)i * l.NL;
     QuotientBatchDev* hb = reinterpret_cast<QuotientBatchDev*>(pin + 128 * 1024);
     hb->point = oods; hb->sum_a = sum_a; hb->sum_b = sum_b; hb->first = 0; hb->count = nq;
-    SB_CK(cudaMemcpyAsync(b.quot_c, hc, nq * sizeof(QM31), cudaMemcpyHostToDevice, s));
-    SB_CK(cudaMemcpyAsync(b.col_ptrs, hp, nq * sizeof(void*), cudaMemcpyHostToDevice, s));
-    SB_CK(cudaMemcpyAsync(b.batch, hb, sizeof(QuotientBatchDev), cudaMemcpyHostToDevice, s));
+    SB_CK(cudaMemcpyAsync(b.quot_c, hc, nq * sizeof(QM31), cudaMemcpyHostToDevice, fs));
+    SB_CK(cudaMemcpyAsync(b.col_ptrs, hp, nq * sizeof(void*), cudaMemcpyHostToDevice, fs));
+    SB_CK(cudaMemcpyAsync(b.batch, hb, sizeof(QuotientBatchDev), cudaMemcpyHostToDevice, fs));
   }
-  SB_CK(accumulate_quotients(T, l.L, 1, b.batch, b.col_ptrs, b.quot_c, b.quot, l.NL, s));
-  SB_CK(cudaEventRecord(ev_[7], s));
+  SB_CK(accumulate_quotients(T, l.L, 1, b.batch, b.col_ptrs, b.quot_c, b.quot, l.NL, fs));
+  SB_CK(cudaEventRecord(ev_[7], fs));
 
   // FRI: first layer, then inner layers each committed before its fold.
   std::vector<std::array<uint8_t, 32>> fri_roots;
   {
-    SB_CK(merkle_commit(l.L, 4, b.quot, l.NL, b.tree_q, s));
-    SB_CK(cudaMemcpyAsync(pin, b.tree_q + (2 * l.NL - 2) * 32, 32, cudaMemcpyDeviceToHost, s));
-    SB_CK(sync());
+    SB_CK(merkle_commit(l.L, 4, b.quot, l.NL, b.tree_q, fs));
+    SB_CK(cudaMemcpyAsync(pin, b.tree_q + (2 * l.NL - 2) * 32, 32, cudaMemcpyDeviceToHost, fs));
+    SB_CK(fsync());
     std::array<uint8_t, 32> r;
     std::memcpy(r.data(), pin, 32);
     fri_roots.push_back(r);
@@ -490,26 +501,26 @@ int32_t WideFibProver::prove(const ProveRequest& req, std::string& out, StageTim
     // Each fold writes the next line layer and, unless it is the last layer,
     // commits it in the same launch sequence.
     SB_CK(fri_fold_commit(T, true, l.L, b.quot, l.NL, alpha, b.line[0], 1ull << (l.L - 1),
-                          l.n_inner > 0 ? b.line_tree[0] : nullptr, s));
+                          l.n_inner > 0 ? b.line_tree[0] : nullptr, fs));
     for (uint32_t k = 0; k < l.n_inner; ++k) {
       uint32_t lg = l.L - 1 - k;
       size_t sz = 1ull << lg;
-      SB_CK(cudaMemcpyAsync(pin, b.line_tree[k] + (2 * sz - 2) * 32, 32, cudaMemcpyDeviceToHost, s));
-      SB_CK(sync());
+      SB_CK(cudaMemcpyAsync(pin, b.line_tree[k] + (2 * sz - 2) * 32, 32, cudaMemcpyDeviceToHost, fs));
+      SB_CK(fsync());
       std::memcpy(r.data(), pin, 32);
       fri_roots.push_back(r);
       ch.mix_root(r.data());
       QM31 a = ch.draw_secure_felt();
       SB_CK(fri_fold_commit(T, false, lg, b.line[k], sz, a, b.line[k + 1], sz / 2,
-                            k + 1 < l.n_inner ? b.line_tree[k + 1] : nullptr, s));
+                            k + 1 < l.n_inner ? b.line_tree[k + 1] : nullptr, fs));
     }
   }
   // Last layer: line IFFT of 2^last_log values (src/backend/line_evaluation.zig:97-145).
   std::vector<QM31> last_coeffs;
   {
     size_t m = 1ull << l.last_log;
-    SB_CK(cudaMemcpyAsync(pin, b.line[l.n_inner], 4 * m * 4, cudaMemcpyDeviceToHost, s));
-    SB_CK(sync());
+    SB_CK(cudaMemcpyAsync(pin, b.line[l.n_inner], 4 * m * 4, cudaMemcpyDeviceToHost, fs));
+    SB_CK(fsync());
     const uint32_t* w = reinterpret_cast<const uint32_t*>(pin);
     std::vector<QM31> v(m);
     for (size_t i = 0; i < m; ++i) v[i] = qmake(w[i], w[m + i], w[2 * m + i], w[3 * m + i]);
@@ -544,7 +555,7 @@ int32_t WideFibProver::prove(const ProveRequest& req, std::string& out, StageTim
     }
     ch.mix_felts(last_coeffs.data(), last_coeffs.size());
   }
-  SB_CK(cudaEventRecord(ev_[8], s));
+  SB_CK(cudaEventRecord(ev_[8], fs));
 
   // Proof of work on the device.
   uint64_t nonce = 0;
@@ -650,14 +661,14 @@ int32_t WideFibProver::prove(const ProveRequest& req, std::string& out, StageTim
          o_outh = (o_outw + out_words_bytes + 255) & ~255ull;
   std::memcpy(pin + o_items, words.data(), words_bytes);
   std::memcpy(pin + o_hitems, hashes.data(), hash_items_bytes);
-  SB_CK(cudaMemcpyAsync(b.scratch, pin, o_outw, cudaMemcpyHostToDevice, s));
+  SB_CK(cudaMemcpyAsync(b.scratch, pin, o_outw, cudaMemcpyHostToDevice, fs));
   SB_CK(gather_words(reinterpret_cast<GatherItem*>(b.scratch + o_items), (uint32_t)words.size(),
-                     reinterpret_cast<uint32_t*>(b.scratch + o_outw), s));
+                     reinterpret_cast<uint32_t*>(b.scratch + o_outw), fs));
   SB_CK(gather_hashes(reinterpret_cast<HashGatherItem*>(b.scratch + o_hitems), (uint32_t)hashes.size(),
-                      b.scratch + o_outh, s));
-  SB_CK(cudaMemcpyAsync(pin + o_outw, b.scratch + o_outw, o_outh - o_outw + out_hash_bytes, cudaMemcpyDeviceToHost, s));
-  SB_CK(cudaEventRecord(ev_[10], s));
-  SB_CK(sync());
+                      b.scratch + o_outh, fs));
+  SB_CK(cudaMemcpyAsync(pin + o_outw, b.scratch + o_outw, o_outh - o_outw + out_hash_bytes, cudaMemcpyDeviceToHost, fs));
+  SB_CK(cudaEventRecord(ev_[10], fs));
+  SB_CK(fsync());
   const uint32_t* gw = reinterpret_cast<const uint32_t*>(pin + o_outw);
   const uint8_t* gh = pin + o_outh;
 

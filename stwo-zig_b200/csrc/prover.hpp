@@ -73,6 +73,10 @@ class WideFibProver {
 
   Context* ctx_;
   cudaStream_t stream_;
+  // High-priority stream for the latency-bound chain after the composition commit (OODS,
+  // quotients, FRI layers with their root readbacks, decommitment): when several proofs
+  // share the device, its kernels are scheduled ahead of other proofs' bulk work.
+  cudaStream_t fast_ = nullptr;
   std::string err_;
   // workspace
   uint8_t* arena_ = nullptr;

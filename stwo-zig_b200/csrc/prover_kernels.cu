@@ -86,6 +86,106 @@ __global__ void __launch_bounds__(256) k_composition(uint32_t log_n, uint32_t W,
   }
 }
 
+// R consecutive rows per thread (RowVec<R>; R = 2 with 8-byte loads measured best:
+// more warps and more loads in flight than 4 rows with 16-byte loads), the column
+// loop unrolled by U (a multiple of 3: U loads in flight before their use, a
+// 64-bit fold per three terms) and each column's square computed once (it is b^2
+// of one constraint and a^2 of the next). Needs columns and output aligned to R
+// words (eval, stride, out, out_stride) and 2^(log_n+1) >= R.
+template <int R>
+struct RowVec;
+template <>
+struct RowVec<2> {
+  uint2 v;
+  __device__ __forceinline__ static RowVec load(const uint32_t* p) { return {__ldg(reinterpret_cast<const uint2*>(p))}; }
+  __device__ __forceinline__ static RowVec load_words(const uint32_t* p) { return {make_uint2(__ldg(p), __ldg(p + 1))}; }
+  __device__ __forceinline__ uint32_t operator[](int j) const { return j == 0 ? v.x : v.y; }
+  __device__ __forceinline__ static void store(uint32_t* p, const uint32_t* w) {
+    *reinterpret_cast<uint2*>(p) = make_uint2(w[0], w[1]);
+  }
+};
+  }
+  __device__ __forceinline__ uint32_t operator[](int j) const { return j == 0 ? v.x : j == 1 ? v.y : j == 2 ? v.z : v.w; }
+  __device__ __forceinline__ static void store(uint32_t* p, const uint32_t* w) {
+    *reinterpret_cast<uint4*>(p) = make_uint4(w[0], w[1], w[2], w[3]);
+  }
+};
+
+// Rows per thread and unroll depth of the vectorized composition and quotient kernels.
+constexpr int COMP_R = 2, COMP_U = 6, QUOT_R = 2, QUOT_U = 6;
+
+template <int R, int U>
+__global__ void __launch_bounds__(256, 4) k_composition_v(uint32_t log_n, uint32_t W, const uint32_t* __restrict__ eval,
+                                                          uint64_t stride, const QM31* __restrict__ coeffs,
+                                                          uint32_t den0, uint32_t den1, uint32_t* out,
+                                                          uint64_t out_stride) {
+  static_assert(U % 3 == 0, "fold every three terms");
+  using V = RowVec<R>;
+  extern __shared__ uint4 scq[];  // W-2 coefficients
+  const uint32_t n_cons = W - 2;
+  for (uint32_t i = threadIdx.x; i < n_cons; i += blockDim.x) {
+    QM31 c = coeffs[i];
+    scq[i] = make_uint4(c.c0.a, c.c0.b, c.c1.a, c.c1.b);
+  }
+  __syncthreads();
+  const uint32_t groups = (2u << log_n) / R;
+  for (uint32_t gi = blockIdx.x * blockDim.x + threadIdx.x; gi < groups; gi += gridDim.x * blockDim.x) {
+    const uint32_t row0 = gi * R;
+    const uint32_t* base = eval + row0;
+    V A = V::load(base), B = V::load(base + stride);
+    uint32_t sa[R], sb[R];
+#pragma unroll
+    for (int j = 0; j < R; ++j) { sa[j] = mmul(A[j], A[j]); sb[j] = mmul(B[j], B[j]); }
+    uint64_t acc[R][4];
+#pragma unroll
+    for (int j = 0; j < R; ++j)
+#pragma unroll
+      for (int c = 0; c < 4; ++c) acc[j][c] = 0;
+    auto step = [&](const V& C, const uint4& q) {
+#pragma unroll
+      for (int j = 0; j < R; ++j) {
+        uint32_t cj = C[j];
+        uint32_t cons = msub(cj, madd(sa[j], sb[j]));
+        sa[j] = sb[j];
+        sb[j] = mmul(cj, cj);
+        acc[j][0] += (uint64_t)q.x * cons;
+        acc[j][1] += (uint64_t)q.y * cons;
+        acc[j][2] += (uint64_t)q.z * cons;
+        acc[j][3] += (uint64_t)q.w * cons;
+      }
+    };
+    auto fold = [&]() {
+#pragma unroll
+      for (int j = 0; j < R; ++j)
+#pragma unroll
+        for (int c = 0; c < 4; ++c) acc[j][c] = mfold64(acc[j][c]);
+    };
+    uint32_t k = 0;
+    for (; k + U <= n_cons; k += U) {
+      V C[U];
+#pragma unroll
+      for (int u = 0; u < U; ++u) C[u] = V::load(base + (uint64_t)(k + 2 + u) * stride);
+#pragma unroll
+      for (int u = 0; u < U; ++u) {
+        step(C[u], scq[k + u]);
+        if (u % 3 == 2) fold();
+      }
+    }
+    for (uint32_t t = 0; k < n_cons; ++k, ++t) {
+      step(V::load(base + (uint64_t)(k + 2) * stride), scq[k]);
+      if (t % 3 == 2) fold();
+    }
+    const uint32_t d = (row0 >> log_n) ? den1 : den0;  // the R rows share row >> log_n
+#pragma unroll
+    for (int c = 0; c < 4; ++c) {
+      uint32_t w[R];
+#pragma unroll
+      for (int j = 0; j < R; ++j) w[j] = mmul(mreduce64(acc[j][c]), d);
+      V::store(out + (uint64_t)c * out_stride + row0, w);
+    }
+  }
+}
+
 // ---------------------------------------------------------------------------
 // OODS evaluation (src/prover/poly/circle/poly.zig:62-230): value = sum_j c_j *
 // prod_{bit b of j} F_b with F_0 = y, F_1 = x, F_b = pi^{b-1}(x). A CTA reduces
@@ -105,12 +205,24 @@ __device__ QM31 subset_product(const OodsFactors& F, uint32_t bits, uint32_t fir
   return r;
 }
 
+// A CTA owns one column and a strided set of its 4096-coefficient chunks. Thread t
+// sums its 16 coefficients of a chunk against the subset products of F_0..F_3,
+// multiplies by the chunk's product of F_12.. (a table built in shared memory by
+// doubling) and accumulates; at the end it multiplies by its own factor (F_4..F_11
+// subset selected by t) and the CTA reduces with warp shuffles to one partial.
+constexpr uint32_t OODS_SMEM_CHUNKS = 1024;  // hi-factor table entries kept in shared memory
+
+__device__ __forceinline__ QM31 shfl_down_q(QM31 v, int d) {
+  return qmake(__shfl_down_sync(0xffffffffu, v.c0.a, d), __shfl_down_sync(0xffffffffu, v.c0.b, d),
+               __shfl_down_sync(0xffffffffu, v.c1.a, d), __shfl_down_sync(0xffffffffu, v.c1.b, d));
+}
+
 __global__ void __launch_bounds__(OODS_THREADS) k_oods_chunks(OodsFactors F, const uint32_t* __restrict__ coeffs,
                                                               uint64_t stride, QM31* partial, uint32_t n_chunks) {
   __shared__ QM31 b4[3][16];
-  __shared__ QM31 s1[OODS_THREADS];
-  __shared__ QM31 s2[16];
-  const uint32_t chunk = blockIdx.x, col = blockIdx.y;
+  __shared__ QM31 hi[OODS_SMEM_CHUNKS];
+  __shared__ QM31 wsum[OODS_THREADS / 32];
+  const uint32_t col = blockIdx.y;
   const uint32_t L = F.log_size;
   const uint32_t chunk_bits = L < OODS_CHUNK_BITS ? L : OODS_CHUNK_BITS;
   if (threadIdx.x < 48) {
@@ -120,22 +232,34 @@ __global__ void __launch_bounds__(OODS_THREADS) k_oods_chunks(OodsFactors F, con
     uint32_t valid_bits = first >= chunk_bits ? 0 : (chunk_bits - first >= 4 ? 4 : chunk_bits - first);
     b4[lvl][r] = (r >> valid_bits) ? qzero() : subset_product(F, r, first);
   }
+  // hi[c] = prod of F[chunk_bits + b] over the set bits b of c, by doubling.
+  const uint32_t n_tab = n_chunks < OODS_SMEM_CHUNKS ? n_chunks : OODS_SMEM_CHUNKS;
+  if (threadIdx.x == 0) hi[0] = qone();
   __syncthreads();
+  for (uint32_t half = 1, b = 0; half < n_tab; half <<= 1, ++b) {
+    for (uint32_t i = threadIdx.x; i < half; i += blockDim.x) hi[half + i] = qmul(hi[i], F.f[chunk_bits + b]);
+    __syncthreads();
+  }
   const uint32_t n_in = 1u << chunk_bits;
-  const uint32_t* c = coeffs + col * stride + ((uint64_t)chunk << chunk_bits);
-  // level 0: thread t sums coefficients 16t .. 16t+15
-  QM31 v = qzero();
-  if (16 * threadIdx.x < n_in) {
-    uint64_t a0 = 0, a1 = 0, a2 = 0, a3 = 0;
-    const uint4* c4 = reinterpret_cast<const uint4*>(c + 16 * threadIdx.x);
+  const uint32_t t = threadIdx.x;
+  const bool active = 16 * t < n_in;
+  const uint32_t nw = active ? (n_in - 16 * t < 16 ? n_in - 16 * t : 16) : 0;
+  QM31 acc = qzero();
+  for (uint32_t chunk = blockIdx.x; chunk < n_chunks; chunk += gridDim.x) {
+    if (!active) break;
+    const uint32_t* c = coeffs + col * stride + ((uint64_t)chunk << chunk_bits) + 16 * t;
     uint32_t w[16];
-    uint32_t nw = n_in - 16 * threadIdx.x < 16 ? n_in - 16 * threadIdx.x : 16;
     if (nw == 16) {
+      const uint4* c4 = reinterpret_cast<const uint4*>(c);
 #pragma unroll
-      for (int q = 0; q < 4; ++q) { uint4 x = __ldg(c4 + q); w[4 * q] = x.x; w[4 * q + 1] = x.y; w[4 * q + 2] = x.z; w[4 * q + 3] = x.w; }
+      for (int q = 0; q < 4; ++q) {
+        uint4 x = __ldg(c4 + q);
+        w[4 * q] = x.x; w[4 * q + 1] = x.y; w[4 * q + 2] = x.z; w[4 * q + 3] = x.w;
+      }
     } else {
-      for (uint32_t r = 0; r < 16; ++r) w[r] = r < nw ? c[16 * threadIdx.x + r] : 0u;
+      for (uint32_t r = 0; r < 16; ++r) w[r] = r < nw ? c[r] : 0u;
     }
+    uint64_t a0 = 0, a1 = 0, a2 = 0, a3 = 0;
 #pragma unroll
     for (int r = 0; r < 16; ++r) {
       QM31 bb = b4[0][r];
@@ -143,25 +267,28 @@ __global__ void __launch_bounds__(OODS_THREADS) k_oods_chunks(OodsFactors F, con
       a2 += (uint64_t)bb.c1.a * w[r]; a3 += (uint64_t)bb.c1.b * w[r];
       if (r % 3 == 2) { a0 = mfold64(a0); a1 = mfold64(a1); a2 = mfold64(a2); a3 = mfold64(a3); }
     }
-    v = qmake(mreduce64(a0), mreduce64(a1), mreduce64(a2), mreduce64(a3));
+    QM31 v = qmake(mreduce64(a0), mreduce64(a1), mreduce64(a2), mreduce64(a3));
+    QM31 h;
+    if (chunk < OODS_SMEM_CHUNKS) {
+      h = hi[chunk];
+    } else {  // chunks beyond the table: low bits from the table, the rest multiplied in
+      h = hi[chunk & (OODS_SMEM_CHUNKS - 1)];
+      uint32_t bits = chunk >> 10;
+      for (uint32_t b = 10; bits; ++b, bits >>= 1)
+        if (bits & 1) h = qmul(h, F.f[chunk_bits + b]);
+    }
+    acc = qadd(acc, qmul(v, h));
   }
-  s1[threadIdx.x] = v;
+  // own factor: subset of F_4..F_7 by bits 0-3 of t, of F_8..F_11 by bits 4-7
+  acc = qmul(acc, qmul(b4[1][t & 15], b4[2][t >> 4]));
+#pragma unroll
+  for (int d = 16; d >= 1; d >>= 1) acc = qadd(acc, shfl_down_q(acc, d));
+  if ((t & 31) == 0) wsum[t >> 5] = acc;
   __syncthreads();
-  if (threadIdx.x < 16) {
-    QM31 acc = qzero();
-    for (int r = 0; r < 16; ++r) acc = qadd(acc, qmul(s1[16 * threadIdx.x + r], b4[1][r]));
-    s2[threadIdx.x] = acc;
-  }
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    QM31 acc = qzero();
-    for (int r = 0; r < 16; ++r) acc = qadd(acc, qmul(s2[r], b4[2][r]));
-    // chunk index bits b correspond to factors chunk_bits + b
-    QM31 hi = qone();
-    uint32_t bits = chunk;
-    for (uint32_t b = 0; bits; ++b, bits >>= 1)
-      if (bits & 1) hi = qmul(hi, F.f[chunk_bits + b]);
-    partial[(uint64_t)col * n_chunks + chunk] = qmul(acc, hi);
+  if (t == 0) {
+    QM31 sum = qzero();
+    for (int i = 0; i < OODS_THREADS / 32; ++i) sum = qadd(sum, wsum[i]);
+    partial[(uint64_t)col * gridDim.x + blockIdx.x] = sum;
   }
 }
 
@@ -216,6 +343,129 @@ __global__ void __launch_bounds__(256) k_quotients(PointTable pts, uint32_t log_
     out[out_stride + row] = acc.c0.b;
     out[2 * out_stride + row] = acc.c1.a;
     out[3 * out_stride + row] = acc.c1.b;
+  }
+}
+
+// R consecutive rows per thread: 8- or 16-byte loads of every column, entries
+// unrolled by U (U loads in flight), and the R rows' denominators inverted
+// together (one CM31 inversion per R rows, Montgomery's trick; a zero product
+// falls back to per-row inversion so a zero denominator gives the same zero as
+// the one-row kernel). Needs an output aligned to R words and 2^log_size >= R; a
+// CTA that finds a column pointer off the vector alignment loads word by word.
+template <int R, int U>
+__global__ void __launch_bounds__(256, 3) k_quotients_v(PointTable pts, uint32_t log_size, uint32_t n_batches,
+                                                        const QuotientBatchDev* __restrict__ batches,
+                                                        const uint32_t* const* __restrict__ col_ptrs,
+                                                        const QM31* __restrict__ coeff_c, uint32_t* out,
+                                                        uint64_t out_stride) {
+  static_assert(U % 3 == 0, "fold every three terms");
+  using V = RowVec<R>;
+  extern __shared__ uint4 sqe[];  // QUOT_MAX_ENTRIES coefficients, then the column pointers
+  const uint32_t** sptr = reinterpret_cast<const uint32_t**>(sqe + QUOT_MAX_ENTRIES);
+  __shared__ int s_bad;
+  uint32_t n_entries = 0;
+  for (uint32_t b = 0; b < n_batches; ++b) n_entries = max(n_entries, batches[b].first + batches[b].count);
+  if (threadIdx.x == 0) s_bad = 0;
+  __syncthreads();
+  for (uint32_t i = threadIdx.x; i < n_entries; i += blockDim.x) {
+    QM31 c = coeff_c[i];
+    sqe[i] = make_uint4(c.c0.a, c.c0.b, c.c1.a, c.c1.b);
+    const uint32_t* p = col_ptrs[i];
+    sptr[i] = p;
+    if (reinterpret_cast<uintptr_t>(p) & (4 * R - 1)) s_bad = 1;
+  }
+  __syncthreads();
+  const bool aligned = !s_bad;
+  auto load = [&](const uint32_t* p) { return aligned ? V::load(p) : V::load_words(p); };
+  const uint32_t groups = (1u << log_size) / R;
+  const CircleDomain dom = canonic_domain(log_size);
+  for (uint32_t gi = blockIdx.x * blockDim.x + threadIdx.x; gi < groups; gi += gridDim.x * blockDim.x) {
+    const uint32_t row0 = gi * R;
+    PointM dp[R];
+#pragma unroll
+    for (int j = 0; j < R; ++j) dp[j] = pts.at(dom.index_at(bitrev(row0 + j, log_size)));
+    QM31 acc[R];
+#pragma unroll
+    for (int j = 0; j < R; ++j) acc[j] = qzero();
+    for (uint32_t b = 0; b < n_batches; ++b) {
+      const QuotientBatchDev bt = batches[b];
+      uint64_t a[R][4];
+#pragma unroll
+      for (int j = 0; j < R; ++j)
+#pragma unroll
+        for (int c = 0; c < 4; ++c) a[j][c] = 0;
+      auto step = [&](const V& v, const uint4& q) {
+#pragma unroll
+        for (int j = 0; j < R; ++j) {
+          uint32_t vj = v[j];
+          a[j][0] += (uint64_t)q.x * vj;
+          a[j][1] += (uint64_t)q.y * vj;
+          a[j][2] += (uint64_t)q.z * vj;
+          a[j][3] += (uint64_t)q.w * vj;
+        }
+      };
+      auto fold = [&]() {
+#pragma unroll
+        for (int j = 0; j < R; ++j)
+#pragma unroll
+          for (int c = 0; c < 4; ++c) a[j][c] = mfold64(a[j][c]);
+      };
+      uint32_t i = 0;
+      const uint32_t e0 = bt.first;
+      for (; i + U <= bt.count; i += U) {
+        V v[U];
+#pragma unroll
+        for (int u = 0; u < U; ++u) v[u] = load(sptr[e0 + i + u] + row0);
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+          step(v[u], sqe[e0 + i + u]);
+          if (u % 3 == 2) fold();
+        }
+      }
+      for (uint32_t t = 0; i < bt.count; ++i, ++t) {
+        step(load(sptr[e0 + i] + row0), sqe[e0 + i]);
+        if (t % 3 == 2) fold();
+      }
+      CM31 prx = bt.point.x.c0, pry = bt.point.y.c0, pix = bt.point.x.c1, piy = bt.point.y.c1;
+      CM31 den[R], pre[R];
+#pragma unroll
+      for (int j = 0; j < R; ++j) {
+        den[j] = csub(cmul(csub(prx, CM31{dp[j].x, 0}), piy), cmul(csub(pry, CM31{dp[j].y, 0}), pix));
+        pre[j] = j == 0 ? den[0] : cmul(pre[j - 1], den[j]);
+      }
+      CM31 inv[R];
+      if (pre[R - 1].a == 0 && pre[R - 1].b == 0) {
+#pragma unroll
+        for (int j = 0; j < R; ++j) inv[j] = cinv(den[j]);
+      } else {
+        CM31 t = cinv(pre[R - 1]);
+#pragma unroll
+        for (int j = R - 1; j >= 1; --j) {
+          inv[j] = cmul(t, pre[j - 1]);
+          t = cmul(t, den[j]);
+        }
+        inv[0] = t;
+      }
+#pragma unroll
+      for (int j = 0; j < R; ++j) {
+        QM31 num = qmake(mreduce64(a[j][0]), mreduce64(a[j][1]), mreduce64(a[j][2]), mreduce64(a[j][3]));
+        num = qsub(num, qadd(qmulm(bt.sum_a, dp[j].y), bt.sum_b));
+        acc[j] = qadd(acc[j], qmulc(num, inv[j]));
+      }
+    }
+    uint32_t w[R];
+#pragma unroll
+    for (int j = 0; j < R; ++j) w[j] = acc[j].c0.a;
+    V::store(out + row0, w);
+#pragma unroll
+    for (int j = 0; j < R; ++j) w[j] = acc[j].c0.b;
+    V::store(out + out_stride + row0, w);
+#pragma unroll
+    for (int j = 0; j < R; ++j) w[j] = acc[j].c1.a;
+    V::store(out + 2 * out_stride + row0, w);
+#pragma unroll
+    for (int j = 0; j < R; ++j) w[j] = acc[j].c1.b;
+    V::store(out + 3 * out_stride + row0, w);
   }
 }
 
@@ -297,8 +547,16 @@ cudaError_t wide_fib_composition(uint32_t log_n, uint32_t W, const uint32_t* eva
     cudaError_t e = cudaFuncSetAttribute(k_composition, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
   }
-  k_composition<<<grid_for(2ull << log_n, 256), 256, smem, stream>>>(log_n, W, eval, stride, coeffs_dev, den_inv0,
-                                                                     den_inv1, out, out_stride); note_launch();
+  const bool vec = ((reinterpret_cast<uintptr_t>(eval) | reinterpret_cast<uintptr_t>(out)) & (4 * COMP_R - 1)) == 0 &&
+                   stride % COMP_R == 0 && out_stride % COMP_R == 0 && (2ull << log_n) >= COMP_R;
+  if (vec) {
+    k_composition_v<COMP_R, COMP_U><<<grid_for(2ull << log_n, 256 * COMP_R), 256, smem, stream>>>(
+        log_n, W, eval, stride, coeffs_dev, den_inv0, den_inv1, out, out_stride);
+  } else {
+    k_composition<<<grid_for(2ull << log_n, 256), 256, smem, stream>>>(log_n, W, eval, stride, coeffs_dev, den_inv0,
+                                                                       den_inv1, out, out_stride);
+  }
+  note_launch();
   return cudaGetLastError();
 }
 
@@ -319,11 +577,15 @@ cudaError_t eval_at_point(const DeviceTables&, uint32_t log_size, uint32_t n_col
   }
   uint32_t chunk_bits = log_size < OODS_CHUNK_BITS ? log_size : OODS_CHUNK_BITS;
   uint32_t n_chunks = 1u << (log_size - chunk_bits);
-  dim3 grid(n_chunks, n_cols);
+  // About 8 CTAs per SM over all columns, never more CTAs per column than chunks.
+  uint32_t per_col = (148 * 8 + n_cols - 1) / n_cols;
+  if (per_col > n_chunks) per_col = n_chunks;
+  if (per_col < 1) per_col = 1;
+  dim3 grid(per_col, n_cols);
   k_oods_chunks<<<grid, OODS_THREADS, 0, stream>>>(F, coeffs, stride, partial, n_chunks); note_launch();
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return e;
-  k_oods_sum<<<(n_cols + 127) / 128, 128, 0, stream>>>(partial, n_chunks, n_cols, out); note_launch();
+  k_oods_sum<<<(n_cols + 127) / 128, 128, 0, stream>>>(partial, per_col, n_cols, out); note_launch();
   return cudaGetLastError();
 }
 
@@ -331,13 +593,22 @@ cudaError_t accumulate_quotients(const DeviceTables& t, uint32_t log_size, uint3
                                  const QuotientBatchDev* batches, const uint32_t* const* col_ptrs, const QM31* coeff_c,
                                  uint32_t* out, uint64_t out_stride, cudaStream_t stream) {
   size_t smem = QUOT_MAX_ENTRIES * 16;
-  static bool attr = false;
-  if (!attr) {
+  size_t smem_v = QUOT_MAX_ENTRIES * (16 + sizeof(void*));
+  static const bool attr = [&] {  // once per process (thread-safe static initialisation)
     cudaFuncSetAttribute(k_quotients, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    attr = true;
-  }
-  k_quotients<<<grid_for(1ull << log_size, 256), 256, smem, stream>>>(PointTable{t.points}, log_size, n_batches,
-                                                                      batches, col_ptrs, coeff_c, out, out_stride); note_launch();
+    cudaFuncSetAttribute(k_quotients_v<QUOT_R, QUOT_U>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_v);
+    return true;
+  }();
+  (void)attr;
+  const bool vec = (reinterpret_cast<uintptr_t>(out) & (4 * QUOT_R - 1)) == 0 && out_stride % QUOT_R == 0 &&
+                   (1ull << log_size) >= QUOT_R;
+  if (vec)
+    k_quotients_v<QUOT_R, QUOT_U><<<grid_for(1ull << log_size, 256 * QUOT_R), 256, smem_v, stream>>>(
+        PointTable{t.points}, log_size, n_batches, batches, col_ptrs, coeff_c, out, out_stride);
+  else
+    k_quotients<<<grid_for(1ull << log_size, 256), 256, smem, stream>>>(PointTable{t.points}, log_size, n_batches,
+                                                                        batches, col_ptrs, coeff_c, out, out_stride);
+  note_launch();
   return cudaGetLastError();
 }
 

@@ -96,6 +96,7 @@ _SIGS = {
     "stwo_b200_eval_at_point": [_vp, _u32, _u32, _vp, _u64, QM31C, QM31C, _vp, _vp],
     "stwo_b200_eval_at_point_noalloc": [_vp, _u32, _u32, _vp, _u64, QM31C, QM31C, _vp, _vp],
     "stwo_b200_merkle_commit": [_vp, _u32, _u32, _vp, _u64, _vp, _vp, _vp],
+    "stwo_b200_merkle_commit_lifted": [_vp, _u32, ctypes.POINTER(_vp), ctypes.POINTER(_u32), _vp, _vp, _vp],
     "stwo_b200_fold_circle_into_line": [_vp, _u32, _vp, _u64, QM31C, _vp, _u64, _i32, _vp],
     "stwo_b200_fold_line": [_vp, _u32, _vp, _u64, QM31C, _vp, _u64, _vp],
     "stwo_b200_accumulate_quotients": [_vp, _u32, _u32, _vp, _vp, QM31C, QM31C, QM31C, QM31C, _vp, _u64, _vp],
@@ -109,6 +110,7 @@ _SIGS = {
                               ctypes.POINTER(RequestStatsC)],
     "stwo_b200_server_snapshot_get": [_vp, ctypes.POINTER(ServerSnapshotC)],
     "stwo_b200_server_destroy": [_vp],
+    "stwo_b200_xor_lookup_trace": [_vp, _u32, _u64, _vp, _vp, _vp, _vp],
     "stwo_b200_batch_inverse": [_vp, _u32, _u64, _vp, _u64, _vp, _u64, _vp],
     "stwo_b200_logup_interaction": [_vp, _u32, _u32, ctypes.POINTER(LogupUseC), ctypes.POINTER(QM31C), QM31C,
                                     _u32, _u32, _vp, _u64, ctypes.POINTER(QM31C), _vp],
@@ -324,6 +326,15 @@ class Context:
                                             _stream(stream)))
         return root.raw
 
+    def merkle_commit_lifted(self, cols: list, layers, stream=None) -> bytes:
+        """Lifted Merkle commitment of device columns of mixed power-of-two lengths; returns the root."""
+        n = len(cols)
+        ptrs = (_vp * max(1, n))(*[_ptr(c) for c in cols])
+        logs = (_u32 * max(1, n))(*[int(c.numel()).bit_length() - 1 for c in cols])
+        root = ctypes.create_string_buffer(32)
+        _check(_lib.stwo_b200_merkle_commit_lifted(self._h, n, ptrs, logs, _ptr(layers), root, _stream(stream)))
+        return root.raw
+
     def fold_circle_into_line(self, src, dst, src_log: int, alpha, accumulate: bool = False, stream=None) -> None:
         _check(_lib.stwo_b200_fold_circle_into_line(self._h, src_log, _ptr(src), 1 << src_log, _qm(alpha), _ptr(dst),
                                                     1 << (src_log - 1), int(accumulate), _stream(stream)))
@@ -359,6 +370,11 @@ class Context:
         _check(_lib.stwo_b200_wide_fib_composition(self._h, log_n_rows, sequence_len, _ptr(eval_cols),
                                                    2 << log_n_rows, _ptr(coeffs), den0, den1, _ptr(out),
                                                    2 << log_n_rows, _stream(stream)))
+
+    def xor_lookup_trace(self, log_n: int, seed: int, main_cols, table, multiplicity, stream=None) -> None:
+        """Seeded u8 pairs (a, b), a ^ b, the 2^16-row XOR table and its multiplicities."""
+        _check(_lib.stwo_b200_xor_lookup_trace(self._h, log_n, seed, _ptr(main_cols), _ptr(table), _ptr(multiplicity),
+                                               _stream(stream)))
 
     def batch_inverse(self, src, dst, n: int, degree: int = 1, src_stride: int | None = None,
                       dst_stride: int | None = None, stream=None) -> None:

@@ -111,3 +111,43 @@ def test_logup_zero_denominator_and_bad_args(ctx):
     with pytest.raises(sb.StwoError) as e:
         ctx.logup_interaction(4, [dict(words=[1] * 9)], [[1, 0, 0, 0]] * 9, [5, 0, 0, 0], out)
     assert e.value.status == sb.E_INVALID
+
+
+@pytest.mark.parametrize("log_n", [12, 16, 20])
+def test_xor_lookup_interaction(ctx, log_n):
+    """The XOR-lookup AIR's interaction phase at serving shapes: trace and multiplicities, LogUp
+    columns of both components, their lifted commitment; the claimed sums cancel, and everything
+    equals the oracle (all of it at 2^12, the trace and multiplicities at every size)."""
+    import torch
+    seed = 1000 + log_n
+    rows = 1 << log_n
+    main = torch.empty(3 * rows, dtype=torch.int32, device="cuda")
+    table = torch.empty(3 * 65536, dtype=torch.int32, device="cuda")
+    mult = torch.empty(65536, dtype=torch.int32, device="cuda")
+    ctx.xor_lookup_trace(log_n, seed, main, table, mult)
+    o_main, o_table, o_mult = oracle.xor_lookup_trace(log_n, seed)
+    assert np.array_equal(_host(main).reshape(3, rows), o_main)
+    assert np.array_equal(_host(table).reshape(3, 65536), o_table)
+    assert np.array_equal(_host(mult), o_mult)
+    rng = np.random.default_rng(log_n)
+    alphas = [rng.integers(0, P, size=4).tolist() for _ in range(3)]
+    z = rng.integers(0, P, size=4).tolist()
+    inter_main = torch.empty(4 * rows, dtype=torch.int32, device="cuda")
+    inter_table = torch.empty(4 * 65536, dtype=torch.int32, device="cuda")
+    c_main = ctx.logup_interaction(log_n, [dict(words=[main[k * rows:(k + 1) * rows] for k in range(3)])], alphas, z,
+                                   inter_main)
+    c_table = ctx.logup_interaction(16, [dict(words=[table[k * 65536:(k + 1) * 65536] for k in range(3)],
+                                              multiplicity=mult, negate=True)], alphas, z, inter_table)
+    import verifier
+    assert verifier.qadd(verifier.qfrom(list(c_main)), verifier.qfrom(list(c_table))) == verifier.q(0)
+    cols = [inter_main[k * rows:(k + 1) * rows] for k in range(4)] + \
+           [inter_table[k * 65536:(k + 1) * 65536] for k in range(4)]
+    max_log = max(log_n, 16)
+    layers = torch.empty(((2 << max_log) - 1) * 32, dtype=torch.uint8, device="cuda")
+    root = ctx.merkle_commit_lifted(cols, layers)
+    if log_n == 12:
+        ref_m, _ = oracle.logup_interaction(log_n, [dict(words=list(o_main))], alphas, z)
+        ref_t, _ = oracle.logup_interaction(16, [dict(words=list(o_table), multiplicity=o_mult, negate=True)], alphas, z)
+        assert np.array_equal(_host(inter_main).reshape(1, 4, rows), ref_m)
+        assert np.array_equal(_host(inter_table).reshape(1, 4, 65536), ref_t)
+        assert root == oracle.merkle_root([*ref_m[0], *ref_t[0]])

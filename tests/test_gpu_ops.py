@@ -140,3 +140,39 @@ def test_bad_arguments_raise(ctx):
         ctx.interpolate(d, 40, 1, 16)
     with pytest.raises(stwo_b200.StwoError):
         ctx.fold_circle_into_line(d, d, 1, [1, 0, 0, 0])
+
+
+@pytest.mark.parametrize("logs", [[3], [4, 2, 4, 1, 3], [10, 9, 10, 8, 9, 10, 7, 10, 8, 10, 9, 10, 6, 10, 9, 10, 8],
+                                  [16] * 3 + [12] * 4 + [14] * 2, [20, 16, 16, 16], [1, 1, 2]])
+def test_lifted_merkle_mixed_sizes(ctx, logs):
+    # Mixed log sizes in one tree (the shape of src/tests/metal/backend/commitment_test.zig's
+    # lifted-root case), including columns given out of size order.
+    import torch
+    rng = np.random.default_rng(sum(logs))
+    cols = [rng.integers(0, 2**31 - 1, size=1 << lg, dtype=np.uint32) for lg in logs]
+    dev = [torch.from_numpy(c.view(np.int32)).cuda() for c in cols]
+    max_log = max(logs)
+    layers = torch.empty(((2 << max_log) - 1) * 32, dtype=torch.uint8, device="cuda")
+    root = ctx.merkle_commit_lifted(dev, layers)
+    assert root == oracle.merkle_root(cols)
+    ref_layers = oracle.merkle_layers(cols)
+    torch.cuda.synchronize()
+    got = layers.cpu().numpy()
+    at = 0
+    for lay in ref_layers:
+        n = lay.shape[0]
+        assert np.array_equal(got[at * 32:(at + n) * 32].reshape(n, 32), lay)
+        at += n
+
+
+def test_lifted_merkle_equals_uniform_commit(ctx):
+    import torch
+    rng = np.random.default_rng(77)
+    cols = rng.integers(0, 2**31 - 1, size=(7, 1 << 12), dtype=np.uint32)
+    dev = torch.from_numpy(cols.reshape(-1).view(np.int32)).cuda()
+    layers_a = torch.empty(((2 << 12) - 1) * 32, dtype=torch.uint8, device="cuda")
+    layers_b = torch.empty_like(layers_a)
+    ra = ctx.merkle_commit(dev, 12, 7, layers_a)
+    rb = ctx.merkle_commit_lifted([dev[i << 12:(i + 1) << 12] for i in range(7)], layers_b)
+    assert ra == rb
+    assert torch.equal(layers_a, layers_b)

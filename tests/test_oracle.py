@@ -218,3 +218,17 @@ def test_logup_zero_denominator():
     col = np.arange(16, dtype=np.uint32)
     with pytest.raises(oracle.DivisionByZero):
         oracle.logup_interaction(4, [dict(words=[col])], [[1, 0, 0, 0]], [5, 0, 0, 0])
+
+
+def test_xor_lookup_logup_sums_cancel():
+    # LogUp identity of the XOR lookup: sum over trace rows of 1/(z - f(a, b, a^b)) equals the sum
+    # over table rows of m/(z - f(row)), i.e. the two claimed sums add to zero.
+    main, table, mult = oracle.xor_lookup_trace(10, 3)
+    assert int(mult.sum()) == 1 << 10
+    alphas = [[1, 0, 0, 0], [77, 1, 2, 3], [5, 9, 11, 13]]
+    z = [123456, 7, 8, 9]
+    _, c_main = oracle.logup_interaction(10, [dict(words=list(main))], alphas, z, batch=1, order=1)
+    _, c_table = oracle.logup_interaction(16, [dict(words=list(table), multiplicity=mult, negate=True)], alphas, z,
+                                          batch=1, order=1)
+    total = verifier.qadd(verifier.qfrom([int(x) for x in c_main]), verifier.qfrom([int(x) for x in c_table]))
+    assert total == verifier.q(0)
