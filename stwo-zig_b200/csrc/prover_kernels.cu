@@ -104,12 +104,6 @@ struct RowVec<2> {
     *reinterpret_cast<uint2*>(p) = make_uint2(w[0], w[1]);
   }
 };
-  }
-  __device__ __forceinline__ uint32_t operator[](int j) const { return j == 0 ? v.x : j == 1 ? v.y : j == 2 ? v.z : v.w; }
-  __device__ __forceinline__ static void store(uint32_t* p, const uint32_t* w) {
-    *reinterpret_cast<uint4*>(p) = make_uint4(w[0], w[1], w[2], w[3]);
-  }
-};
 
 // Rows per thread and unroll depth of the vectorized composition and quotient kernels.
 constexpr int COMP_R = 2, COMP_U = 6, QUOT_R = 2, QUOT_U = 6;
