@@ -357,10 +357,15 @@ struct PowPrefix { uint32_t w[8]; };
 // Rounds are enqueued in nonce order on one stream; a round starts by leaving
 // at once when an earlier round already found a smaller nonce, and each thread
 // stops at its first valid nonce or once the best known nonce is below its own.
+// LOW32: for n_bits <= 32 the condition is that the low n_bits of the first hash
+// word are zero, so only that word is live and the compiler drops the last
+// round's work that only feeds the other words.
+template <bool LOW32>
 __global__ void __launch_bounds__(256) k_pow_round(PowPrefix pre, uint32_t n_bits, uint64_t base,
                                                    uint32_t per_thread, unsigned long long* found, uint32_t one) {
   const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
   uint64_t nonce = base + (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const uint32_t mask = n_bits >= 32 ? 0xffffffffu : (1u << n_bits) - 1u;
   unsigned long long best = *((volatile unsigned long long*)found);
   for (uint32_t k = 0; k < per_thread && nonce < best; ++k, nonce += stride) {
     uint32_t h[8];
@@ -372,7 +377,8 @@ __global__ void __launch_bounds__(256) k_pow_round(PowPrefix pre, uint32_t n_bit
 #pragma unroll
     for (int i = 10; i < 16; ++i) m[i] = 0;
     b2s_compress(h, m, 40, true, one);
-    if (ctz128(h[0], h[1], h[2], h[3]) >= n_bits) {
+    const bool ok = LOW32 ? (h[0] & mask) == 0 : ctz128(h[0], h[1], h[2], h[3]) >= n_bits;
+    if (ok) {
       atomicMin(found, (unsigned long long)nonce);
       return;
     }
@@ -390,8 +396,12 @@ cudaError_t pow_round(const uint32_t prefix_words[8], uint32_t n_bits, uint64_t 
   for (int i = 0; i < 8; ++i) pre.w[i] = prefix_words[i];
   // Eight waves of short CTAs (14 nonces per thread, ~0.1 ms each) rather than one
   // wave of long ones, so that other streams' work gets SMs between them.
-  k_pow_round<<<sm_count * 4 * 8, 256, 0, stream>>>(pre, n_bits, base, 14,
-                                                   reinterpret_cast<unsigned long long*>(result_dev), 1u); note_launch();
+  auto* res = reinterpret_cast<unsigned long long*>(result_dev);
+  if (n_bits <= 32)
+    k_pow_round<true><<<sm_count * 4 * 8, 256, 0, stream>>>(pre, n_bits, base, 14, res, 1u);
+  else
+    k_pow_round<false><<<sm_count * 4 * 8, 256, 0, stream>>>(pre, n_bits, base, 14, res, 1u);
+  note_launch();
   return cudaGetLastError();
 }
 
