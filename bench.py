@@ -504,31 +504,44 @@ def run_kernels128(args, ctx):
 
 
 def run_serve(args, ctx):
-    """Poisson arrivals (seeded) of wide-Fibonacci requests (log_n_rows 12..22, sequence_len
-    {16, 32, 100}) into the serving loop at each rate; latency = submit to proof bytes. The same
-    requests proved one at a time give the single-proof throughput they are compared with."""
-    import torch
+    """Poisson arrivals (seeded) into the serving loop at each rate: 70% wide-Fibonacci requests
+    (log_n_rows 12..22, sequence_len {16, 32, 100}) and 30% LogUp XOR-lookup requests (2^n lookups of
+    seeded u8 pairs, n 12..20, into the 2^16-row XOR table); latency = submit to proof bytes. The
+    same requests proved one at a time give the single-proof throughput they are compared with."""
+    import numpy as np
     import stwo_b200 as sb
     cfg = sb.PcsConfig.preset(args.preset)
     rates = [float(x) for x in args.rates.split(",")]
     results = []
     stmts = mixed_statements(4242, args.requests, 12, 22)
-    # single-proof path over the same requests
+    rng = np.random.default_rng(4243)
+    for r in stmts:  # 30% XOR lookups, n uniform in 12..20
+        r["xor"] = bool(rng.random() < 0.3)
+        if r["xor"]:
+            r["log_n"] = int(rng.integers(12, 21))
+
+    def single(r):
+        if r["xor"]:
+            return ctx.prove_logup_xor(r["log_n"], cfg, seed=r["trace_seed"], channel_seed=r["channel_seed"])
+        return ctx.prove_wide_fibonacci(sb.Statement(r["log_n"], r["W"]), cfg, trace_kind=sb.TRACE_SEEDED,
+                                        trace_seed=r["trace_seed"], channel_seed=r["channel_seed"])
+
+    def submit(srv, r):
+        if r["xor"]:
+            return srv.submit_xor(r["log_n"], cfg, seed=r["trace_seed"], channel_seed=r["channel_seed"])
+        return srv.submit(sb.Statement(r["log_n"], r["W"]), cfg, trace_kind=sb.TRACE_SEEDED,
+                          trace_seed=r["trace_seed"], channel_seed=r["channel_seed"])
+
     for r in stmts[:4]:
-        ctx.prove_wide_fibonacci(sb.Statement(r["log_n"], r["W"]), cfg, trace_kind=sb.TRACE_SEEDED,
-                                 trace_seed=r["trace_seed"], channel_seed=r["channel_seed"])
+        single(r)
     t0 = time.perf_counter()
-    alone = []
-    for r in stmts:
-        alone.append(ctx.prove_wide_fibonacci(sb.Statement(r["log_n"], r["W"]), cfg, trace_kind=sb.TRACE_SEEDED,
-                                              trace_seed=r["trace_seed"], channel_seed=r["channel_seed"]))
+    alone = [single(r) for r in stmts]
     single_s = time.perf_counter() - t0
     for rate in rates:
         with sb.Server(ctx, slots=args.slots, profile=2, persistent_workspaces=True) as srv:
-            for r in stmts[:args.slots]:  # warm the stream-ordered pool
-                srv.wait(srv.submit(sb.Statement(r["log_n"], r["W"]), cfg, trace_kind=sb.TRACE_SEEDED,
-                                    trace_seed=r["trace_seed"], channel_seed=r["channel_seed"]))
-            tickets, submit_t = [None] * len(stmts), [0.0] * len(stmts)
+            for r in stmts[:args.slots]:  # warm the slots
+                srv.wait(submit(srv, r))
+            tickets = [None] * len(stmts)
 
             def producer():
                 start = time.perf_counter()
@@ -538,9 +551,7 @@ def run_serve(args, ctx):
                     delay = start + at - time.perf_counter()
                     if delay > 0:
                         time.sleep(delay)
-                    submit_t[i] = time.perf_counter()
-                    tickets[i] = srv.submit(sb.Statement(r["log_n"], r["W"]), cfg, trace_kind=sb.TRACE_SEEDED,
-                                            trace_seed=r["trace_seed"], channel_seed=r["channel_seed"])
+                    tickets[i] = submit(srv, r)
             th = threading.Thread(target=producer)
             t_begin = time.perf_counter()
             th.start()
@@ -561,9 +572,11 @@ def run_serve(args, ctx):
     best = max(x["proofs_per_s"] for x in results)
     out = {"metric": "proofs/s and p50/p99 ms, serving loop under Poisson arrivals", "workload": "serve",
            "value": best, "unit": "proofs/s", "n_gpus": 1, "higher_is_better": True, "dtype": "u32",
-           "data": "synthetic: seeded traces, master seed 4242",
-           "config": {"workload": f"{len(stmts)} wide-Fibonacci requests, log_n_rows uniform 12..22, sequence_len "
-                                  "in {16, 32, 100}, Poisson arrivals", "protocol": args.preset,
+           "data": "synthetic: seeded traces, master seeds 4242/4243",
+           "config": {"workload": f"{len(stmts)} requests, Poisson arrivals: 70% wide-Fibonacci (log_n_rows 12..22, "
+                                  "sequence_len {16, 32, 100}), 30% LogUp XOR lookups (2^12..2^20 u8 pairs into a "
+                                  "2^16-row table)", "protocol": args.preset,
+                      "xor_requests": sum(r["xor"] for r in stmts),
                       "slots": args.slots, "profile": "extreme", "workspaces": "persistent per slot"},
            "rates": results,
            "single": {"proofs_per_s": len(stmts) / single_s, "wall_ms": 1e3 * single_s},

@@ -118,6 +118,25 @@ int32_t stwo_b200_prove_wide_fibonacci_batch(stwo_b200_context* ctx, const stwo_
                                              size_t* proof_lens, int32_t* statuses, uint32_t max_in_flight,
                                              stwo_b200_stage_times* times);
 
+/* LogUp XOR-lookup AIR request: 2^log_n lookups of seeded w-bit operand pairs (w = log_table / 2;
+ * log_table 16 for u8 pairs, 8 for 4-bit pairs) into the 2^log_table-row XOR table. No reference
+ * AIR exists; the proof uses the reference's PCS, FRI, channel and wire layout with four trees
+ * (preprocessed table and selector, main trace and multiplicities, LogUp interaction, composition)
+ * and the two LogUp claimed sums, which the verifier requires to cancel. */
+typedef struct {
+  uint32_t log_n;
+  uint32_t log_table;
+  stwo_b200_pcs_config config;
+  uint64_t seed;
+  uint32_t has_channel_seed;
+  uint32_t reserved;
+  uint64_t channel_seed;
+} stwo_b200_xor_request;
+
+/* Proves the LogUp XOR-lookup AIR; proof bytes as for stwo_b200_prove_wide_fibonacci. */
+int32_t stwo_b200_prove_logup_xor(stwo_b200_context* ctx, const stwo_b200_xor_request* req, uint8_t* proof_out,
+                                  size_t proof_cap, size_t* proof_len);
+
 /* ---- Serving loop ------------------------------------------------------------------------------- */
 
 /* Continuous batching of wide-Fibonacci proofs on one device: `slots` proofs in flight (each a host
@@ -155,6 +174,8 @@ int32_t stwo_b200_server_create(stwo_b200_context* ctx, const stwo_b200_server_c
                                 stwo_b200_server** out);
 /* Queues a request and returns at once; host/device trace buffers must stay valid until wait returns. */
 int32_t stwo_b200_server_submit(stwo_b200_server* server, const stwo_b200_wide_fib_request* req, uint64_t* ticket);
+/* Queues a LogUp XOR-lookup AIR request (committed cells: 16 columns of 2^max(log_n, log_table) rows). */
+int32_t stwo_b200_server_submit_xor(stwo_b200_server* server, const stwo_b200_xor_request* req, uint64_t* ticket);
 /* Blocks until the request is done and returns its status; STWO_B200_E_BUFFER_TOO_SMALL sets
  * *proof_len and keeps the result for another call. */
 int32_t stwo_b200_server_wait(stwo_b200_server* server, uint64_t ticket, uint8_t* proof_out, size_t proof_cap,

@@ -309,7 +309,20 @@ def verify_wide_fib(proof_bytes: bytes, log_n_rows: int, sequence_len: int, chan
 
     ch.mix_felts(main + comp)
     quot_coeff = ch.draw_secure_felt()
-    L = n + B  # lifting log size
+    # one batch at the OODS point: every column's sample, powers 1, q, q^2, ... in column order
+    rp = q(1)
+    entries = []
+    for c, v in enumerate(main + comp):
+        entries.append((c, v, rp))
+        rp = qmul(rp, quot_coeff)
+    return _verify_pcs_tail(pr, ch, roots, [0, W, 8], [(oods, entries)], n + B, B, pow_bits, log_last, n_queries)
+
+
+def _verify_pcs_tail(pr, ch, roots, tree_cols, batches, L, B, pow_bits, log_last, n_queries):
+    """FRI commitments and alphas, last layer, proof of work, queries, the trees' Merkle
+    decommitments and the FRI decommitment, for a proof whose trees hold tree_cols[t] columns on
+    the lifting domain of log size L. batches: [(point, [(flat column, value, random power)])]
+    (src/core/pcs/quotients/fri_answers.zig, src/core/fri.zig)."""
     fri = pr["fri_proof"]
     ch.mix_root(bytes(fri["first_layer"]["commitment"]))
     alphas = [ch.draw_secure_felt()]
@@ -338,38 +351,45 @@ def verify_wide_fib(proof_bytes: bytes, log_n_rows: int, sequence_len: int, chan
 
     qv = pr["queried_values"]
     dec = pr["decommitments"]
-    if len(qv) != 3 or len(dec) != 3 or qv[0] or dec[0]["hash_witness"]:
-        raise VerificationError("preprocessed tree shape")
-    for t_idx, ncols in ((1, W), (2, 8)):
-        cols = qv[t_idx]
-        if len(cols) != ncols or any(len(c) != len(queries) for c in cols):
+    if len(qv) != len(tree_cols) or len(dec) != len(tree_cols):
+        raise VerificationError("number of trees")
+    cols = []
+    for t_idx, ncols in enumerate(tree_cols):
+        tcols = qv[t_idx]
+        if len(tcols) != ncols or any(len(c) != len(queries) for c in tcols):
             raise VerificationError("queried values shape")
-        merkle_verify(roots[t_idx], L, queries, cols, [bytes(h) for h in dec[t_idx]["hash_witness"]])
+        if ncols == 0:
+            if dec[t_idx]["hash_witness"]:
+                raise VerificationError("preprocessed tree shape")
+            continue
+        merkle_verify(roots[t_idx], L, queries, tcols, [bytes(h) for h in dec[t_idx]["hash_witness"]])
+        cols.extend(tcols)
 
-    # quotient answers at the queries (src/core/pcs/quotients/fri_answers.zig)
-    vals = main + comp
-    cols = qv[1] + qv[2]
-    rp = q(1)
-    lc = []
-    cy = qsub(qconj(oods[1]), oods[1])
-    sum_a, sum_b = q(0), q(0)
-    for v in vals:
-        aa = qsub(qconj(v), v)
-        bb = qsub(qmul(v, cy), qmul(aa, oods[1]))
-        lc.append(qmul(rp, cy))
-        sum_a = qadd(sum_a, qmul(rp, aa))
-        sum_b = qadd(sum_b, qmul(rp, bb))
-        rp = qmul(rp, quot_coeff)
-    prx, pry, pix, piy = oods[0][0], oods[1][0], oods[0][1], oods[1][1]
+    # quotient answers at the queries (src/core/pcs/quotients/fri_answers.zig, row_evaluation.zig)
+    consts = []
+    for point, entries in batches:
+        cy = qsub(qconj(point[1]), point[1])
+        sum_a, sum_b, lc = q(0), q(0), []
+        for c, v, rp in entries:
+            aa = qsub(qconj(v), v)
+            bb = qsub(qmul(v, cy), qmul(aa, point[1]))
+            lc.append((c, qmul(rp, cy)))
+            sum_a = qadd(sum_a, qmul(rp, aa))
+            sum_b = qadd(sum_b, qmul(rp, bb))
+        consts.append((point, lc, sum_a, sum_b))
     answers = []
     for j, pos in enumerate(queries):
         x, y = index_point(domain_index(L, bitrev(pos, L)))
-        num = q(0)
-        for c in range(len(vals)):
-            num = qadd(num, qmulm(lc[c], cols[c][j]))
-        num = qsub(num, qadd(qmulm(sum_a, y), sum_b))
-        den = csub(cmul(csub(prx, (x, 0)), piy), cmul(csub(pry, (y, 0)), pix))
-        answers.append(qmulc(num, cinv(den)))
+        acc = q(0)
+        for point, lc, sum_a, sum_b in consts:
+            num = q(0)
+            for c, coef in lc:
+                num = qadd(num, qmulm(coef, cols[c][j]))
+            num = qsub(num, qadd(qmulm(sum_a, y), sum_b))
+            prx, pry, pix, piy = point[0][0], point[1][0], point[0][1], point[1][1]
+            den = csub(cmul(csub(prx, (x, 0)), piy), cmul(csub(pry, (y, 0)), pix))
+            acc = qadd(acc, qmulc(num, cinv(den)))
+        answers.append(acc)
 
     # FRI decommitment (src/core/fri.zig:171-216, folding.zig:160-230)
     def layer_check(layer, qpos, qevals, log_size, fold):
@@ -445,3 +465,110 @@ def verify_wide_fib(proof_bytes: bytes, log_n_rows: int, sequence_len: int, chan
         if fold(coeffs, factors) != ev:
             raise VerificationError("last layer evaluation")
     return True
+
+
+def verify_logup_xor(proof_bytes: bytes, log_n: int, log_table: int = 16, channel_seed: int | None = None):
+    """Verifier of the LogUp XOR-lookup AIR proofs of the B200 prover (the AIR is described in
+    stwo-zig_b200/csrc/xor_prover.cu; it has no reference counterpart). Checks the transcript, the
+    cancellation of the two LogUp claimed sums, both LogUp transition constraints and the
+    composition at the OODS point, and the PCS / FRI decommitments."""
+    pr = json.loads(proof_bytes)
+    cfg = pr["config"]
+    fc = cfg["fri_config"]
+    pow_bits, B, log_last, n_queries = cfg["pow_bits"], fc["log_blowup_factor"], fc["log_last_layer_degree_bound"], \
+        fc["n_queries"]
+    if fc.get("fold_step", 1) != 1 or cfg.get("lifting_log_size") is not None:
+        raise VerificationError("unsupported config")
+    if pr["statement"] != {"log_n": log_n, "log_table": log_table}:
+        raise VerificationError("statement mismatch")
+    L = max(log_n, log_table)
+    N = 1 << L
+    roots = [bytes(c) for c in pr["commitments"]]
+    if len(roots) != 4:
+        raise VerificationError("expected 4 commitments")
+    ch = Channel()
+    ch.mix_felts([q(pow_bits, B, n_queries, log_last)])
+    ch.mix_root(roots[0])
+    ch.mix_root(roots[1])
+    ch.mix_u32s([log_n, log_table])
+    if channel_seed is not None:
+        ch.mix_u64(channel_seed)
+    z = ch.draw_secure_felt()
+    alpha = ch.draw_secure_felt()
+    alpha2 = qmul(alpha, alpha)
+    ch.mix_root(roots[2])
+    claimed = [qfrom(c) for c in pr["claimed_sums"]]
+    if len(claimed) != 2:
+        raise VerificationError("claimed sums")
+    ch.mix_felts(claimed)
+    if qadd(claimed[0], claimed[1]) != q(0):
+        raise VerificationError("LogUp claimed sums do not cancel")
+    random_coeff = ch.draw_secure_felt()
+    ch.mix_root(roots[3])
+    t = ch.draw_secure_felt()
+    t2 = qmul(t, t)
+    inv = qinv(qadd(t2, q(1)))
+    oods = (qmul(qsub(q(1), t2), inv), qmul(qadd(t, t), inv))
+    g = index_point(subgroup_gen(L))
+    prev = qpadd(oods, (q(g[0]), q(-g[1])))
+
+    sv = pr["sampled_values"]
+    if [len(x) for x in sv] != [4, 4, 8, 8] or any(len(c) != 1 for t_ in (0, 1, 3) for c in sv[t_]) or \
+            any(len(c) != 2 for c in sv[2]):
+        raise VerificationError("sampled values shape")
+    pre = [qfrom(c[0]) for c in sv[0]]
+    main = [qfrom(c[0]) for c in sv[1]]
+    inter_prev = [qfrom(c[0]) for c in sv[2]]
+    inter_cur = [qfrom(c[1]) for c in sv[2]]
+    comp = [qfrom(c[0]) for c in sv[3]]
+    basis = [q(1), q(0, 1), q(0, 0, 1), q(0, 0, 0, 1)]
+
+    def secure(vals):
+        r = q(0)
+        for k in range(4):
+            r = qadd(r, qmul(vals[k], basis[k]))
+        return r
+    left, right = secure(comp[:4]), secure(comp[4:])
+    pt = oods
+    for _ in range(L + 1 - 2):
+        pt = qpadd(pt, pt)
+    comp_eval = qadd(left, qmul(pt[0], right))
+    inv_n = pow(N, P - 2, P)
+    sm, sm_prev = secure(inter_cur[:4]), secure(inter_prev[:4])
+    st, st_prev = secure(inter_cur[4:]), secure(inter_prev[4:])
+    d_main = qsub(qadd(qadd(main[0], qmul(alpha, main[1])), qmul(alpha2, main[2])), z)
+    d_table = qsub(qadd(qadd(pre[0], qmul(alpha, pre[1])), qmul(alpha2, pre[2])), z)
+    c_main = qsub(qmul(qadd(qsub(sm, sm_prev), qmulm(claimed[0], inv_n)), d_main), pre[3])
+    c_table = qadd(qmul(qadd(qsub(st, st_prev), qmulm(claimed[1], inv_n)), d_table), main[3])
+    dinv = qinv(coset_vanishing_q(L, subgroup_gen(L + 1), subgroup_gen(L), oods))
+    if qmul(qadd(qmul(random_coeff, c_main), c_table), dinv) != comp_eval:
+        raise VerificationError("OODS mismatch")
+
+    flat = pre + main
+    for c in range(8):
+        flat += [inter_prev[c], inter_cur[c]]
+    flat += comp
+    ch.mix_felts(flat)
+    quot_coeff = ch.draw_secure_felt()
+    # samples with random powers over (tree, column, sample), a two-sample column's periodicity
+    # sample (at P, the lifting generator doubled to the column's log size being the identity)
+    # first; batches by point in order of first appearance: P, then P - g
+    rp = [q(1)]
+
+    def nxt():
+        r = rp[0]
+        rp[0] = qmul(r, quot_coeff)
+        return r
+    b_p, b_prev = [], []
+    for c in range(4):
+        b_p.append((c, pre[c], nxt()))
+    for c in range(4):
+        b_p.append((4 + c, main[c], nxt()))
+    for c in range(8):
+        b_p.append((8 + c, inter_cur[c], nxt()))
+        b_prev.append((8 + c, inter_prev[c], nxt()))
+        b_p.append((8 + c, inter_cur[c], nxt()))
+    for c in range(8):
+        b_p.append((16 + c, comp[c], nxt()))
+    return _verify_pcs_tail(pr, ch, roots, [4, 4, 8, 8], [(oods, b_p), (prev, b_prev)], L + B, B, pow_bits,
+                            log_last, n_queries)

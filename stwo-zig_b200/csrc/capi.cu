@@ -381,6 +381,32 @@ int32_t stwo_b200_pow_grind(stwo_b200_context* ctx, const uint8_t prefix_digest[
   return STWO_B200_OK;
 }
 
+int32_t stwo_b200_prove_logup_xor(stwo_b200_context* ctx, const stwo_b200_xor_request* req, uint8_t* proof_out,
+                                  size_t proof_cap, size_t* proof_len) {
+  CK_CTX(ctx);
+  if (!req || !proof_len) return set_error(STWO_B200_E_INVALID, "null argument");
+  sb::XorRequest r;
+  r.log_n = req->log_n;
+  r.log_table = req->log_table;
+  r.seed = req->seed;
+  r.config.pow_bits = req->config.pow_bits;
+  r.config.log_blowup_factor = req->config.log_blowup_factor;
+  r.config.log_last_layer_degree_bound = req->config.log_last_layer_degree_bound;
+  r.config.n_queries = req->config.n_queries;
+  r.has_channel_seed = req->has_channel_seed != 0;
+  r.channel_seed = req->channel_seed;
+  sb::LogupXorProver* p = ctx->ctx.acquire_xor();
+  std::string proof;
+  int32_t rc = p->prove(r, proof);
+  std::string err = p->error();
+  ctx->ctx.release_xor(p);
+  if (rc != STWO_B200_OK) return set_error(rc, err);
+  *proof_len = proof.size();
+  if (!proof_out || proof_cap < proof.size()) return set_error(STWO_B200_E_BUFFER_TOO_SMALL, "proof buffer too small");
+  std::memcpy(proof_out, proof.data(), proof.size());
+  return STWO_B200_OK;
+}
+
 struct stwo_b200_server {
   sb::Server* server;
   stwo_b200_context* ctx;
@@ -414,6 +440,23 @@ int32_t stwo_b200_server_submit(stwo_b200_server* server, const stwo_b200_wide_f
   if (!server || !req || !ticket) return set_error(STWO_B200_E_INVALID, "null server argument");
   std::string err;
   int32_t rc = server->server->submit(to_request(*req), ticket, &err);
+  return rc == STWO_B200_OK ? rc : set_error(rc, err);
+}
+
+int32_t stwo_b200_server_submit_xor(stwo_b200_server* server, const stwo_b200_xor_request* req, uint64_t* ticket) {
+  if (!server || !req || !ticket) return set_error(STWO_B200_E_INVALID, "null server argument");
+  sb::XorRequest r;
+  r.log_n = req->log_n;
+  r.log_table = req->log_table;
+  r.seed = req->seed;
+  r.config.pow_bits = req->config.pow_bits;
+  r.config.log_blowup_factor = req->config.log_blowup_factor;
+  r.config.log_last_layer_degree_bound = req->config.log_last_layer_degree_bound;
+  r.config.n_queries = req->config.n_queries;
+  r.has_channel_seed = req->has_channel_seed != 0;
+  r.channel_seed = req->channel_seed;
+  std::string err;
+  int32_t rc = server->server->submit_xor(r, ticket, &err);
   return rc == STWO_B200_OK ? rc : set_error(rc, err);
 }
 

@@ -15,125 +15,11 @@
 
 #include "blake2s.cuh"
 #include "prover.hpp"
+#include "prover_common.hpp"
 
 namespace sb {
 
-// ---------------------------------------------------------------------------
-// Host Blake2s channel (src/core/channel/blake2s.zig:33-280).
-// ---------------------------------------------------------------------------
 namespace {
-
-struct Channel {
-  uint8_t digest[32] = {0};
-  uint32_t n_draws = 0;
-  void set(const uint8_t d[32]) { std::memcpy(digest, d, 32); n_draws = 0; }
-  void mix_words(const uint32_t* w, size_t n) {
-    Blake2sHost h;
-    h.update(digest, 32);
-    if (n) h.update(w, n * 4);
-    uint8_t o[32];
-    h.finalize(o);
-    set(o);
-  }
-  void mix_felts(const QM31* f, size_t n) {
-    std::vector<uint32_t> w(4 * n);
-    for (size_t i = 0; i < n; ++i) qstore4(f[i], &w[4 * i]);
-    mix_words(w.data(), w.size());
-  }
-  void mix_u64(uint64_t v) { uint32_t w[2] = {(uint32_t)v, (uint32_t)(v >> 32)}; mix_words(w, 2); }
-  void mix_root(const uint8_t root[32]) {  // src/core/vcs_lifted/blake2_merkle.zig:236-247
-    Blake2sHost h;
-    h.update(digest, 32);
-    h.update(root, 32);
-    uint8_t o[32];
-    h.finalize(o);
-    set(o);
-  }
-  void draw_u32s(uint32_t out[8]) {
-    uint8_t in[37];
-    std::memcpy(in, digest, 32);
-    std::memcpy(in + 32, &n_draws, 4);
-    in[36] = 0;
-    n_draws += 1;
-    Blake2sHost h;
-    h.update(in, 37);
-    uint8_t o[32];
-    h.finalize(o);
-    std::memcpy(out, o, 32);
-  }
-  QM31 draw_secure_felt() {
-    for (;;) {
-      uint32_t w[8];
-      draw_u32s(w);
-      bool ok = true;
-      for (uint32_t x : w) if (x >= 2 * P) ok = false;
-      if (!ok) continue;
-      for (uint32_t& x : w) x = mreduce64(x);
-      return qmake(w[0], w[1], w[2], w[3]);
-    }
-  }
-};
-
-// randomSecureFieldPoint (src/core/circle.zig:159-167).
-PointQ random_secure_point(Channel& ch) {
-  QM31 t = ch.draw_secure_felt();
-  QM31 t2 = qsq(t);
-  QM31 inv = qinv(qadd(t2, qone()));
-  return {qmul(qsub(qone(), t2), inv), qmul(qadd(t, t), inv)};
-}
-
-// cosetVanishing (src/core/constraints.zig:17-27) on base and secure points.
-uint32_t coset_vanishing_m(const PointTable& pt, const Coset& c, PointM p) {
-  PointM q = padd(padd(p, pconj(pt.at(c.initial))), pt.at(c.step / 2));
-  uint32_t x = q.x;
-  for (uint32_t i = 1; i < c.log_size; ++i) x = double_x(x);
-  return x;
-}
-
-const PointTable& host_points() {
-  static std::vector<PointM> t = build_point_table();
-  static PointTable pt{t.data()};
-  return pt;
-}
-
-struct Json {
-  std::string s;
-  void u(uint64_t v) { s += std::to_string(v); }
-  void hash(const uint8_t* h) { s += '['; for (int i = 0; i < 32; ++i) { if (i) s += ','; u(h[i]); } s += ']'; }
-  void qm(QM31 q) { uint32_t w[4]; qstore4(q, w); s += '['; for (int i = 0; i < 4; ++i) { if (i) s += ','; u(w[i]); } s += ']'; }
-};
-
-// Decommitment plan of a lifted tree at sorted unique leaf positions: the nodes
-// whose hashes are witnesses, in proof order (src/prover/vcs_lifted/decommit.zig:154-230).
-std::vector<uint64_t> witness_nodes(uint32_t max_log, const std::vector<uint64_t>& positions) {
-  std::vector<uint64_t> out, prev = positions, cur;
-  for (int layer = (int)max_log - 1; layer >= 0; --layer) {
-    cur.clear();
-    size_t q = 0;
-    while (q < prev.size()) {
-      uint64_t first = prev[q];
-      bool sib = q + 1 < prev.size() && (first ^ 1) == prev[q + 1];
-      if (!sib) out.push_back(merkle_layer_offset(max_log, layer + 1) + (first ^ 1));
-      cur.push_back(first >> 1);
-      q += sib ? 2 : 1;
-    }
-    prev.swap(cur);
-  }
-  return out;
-}
-
-struct Arena {
-  uint8_t* base;
-  size_t off = 0, cap;
-  template <class T>
-  T* take(size_t count) {
-    off = (off + 255) & ~(size_t)255;
-    T* p = reinterpret_cast<T*>(base + off);
-    off += count * sizeof(T);
-    if (off > cap) throw std::runtime_error("arena overflow");
-    return p;
-  }
-};
 
 struct Layout {
   uint32_t n, W, B, L, CL, n_inner, last_log;
@@ -162,8 +48,6 @@ struct Buffers {
   uint8_t* scratch;  // gathers
   size_t scratch_bytes;
 };
-
-constexpr size_t GATHER_SCRATCH = 8 << 20;
 
 Buffers carve(Arena& a, const Layout& l) {
   Buffers b{};
@@ -214,6 +98,7 @@ size_t layout_bytes(const Layout& l) {
 // ---------------------------------------------------------------------------
 Context::~Context() {
   for (WideFibProver* p : pool) delete p;
+  for (LogupXorProver* p : xor_pool) delete p;
   if (tables.points) cudaFree(tables.points);
   if (tables.tw) cudaFree(tables.tw);
   if (tables.itw) cudaFree(tables.itw);
@@ -264,6 +149,24 @@ WideFibProver* Context::acquire() {
 void Context::release(WideFibProver* p) {
   std::lock_guard<std::mutex> g(mu);
   pool.push_back(p);
+}
+
+LogupXorProver* Context::acquire_xor() {
+  {
+    std::lock_guard<std::mutex> g(mu);
+    if (!xor_pool.empty()) {
+      LogupXorProver* p = xor_pool.back();
+      xor_pool.pop_back();
+      return p;
+    }
+  }
+  cudaSetDevice(device);
+  return new LogupXorProver(this);
+}
+
+void Context::release_xor(LogupXorProver* p) {
+  std::lock_guard<std::mutex> g(mu);
+  xor_pool.push_back(p);
 }
 
 // ---------------------------------------------------------------------------
@@ -487,190 +390,31 @@ int32_t WideFibProver::prove(const ProveRequest& req, std::string& out, StageTim
   SB_CK(accumulate_quotients(T, l.L, 1, b.batch, b.col_ptrs, b.quot_c, b.quot, l.NL, fs));
   SB_CK(cudaEventRecord(ev_[7], fs));
 
-  // FRI: first layer, then inner layers each committed before its fold.
-  std::vector<std::array<uint8_t, 32>> fri_roots;
+  // FRI, last layer, proof of work and queries.
+  FriBuffers fbuf{b.quot, b.tree_q, b.line, b.line_tree, b.pow_result};
+  FriResult fr;
   {
-    SB_CK(merkle_commit(l.L, 4, b.quot, l.NL, b.tree_q, fs));
-    SB_CK(cudaMemcpyAsync(pin, b.tree_q + (2 * l.NL - 2) * 32, 32, cudaMemcpyDeviceToHost, fs));
-    SB_CK(fsync());
-    std::array<uint8_t, 32> r;
-    std::memcpy(r.data(), pin, 32);
-    fri_roots.push_back(r);
-    ch.mix_root(r.data());
-    QM31 alpha = ch.draw_secure_felt();
-    // Each fold writes the next line layer and, unless it is the last layer,
-    // commits it in the same launch sequence.
-    SB_CK(fri_fold_commit(T, true, l.L, b.quot, l.NL, alpha, b.line[0], 1ull << (l.L - 1),
-                          l.n_inner > 0 ? b.line_tree[0] : nullptr, fs));
-    for (uint32_t k = 0; k < l.n_inner; ++k) {
-      uint32_t lg = l.L - 1 - k;
-      size_t sz = 1ull << lg;
-      SB_CK(cudaMemcpyAsync(pin, b.line_tree[k] + (2 * sz - 2) * 32, 32, cudaMemcpyDeviceToHost, fs));
-      SB_CK(fsync());
-      std::memcpy(r.data(), pin, 32);
-      fri_roots.push_back(r);
-      ch.mix_root(r.data());
-      QM31 a = ch.draw_secure_felt();
-      SB_CK(fri_fold_commit(T, false, lg, b.line[k], sz, a, b.line[k + 1], sz / 2,
-                            k + 1 < l.n_inner ? b.line_tree[k + 1] : nullptr, fs));
-    }
+    std::string ferr;
+    int32_t frc = fri_pow_queries(T, ctx_->sm_count, ch, cfg, l.L, l.n_inner, l.last_log, fbuf, pin, s, fs, ev_[8],
+                                  ev_[9], fr, ferr);
+    if (frc != OK) return fail(frc, ferr);
   }
-  // Last layer: line IFFT of 2^last_log values (src/backend/line_evaluation.zig:97-145).
-  std::vector<QM31> last_coeffs;
-  {
-    size_t m = 1ull << l.last_log;
-    SB_CK(cudaMemcpyAsync(pin, b.line[l.n_inner], 4 * m * 4, cudaMemcpyDeviceToHost, fs));
-    SB_CK(fsync());
-    const uint32_t* w = reinterpret_cast<const uint32_t*>(pin);
-    std::vector<QM31> v(m);
-    for (size_t i = 0; i < m; ++i) v[i] = qmake(w[i], w[m + i], w[2 * m + i], w[3 * m + i]);
-    auto brev = [&](std::vector<QM31>& x) {
-      uint32_t lg = l.last_log;
-      for (size_t i = 0; i < x.size(); ++i) { size_t j = bitrev((uint32_t)i, lg); if (j > i) std::swap(x[i], x[j]); }
-    };
-    brev(v);
-    const PointTable& pt = host_points();
-    Coset d = coset_half_odds(l.last_log);
-    while (d.log_size > 0) {
-      size_t chunk = 1ull << d.log_size, half = chunk / 2;
-      for (size_t st = 0; st < m; st += chunk)
-        for (size_t i = 0; i < half; ++i) {
-          uint32_t ix = minv(pt.at(d.index_at(i)).x);
-          QM31 a = v[st + i], c = v[st + half + i];
-          v[st + i] = qadd(a, c);
-          v[st + half + i] = qmulm(qsub(a, c), ix);
-        }
-      d = d.dbl();
-    }
-    uint32_t li = minv((uint32_t)(m % P));
-    for (QM31& x : v) x = qmulm(x, li);
-    brev(v);
-    size_t bound = 1ull << cfg.log_last_layer_degree_bound;
-    for (size_t i = bound; i < m; ++i)
-      if (!qiszero(v[i])) return fail(E_CONSTRAINTS, "last FRI layer exceeds its degree bound");
-    last_coeffs.assign(v.begin(), v.begin() + bound);
-    if (last_coeffs.size() > 1) {
-      uint32_t lg = 0; while ((1ull << lg) < last_coeffs.size()) ++lg;
-      for (size_t i = 0; i < last_coeffs.size(); ++i) { size_t j = bitrev((uint32_t)i, lg); if (j > i) std::swap(last_coeffs[i], last_coeffs[j]); }
-    }
-    ch.mix_felts(last_coeffs.data(), last_coeffs.size());
-  }
-  SB_CK(cudaEventRecord(ev_[8], fs));
+  const std::vector<uint64_t>& queries = fr.queries;
 
-  // Proof of work on the device.
-  uint64_t nonce = 0;
-  if (cfg.pow_bits > 0) {
-    uint8_t prefix[32];
-    {
-      Blake2sHost h;
-      uint32_t tag = 0x12345678u;
-      uint8_t z[12] = {0};
-      h.update(&tag, 4); h.update(z, 12); h.update(ch.digest, 32); h.update(&cfg.pow_bits, 4);
-      h.finalize(prefix);
-    }
-    uint32_t pw[8];
-    std::memcpy(pw, prefix, 32);
-    // Rounds of ~17M nonces, four per check; the search bound is 2^(bits+16) nonces.
-    const uint64_t max_nonce = cfg.pow_bits >= 48 ? ~0ull : (1ull << (cfg.pow_bits + 16));
-    const uint64_t per_round = pow_round_nonces(ctx_->sm_count);
-    SB_CK(cudaMemsetAsync(b.pow_result, 0xff, 8, s));
-    nonce = ~0ull;
-    for (uint64_t base = 0; base < max_nonce && nonce == ~0ull;) {
-      for (int r = 0; r < 4 && base < max_nonce; ++r, base += per_round)
-        SB_CK(pow_round(pw, cfg.pow_bits, base, b.pow_result, ctx_->sm_count, s));
-      SB_CK(cudaMemcpyAsync(pin, b.pow_result, 8, cudaMemcpyDeviceToHost, s));
-      SB_CK(sync());
-      std::memcpy(&nonce, pin, 8);
-    }
-    if (nonce == ~0ull) return fail(E_TIMEOUT, "proof-of-work search bound reached");
-  }
-  ch.mix_u64(nonce);
-  SB_CK(cudaEventRecord(ev_[9], s));
-
-  // Queries (src/core/queries.zig:8-60).
-  std::vector<uint64_t> queries;
+  // Decommitment: queried values and witnesses of the trace trees and the FRI layers.
+  DecommitPlan plan;
   {
-    uint32_t mask = (uint32_t)((1ull << l.L) - 1);
-    while (queries.size() < cfg.n_queries) {
-      uint32_t w[8];
-      ch.draw_u32s(w);
-      for (uint32_t x : w) { queries.push_back(x & mask); if (queries.size() == cfg.n_queries) break; }
-    }
-    std::sort(queries.begin(), queries.end());
-    queries.erase(std::unique(queries.begin(), queries.end()), queries.end());
+    std::vector<const uint32_t*> c1, c2;
+    for (uint32_t c = 0; c < W; ++c) c1.push_back(b.lde + (size_t)c * l.NL);
+    for (uint32_t c = 0; c < 8; ++c) c2.push_back(b.comp_lde + (size_t)c * l.NL);
+    plan.add_tree(nullptr, 0, {}, queries);  // preprocessed: empty
+    plan.add_tree(b.tree1, l.L, c1, queries);
+    plan.add_tree(b.tree2, l.L, c2, queries);
+    plan.add_fri(fbuf, l.L, l.n_inner, queries);
+    std::string gerr;
+    int32_t grc = plan.gather(b.scratch, b.scratch_bytes, pin, pinned_size_, fs, ev_[10], gerr);
+    if (grc != OK) return fail(grc, gerr);
   }
-
-  // Decommitment plan: gather words and hashes in one pass.
-  std::vector<GatherItem> words;
-  std::vector<HashGatherItem> hashes;
-  struct LayerPlan { size_t wit_word0, n_wit, hash0, n_hash; };
-  // trace trees
-  size_t q1_words = words.size();
-  for (uint32_t c = 0; c < W; ++c)
-    for (uint64_t q : queries) words.push_back({b.lde + (size_t)c * l.NL, q});
-  size_t q2_words = words.size();
-  for (uint32_t c = 0; c < 8; ++c)
-    for (uint64_t q : queries) words.push_back({b.comp_lde + (size_t)c * l.NL, q});
-  std::vector<uint64_t> wn1 = witness_nodes(l.L, queries);
-  size_t h1 = hashes.size();
-  for (uint64_t nd : wn1) hashes.push_back({b.tree1, nd});
-  size_t h2 = hashes.size();
-  for (uint64_t nd : wn1) hashes.push_back({b.tree2, nd});
-  // FRI layers
-  std::vector<LayerPlan> fplan;
-  std::vector<std::vector<uint64_t>> fpos;  // decommitment positions per layer
-  {
-    std::vector<uint64_t> lq = queries;
-    for (uint32_t k = 0; k <= l.n_inner; ++k) {
-      // k = 0: first layer (quotient column, log L); k >= 1: inner layer k-1.
-      const uint32_t* colbase = k == 0 ? b.quot : b.line[k - 1];
-      uint64_t csz = k == 0 ? l.NL : (1ull << (l.L - k));
-      uint32_t lg = k == 0 ? l.L : l.L - k;
-      const uint8_t* tree = k == 0 ? b.tree_q : b.line_tree[k - 1];
-      LayerPlan lp{words.size(), 0, hashes.size(), 0};
-      std::vector<uint64_t> positions;
-      size_t q = 0;
-      while (q < lq.size()) {
-        uint64_t key = lq[q] >> 1;
-        size_t end = q + 1;
-        while (end < lq.size() && (lq[end] >> 1) == key) ++end;
-        size_t at = q;
-        for (uint64_t pos = key << 1; pos < (key << 1) + 2; ++pos) {
-          positions.push_back(pos);
-          if (at < end && lq[at] == pos) { ++at; continue; }
-          for (int c = 0; c < 4; ++c) words.push_back({colbase + c * csz, pos});
-          lp.n_wit += 1;
-        }
-        q = end;
-      }
-      std::vector<uint64_t> wn = witness_nodes(lg, positions);
-      for (uint64_t nd : wn) hashes.push_back({tree, nd});
-      lp.n_hash = wn.size();
-      fplan.push_back(lp);
-      // fold queries
-      std::vector<uint64_t> nq;
-      for (uint64_t p : lq) { uint64_t f = p >> 1; if (nq.empty() || nq.back() != f) nq.push_back(f); }
-      lq.swap(nq);
-    }
-  }
-  size_t words_bytes = words.size() * sizeof(GatherItem), hash_items_bytes = hashes.size() * sizeof(HashGatherItem);
-  size_t out_words_bytes = words.size() * 4, out_hash_bytes = hashes.size() * 32;
-  size_t total = 4 * 256 + words_bytes + hash_items_bytes + out_words_bytes + out_hash_bytes;
-  if (total > b.scratch_bytes || total > pinned_size_) return fail(E_INVALID, "decommitment exceeds staging capacity");
-  size_t o_items = 0, o_hitems = (words_bytes + 255) & ~255ull, o_outw = (o_hitems + hash_items_bytes + 255) & ~255ull,
-         o_outh = (o_outw + out_words_bytes + 255) & ~255ull;
-  std::memcpy(pin + o_items, words.data(), words_bytes);
-  std::memcpy(pin + o_hitems, hashes.data(), hash_items_bytes);
-  SB_CK(cudaMemcpyAsync(b.scratch, pin, o_outw, cudaMemcpyHostToDevice, fs));
-  SB_CK(gather_words(reinterpret_cast<GatherItem*>(b.scratch + o_items), (uint32_t)words.size(),
-                     reinterpret_cast<uint32_t*>(b.scratch + o_outw), fs));
-  SB_CK(gather_hashes(reinterpret_cast<HashGatherItem*>(b.scratch + o_hitems), (uint32_t)hashes.size(),
-                      b.scratch + o_outh, fs));
-  SB_CK(cudaMemcpyAsync(pin + o_outw, b.scratch + o_outw, o_outh - o_outw + out_hash_bytes, cudaMemcpyDeviceToHost, fs));
-  SB_CK(cudaEventRecord(ev_[10], fs));
-  SB_CK(fsync());
-  const uint32_t* gw = reinterpret_cast<const uint32_t*>(pin + o_outw);
-  const uint8_t* gh = pin + o_outh;
 
   // Wire encoding (src/interop/proof_wire.zig:19-77).
   Json j;
@@ -685,47 +429,14 @@ int32_t WideFibProver::prove(const ProveRequest& req, std::string& out, StageTim
   for (uint32_t c = 0; c < W; ++c) { if (c) j.s += ','; j.s += '['; j.qm(sampled[c]); j.s += ']'; }
   j.s += "],[";
   for (uint32_t c = 0; c < 8; ++c) { if (c) j.s += ','; j.s += '['; j.qm(sampled[W + c]); j.s += ']'; }
-  auto hash_list = [&](size_t first, size_t count) {
-    j.s += '[';
-    for (size_t i = 0; i < count; ++i) { if (i) j.s += ','; j.hash(gh + (first + i) * 32); }
-    j.s += ']';
-  };
-  j.s += "]],\"decommitments\":[{\"hash_witness\":[]},{\"hash_witness\":";
-  hash_list(h1, wn1.size());
-  j.s += "},{\"hash_witness\":";
-  hash_list(h2, wn1.size());
-  j.s += "}],\"queried_values\":[[],[";
-  const size_t nqv = queries.size();
-  auto qv = [&](size_t first, uint32_t cols) {
-    for (uint32_t c = 0; c < cols; ++c) {
-      if (c) j.s += ',';
-      j.s += '[';
-      for (size_t q = 0; q < nqv; ++q) { if (q) j.s += ','; j.u(gw[first + c * nqv + q]); }
-      j.s += ']';
-    }
-  };
-  qv(q1_words, W);
-  j.s += "],[";
-  qv(q2_words, 8);
-  j.s += "]],\"proof_of_work\":"; j.u(nonce);
-  auto layer = [&](size_t k) {
-    const LayerPlan& lp = fplan[k];
-    j.s += "{\"fri_witness\":[";
-    for (size_t i = 0; i < lp.n_wit; ++i) {
-      if (i) j.s += ',';
-      const uint32_t* w = gw + lp.wit_word0 + 4 * i;
-      j.qm(qmake(w[0], w[1], w[2], w[3]));
-    }
-    j.s += "],\"decommitment\":{\"hash_witness\":";
-    hash_list(lp.hash0, lp.n_hash);
-    j.s += "},\"commitment\":"; j.hash(fri_roots[k].data()); j.s += '}';
-  };
-  j.s += ",\"fri_proof\":{\"first_layer\":"; layer(0);
-  j.s += ",\"inner_layers\":[";
-  for (uint32_t k = 1; k <= l.n_inner; ++k) { if (k > 1) j.s += ','; layer(k); }
-  j.s += "],\"last_layer_poly\":[";
-  for (size_t i = 0; i < last_coeffs.size(); ++i) { if (i) j.s += ','; j.qm(last_coeffs[i]); }
-  j.s += "]}}";
+  j.s += "]],\"decommitments\":[";
+  for (size_t t = 0; t < 3; ++t) { if (t) j.s += ','; j.s += "{\"hash_witness\":"; plan.json_witness(j, t); j.s += '}'; }
+  j.s += "],\"queried_values\":[";
+  for (size_t t = 0; t < 3; ++t) { if (t) j.s += ','; plan.json_queried(j, t); }
+  j.s += "],\"proof_of_work\":"; j.u(fr.nonce);
+  j.s += ",\"fri_proof\":";
+  plan.json_fri(j, fr);
+  j.s += '}';
 
   // Prover self-check of the composition OODS value (src/prover/prove.zig:366-386).
   {

@@ -88,12 +88,42 @@ class WideFibProver {
   cudaEvent_t ev_[12];
 };
 
+// LogUp XOR-lookup AIR request (xor_prover.cu): 2^log_n lookups of seeded w-bit pairs
+// (w = log_table / 2) into the 2^log_table-row XOR table.
+struct XorRequest {
+  uint32_t log_n = 0, log_table = 16;
+  uint64_t seed = 0;
+  PcsConfig config;
+  bool has_channel_seed = false;
+  uint64_t channel_seed = 0;
+};
+
+// Prover of the LogUp XOR-lookup AIR; its workspace comes from the stream-ordered pool per proof.
+class LogupXorProver {
+ public:
+  explicit LogupXorProver(Context* ctx);
+  ~LogupXorProver();
+  int32_t prove(const XorRequest& req, std::string& proof_json);
+  const std::string& error() const { return err_; }
+  // Device workspace of one proof of this shape (bytes); 0 for an impossible shape.
+  static size_t workspace_bytes(uint32_t log_n, uint32_t log_table, uint32_t log_blowup, uint32_t log_last_layer);
+
+ private:
+  static constexpr size_t PINNED_BYTES = (8 << 20) + (1 << 20);
+  int32_t fail(int32_t code, const std::string& msg) { err_ = msg; return code; }
+  Context* ctx_;
+  cudaStream_t stream_ = nullptr, fast_ = nullptr;
+  uint8_t* pinned_ = nullptr;
+  std::string err_;
+};
+
 struct Context {
   int device = 0;
   int sm_count = 0;
   DeviceTables tables;
   std::mutex mu;
   std::vector<WideFibProver*> pool;  // idle provers
+  std::vector<LogupXorProver*> xor_pool;
   cudaStream_t stream = nullptr;
   uint32_t* small = nullptr;  // 256 bytes of device scratch for single-value results (PoW nonce)
   std::mutex small_mu;
@@ -101,6 +131,8 @@ struct Context {
   int32_t init(int device, uint32_t tower_log);
   WideFibProver* acquire();
   void release(WideFibProver* p);
+  LogupXorProver* acquire_xor();
+  void release_xor(LogupXorProver* p);
 };
 
 const char* status_string(int32_t code);

@@ -1,0 +1,193 @@
+// Host-side pieces shared by the provers: the Blake2s channel, proof JSON
+// writer, Merkle witness plans, workspace arena, and the proof tail (FRI, last
+// layer, proof of work, queries, decommitment gathers) over a quotient column.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <array>
+#include <cstring>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "blake2s.cuh"
+#include "prover.hpp"
+
+namespace sb {
+
+// ---------------------------------------------------------------------------
+// Host Blake2s channel (src/core/channel/blake2s.zig:33-280).
+// ---------------------------------------------------------------------------
+struct Channel {
+  uint8_t digest[32] = {0};
+  uint32_t n_draws = 0;
+  void set(const uint8_t d[32]) { std::memcpy(digest, d, 32); n_draws = 0; }
+  void mix_words(const uint32_t* w, size_t n) {
+    Blake2sHost h;
+    h.update(digest, 32);
+    if (n) h.update(w, n * 4);
+    uint8_t o[32];
+    h.finalize(o);
+    set(o);
+  }
+  void mix_felts(const QM31* f, size_t n) {
+    std::vector<uint32_t> w(4 * n);
+    for (size_t i = 0; i < n; ++i) qstore4(f[i], &w[4 * i]);
+    mix_words(w.data(), w.size());
+  }
+  void mix_u64(uint64_t v) { uint32_t w[2] = {(uint32_t)v, (uint32_t)(v >> 32)}; mix_words(w, 2); }
+  void mix_root(const uint8_t root[32]) {  // src/core/vcs_lifted/blake2_merkle.zig:236-247
+    Blake2sHost h;
+    h.update(digest, 32);
+    h.update(root, 32);
+    uint8_t o[32];
+    h.finalize(o);
+    set(o);
+  }
+  void draw_u32s(uint32_t out[8]) {
+    uint8_t in[37];
+    std::memcpy(in, digest, 32);
+    std::memcpy(in + 32, &n_draws, 4);
+    in[36] = 0;
+    n_draws += 1;
+    Blake2sHost h;
+    h.update(in, 37);
+    uint8_t o[32];
+    h.finalize(o);
+    std::memcpy(out, o, 32);
+  }
+  QM31 draw_secure_felt() {
+    for (;;) {
+      uint32_t w[8];
+      draw_u32s(w);
+      bool ok = true;
+      for (uint32_t x : w) if (x >= 2 * P) ok = false;
+      if (!ok) continue;
+      for (uint32_t& x : w) x = mreduce64(x);
+      return qmake(w[0], w[1], w[2], w[3]);
+    }
+  }
+};
+
+// randomSecureFieldPoint (src/core/circle.zig:159-167).
+inline PointQ random_secure_point(Channel& ch) {
+  QM31 t = ch.draw_secure_felt();
+  QM31 t2 = qsq(t);
+  QM31 inv = qinv(qadd(t2, qone()));
+  return {qmul(qsub(qone(), t2), inv), qmul(qadd(t, t), inv)};
+}
+
+// cosetVanishing (src/core/constraints.zig:17-27) on base and secure points.
+inline uint32_t coset_vanishing_m(const PointTable& pt, const Coset& c, PointM p) {
+  PointM q = padd(padd(p, pconj(pt.at(c.initial))), pt.at(c.step / 2));
+  uint32_t x = q.x;
+  for (uint32_t i = 1; i < c.log_size; ++i) x = double_x(x);
+  return x;
+}
+
+inline const PointTable& host_points() {
+  static std::vector<PointM> t = build_point_table();
+  static PointTable pt{t.data()};
+  return pt;
+}
+
+struct Json {
+  std::string s;
+  void u(uint64_t v) { s += std::to_string(v); }
+  void hash(const uint8_t* h) { s += '['; for (int i = 0; i < 32; ++i) { if (i) s += ','; u(h[i]); } s += ']'; }
+  void qm(QM31 q) { uint32_t w[4]; qstore4(q, w); s += '['; for (int i = 0; i < 4; ++i) { if (i) s += ','; u(w[i]); } s += ']'; }
+};
+
+// Decommitment plan of a lifted tree at sorted unique leaf positions: the nodes
+// whose hashes are witnesses, in proof order (src/prover/vcs_lifted/decommit.zig:154-230).
+inline std::vector<uint64_t> witness_nodes(uint32_t max_log, const std::vector<uint64_t>& positions) {
+  std::vector<uint64_t> out, prev = positions, cur;
+  for (int layer = (int)max_log - 1; layer >= 0; --layer) {
+    cur.clear();
+    size_t q = 0;
+    while (q < prev.size()) {
+      uint64_t first = prev[q];
+      bool sib = q + 1 < prev.size() && (first ^ 1) == prev[q + 1];
+      if (!sib) out.push_back(merkle_layer_offset(max_log, layer + 1) + (first ^ 1));
+      cur.push_back(first >> 1);
+      q += sib ? 2 : 1;
+    }
+    prev.swap(cur);
+  }
+  return out;
+}
+
+struct Arena {
+  uint8_t* base;
+  size_t off = 0, cap;
+  template <class T>
+  T* take(size_t count) {
+    off = (off + 255) & ~(size_t)255;
+    T* p = reinterpret_cast<T*>(base + off);
+    off += count * sizeof(T);
+    if (off > cap) throw std::runtime_error("arena overflow");
+    return p;
+  }
+};
+
+
+constexpr size_t GATHER_SCRATCH = 8 << 20;
+
+// ---------------------------------------------------------------------------
+// Proof tail over a committed quotient column (src/prover/fri.zig:163-619,
+// src/prover/pcs/scheme.zig:633-799): FRI first layer and inner layers (each
+// root mixed before its fold's alpha is drawn), the last layer's coefficients,
+// the proof of work and the queries.
+// ---------------------------------------------------------------------------
+struct FriBuffers {
+  uint32_t* quot;                   // 4 coordinate columns of 2^L
+  uint8_t* tree_q;                  // first-layer tree
+  std::vector<uint32_t*> line;      // line layers 0..n_inner (the last one is the last layer)
+  std::vector<uint8_t*> line_tree;  // trees of line layers 0..n_inner-1
+  uint32_t* pow_result;             // 2 words of device scratch
+};
+struct FriResult {
+  std::vector<std::array<uint8_t, 32>> roots;  // first layer, then inner layers
+  std::vector<QM31> last_coeffs;
+  uint64_t nonce = 0;
+  std::vector<uint64_t> queries;  // sorted, unique
+};
+// Runs on `fs` (FRI, latency-bound) and `s` (proof of work); `pin` is pinned host staging.
+// ev_fri and ev_pow (nullable) are recorded after the last layer and after the grind.
+int32_t fri_pow_queries(const DeviceTables& T, int sm_count, Channel& ch, const PcsConfig& cfg, uint32_t L,
+                        uint32_t n_inner, uint32_t last_log, const FriBuffers& fb, uint8_t* pin, cudaStream_t s,
+                        cudaStream_t fs, cudaEvent_t ev_fri, cudaEvent_t ev_pow, FriResult& out, std::string& err);
+
+// ---------------------------------------------------------------------------
+// Decommitment (src/prover/vcs_lifted/decommit.zig:56-352, src/prover/fri.zig:624-850):
+// the queried values and witness hashes of every tree, and the FRI layers' witnesses,
+// gathered on the device in one pass and copied back once.
+// ---------------------------------------------------------------------------
+class DecommitPlan {
+ public:
+  // A trace tree of `cols` columns (each 2^max_log words) at the queried leaf positions;
+  // a tree without columns contributes nothing.
+  void add_tree(const uint8_t* layers, uint32_t max_log, const std::vector<const uint32_t*>& cols,
+                const std::vector<uint64_t>& queries);
+  void add_fri(const FriBuffers& fb, uint32_t L, uint32_t n_inner, const std::vector<uint64_t>& queries);
+  // Gathers through `scratch` (device) and `pin` (pinned host); synchronizes `fs`.
+  int32_t gather(uint8_t* scratch, size_t scratch_bytes, uint8_t* pin, size_t pin_bytes, cudaStream_t fs,
+                 cudaEvent_t ev_done, std::string& err);
+  void json_witness(Json& j, size_t tree) const;   // [hash, ...]
+  void json_queried(Json& j, size_t tree) const;   // [[col 0 values], [col 1 values], ...]
+  void json_fri(Json& j, const FriResult& fr) const;
+
+ private:
+  struct TreePlan { size_t word0 = 0, n_cols = 0, hash0 = 0, n_hash = 0; };
+  struct LayerPlan { size_t wit_word0, n_wit, hash0, n_hash; };
+  std::vector<GatherItem> words_;
+  std::vector<HashGatherItem> hashes_;
+  std::vector<TreePlan> trees_;
+  std::vector<LayerPlan> fri_;
+  size_t n_queries_ = 0;
+  const uint32_t* gw_ = nullptr;
+  const uint8_t* gh_ = nullptr;
+  void hash_list(Json& j, size_t first, size_t count) const;
+};
+
+}  // namespace sb

@@ -32,6 +32,7 @@ int32_t Server::start() {
     p->set_transient(!(flags_ & SERVER_PERSISTENT_WORKSPACES));
     provers_.push_back(p);
   }
+  xor_provers_.assign(n_slots_, nullptr);
   for (uint32_t i = 0; i < n_slots_; ++i) threads_.emplace_back(&Server::worker, this, i);
   return OK;
 }
@@ -44,33 +45,25 @@ Server::~Server() {
   cv_work_.notify_all();
   for (auto& t : threads_) t.join();
   for (auto* p : provers_) delete p;
+  for (auto* p : xor_provers_) delete p;
   for (auto& kv : table_) delete kv.second;
 }
 
-int32_t Server::submit(const ProveRequest& r, uint64_t* ticket, std::string* err) {
-  // admit(profile, log_rows, columns), resource_admission.zig: rows in [1, 22], cells and
-  // accounted bytes within the profile.
-  if (r.log_n_rows < 1 || r.log_n_rows > ADMISSION_MAX_LOG_ROWS || r.sequence_len < 2 || r.sequence_len > 1000 ||
-      r.config.log_blowup_factor < 1 || r.config.log_blowup_factor > 4) {
-    *err = "invalid proof shape";
-    return E_INVALID;
-  }
-  uint64_t cells = (uint64_t)r.sequence_len << r.log_n_rows;
-  uint64_t accounted = cells * ACCOUNTED_BYTES_PER_CELL;
+int32_t Server::enqueue(Entry* e, uint64_t cells, size_t ws, uint64_t* ticket, std::string* err) {
+  const uint64_t accounted = cells * ACCOUNTED_BYTES_PER_CELL;
   std::lock_guard<std::mutex> g(mu_);
   if (cells > limits_.max_committed_cells || accounted > limits_.max_accounted_bytes) {
     ++snap_.rejected;
+    delete e;
     *err = "committed cell budget of the resource profile exceeded";
     return E_REJECTED;
   }
-  size_t ws = WideFibProver::workspace_bytes(r.log_n_rows, r.sequence_len, r.config.log_blowup_factor);
-  if (ws > budget_) {
+  if (ws == 0 || ws > budget_) {
     ++snap_.rejected;
+    delete e;
     *err = "proof workspace exceeds the server's device memory budget";
     return E_REJECTED;
   }
-  Entry* e = new Entry();
-  e->req = r;
   e->ticket = next_ticket_++;
   e->workspace = ws;
   e->stats.accounted_bytes = accounted;
@@ -82,6 +75,38 @@ int32_t Server::submit(const ProveRequest& r, uint64_t* ticket, std::string* err
   *ticket = e->ticket;
   cv_work_.notify_one();
   return OK;
+}
+
+int32_t Server::submit(const ProveRequest& r, uint64_t* ticket, std::string* err) {
+  // admit(profile, log_rows, columns), resource_admission.zig: rows in [1, 22], cells and
+  // accounted bytes within the profile.
+  if (r.log_n_rows < 1 || r.log_n_rows > ADMISSION_MAX_LOG_ROWS || r.sequence_len < 2 || r.sequence_len > 1000 ||
+      r.config.log_blowup_factor < 1 || r.config.log_blowup_factor > 4) {
+    *err = "invalid proof shape";
+    return E_INVALID;
+  }
+  Entry* e = new Entry();
+  e->req = r;
+  return enqueue(e, (uint64_t)r.sequence_len << r.log_n_rows,
+                 WideFibProver::workspace_bytes(r.log_n_rows, r.sequence_len, r.config.log_blowup_factor), ticket,
+                 err);
+}
+
+int32_t Server::submit_xor(const XorRequest& r, uint64_t* ticket, std::string* err) {
+  if (r.log_n < 1 || r.log_n > ADMISSION_MAX_LOG_ROWS || (r.log_table != 8 && r.log_table != 16) ||
+      r.config.log_blowup_factor < 1 || r.config.log_blowup_factor > 4) {
+    *err = "invalid proof shape";
+    return E_INVALID;
+  }
+  Entry* e = new Entry();
+  e->is_xor = true;
+  e->xreq = r;
+  // Committed columns: 4 preprocessed, 4 main, 8 interaction, of 2^max(log_n, log_table) rows.
+  const uint32_t L = std::max(r.log_n, r.log_table);
+  return enqueue(e, 16ull << L,
+                 LogupXorProver::workspace_bytes(r.log_n, r.log_table, r.config.log_blowup_factor,
+                                                 r.config.log_last_layer_degree_bound),
+                 ticket, err);
 }
 
 void Server::worker(uint32_t slot) {
@@ -114,8 +139,16 @@ void Server::worker(uint32_t slot) {
     lk.unlock();
     // Another head may fit beside this one.
     cv_work_.notify_one();
-    std::string proof;
-    int32_t rc = prover->prove(e->req, proof, &e->stats.stages);
+    std::string proof, xerr;
+    int32_t rc;
+    if (e->is_xor) {
+      if (!xor_provers_[slot]) xor_provers_[slot] = new LogupXorProver(ctx_);
+      rc = xor_provers_[slot]->prove(e->xreq, proof);
+      if (rc != OK) xerr = xor_provers_[slot]->error();
+    } else {
+      rc = prover->prove(e->req, proof, &e->stats.stages);
+      if (rc != OK) xerr = prover->error();
+    }
     auto t_end = std::chrono::steady_clock::now();
     lk.lock();
     if (!persistent) in_use_ -= e->workspace;
@@ -125,7 +158,7 @@ void Server::worker(uint32_t slot) {
       e->proof.swap(proof);
       ++snap_.completed;
     } else {
-      e->error = prover->error();
+      e->error = xerr;
       ++snap_.failed;
     }
     e->stats.queued_ms = std::chrono::duration<double, std::milli>(e->t_start - e->t_submit).count();

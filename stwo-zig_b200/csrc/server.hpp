@@ -50,13 +50,16 @@ class Server {
   ~Server();
   int32_t start();
   int32_t submit(const ProveRequest& r, uint64_t* ticket, std::string* err);
+  int32_t submit_xor(const XorRequest& r, uint64_t* ticket, std::string* err);
   // Blocks until the request is done. E_BUFFER_TOO_SMALL keeps the result for another call.
   int32_t wait(uint64_t ticket, uint8_t* out, size_t cap, size_t* len, RequestStats* stats, std::string* err);
   ServerSnapshot snapshot();
 
  private:
   struct Entry {
+    bool is_xor = false;
     ProveRequest req;
+    XorRequest xreq;
     uint64_t ticket = 0;
     size_t workspace = 0;
     RequestStats stats;
@@ -66,6 +69,7 @@ class Server {
     std::string proof, error;
   };
   void worker(uint32_t slot);
+  int32_t enqueue(Entry* e, uint64_t cells, size_t workspace, uint64_t* ticket, std::string* err);
 
   Context* ctx_;
   uint32_t n_slots_;
@@ -81,6 +85,7 @@ class Server {
   bool stopping_ = false;
   ServerSnapshot snap_;
   std::vector<WideFibProver*> provers_;
+  std::vector<LogupXorProver*> xor_provers_;  // created on a slot's first XOR request
   std::vector<std::thread> threads_;
 };
 

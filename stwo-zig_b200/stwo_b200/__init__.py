@@ -61,6 +61,11 @@ class LogupUseC(ctypes.Structure):
                 ("multiplicity", _vp)]
 
 
+class XorRequestC(ctypes.Structure):
+    _fields_ = [("log_n", _u32), ("log_table", _u32), ("config", PcsConfigC), ("seed", _u64),
+                ("has_channel_seed", _u32), ("reserved", _u32), ("channel_seed", _u64)]
+
+
 class ServerConfigC(ctypes.Structure):
     _fields_ = [("slots", _u32), ("profile", _u32), ("memory_budget", _u64), ("flags", _u32)]
 
@@ -104,8 +109,11 @@ _SIGS = {
     "stwo_b200_wide_fib_composition": [_vp, _u32, _u32, _vp, _u64, _vp, _u32, _u32, _vp, _u64, _vp],
     "stwo_b200_pow_grind": [_vp, ctypes.c_char_p, _u32, ctypes.POINTER(_u64)],
     "stwo_b200_telemetry_snapshot": [ctypes.POINTER(_u64)],
+    "stwo_b200_prove_logup_xor": [_vp, ctypes.POINTER(XorRequestC), _vp, ctypes.c_size_t,
+                                  ctypes.POINTER(ctypes.c_size_t)],
     "stwo_b200_server_create": [_vp, ctypes.POINTER(ServerConfigC), ctypes.POINTER(_vp)],
     "stwo_b200_server_submit": [_vp, ctypes.POINTER(RequestC), ctypes.POINTER(_u64)],
+    "stwo_b200_server_submit_xor": [_vp, ctypes.POINTER(XorRequestC), ctypes.POINTER(_u64)],
     "stwo_b200_server_wait": [_vp, _u64, _vp, ctypes.c_size_t, ctypes.POINTER(ctypes.c_size_t),
                               ctypes.POINTER(RequestStatsC)],
     "stwo_b200_server_snapshot_get": [_vp, ctypes.POINTER(ServerSnapshotC)],
@@ -277,6 +285,21 @@ class Context:
             return proof, {name: getattr(times, name) for name, _ in StageTimesC._fields_}
         return proof
 
+    def prove_logup_xor(self, log_n: int, config: PcsConfig, seed: int = 0, log_table: int = 16,
+                        channel_seed: int | None = None) -> bytes:
+        """Proves the LogUp XOR-lookup AIR (2^log_n seeded lookups into the 2^log_table XOR table)."""
+        req = XorRequestC(log_n, log_table, config._c(), seed, int(channel_seed is not None), 0, channel_seed or 0)
+        n = ctypes.c_size_t(0)
+        cap = self._cap
+        buf = ctypes.create_string_buffer(cap)
+        rc = _lib.stwo_b200_prove_logup_xor(self._h, ctypes.byref(req), buf, cap, ctypes.byref(n))
+        if rc == E_BUFFER_TOO_SMALL:
+            self._cap = cap = max(2 * cap, n.value)
+            buf = ctypes.create_string_buffer(cap)
+            rc = _lib.stwo_b200_prove_logup_xor(self._h, ctypes.byref(req), buf, cap, ctypes.byref(n))
+        _check(rc)
+        return buf.raw[: n.value]
+
     def prove_wide_fibonacci_batch(self, requests: list[dict], max_in_flight: int = 4, with_times: bool = False,
                                    proof_cap: int = 1 << 21):
         """requests: dicts with statement, config and optional trace / trace_kind / trace_seed / channel_seed."""
@@ -429,6 +452,13 @@ class Server:
         ticket = _u64(0)
         _check(_lib.stwo_b200_server_submit(self._h, ctypes.byref(req), ctypes.byref(ticket)))
         self._keep[ticket.value] = keep
+        return ticket.value
+
+    def submit_xor(self, log_n: int, config: PcsConfig, seed: int = 0, log_table: int = 16,
+                   channel_seed: int | None = None) -> int:
+        req = XorRequestC(log_n, log_table, config._c(), seed, int(channel_seed is not None), 0, channel_seed or 0)
+        ticket = _u64(0)
+        _check(_lib.stwo_b200_server_submit_xor(self._h, ctypes.byref(req), ctypes.byref(ticket)))
         return ticket.value
 
     def wait(self, ticket: int) -> tuple[bytes, dict]:

@@ -97,3 +97,35 @@ def test_close_finishes_queued_requests(ctx):
     for i in range(6):
         srv.submit(sb.Statement(14, 16), g, trace_kind=sb.TRACE_SEEDED, trace_seed=i)
     srv.close()  # drains without a wait per request
+
+
+def test_served_mix_with_xor_lookups(ctx):
+    """70% wide-Fibonacci and 30% LogUp XOR-lookup requests through one serving loop: every proof
+    equals its single run, and the XOR proofs verify."""
+    import stwo_b200 as sb
+    import verifier
+    g = _cfg()
+    rng = np.random.default_rng(11)
+    reqs = []
+    for i in range(16):
+        if rng.random() < 0.3:
+            reqs.append(("xor", int(rng.integers(12, 17)), int(rng.integers(1, 2**40))))
+        else:
+            reqs.append(("wf", int(rng.integers(12, 17)), int(rng.choice([16, 32, 100])), int(rng.integers(1, 2**40))))
+    if not any(r[0] == "xor" for r in reqs):
+        reqs[0] = ("xor", 14, 5)
+    with sb.Server(ctx, slots=4, profile=2) as srv:
+        tickets = []
+        for r in reqs:
+            if r[0] == "xor":
+                tickets.append(srv.submit_xor(r[1], g, seed=r[2]))
+            else:
+                tickets.append(srv.submit(sb.Statement(r[1], r[2]), g, trace_kind=sb.TRACE_SEEDED, trace_seed=r[3]))
+        served = [srv.wait(t)[0] for t in tickets]
+    for r, p in zip(reqs, served):
+        if r[0] == "xor":
+            assert p == ctx.prove_logup_xor(r[1], g, seed=r[2])
+            assert verifier.verify_logup_xor(p, r[1], 16)
+        else:
+            assert p == ctx.prove_wide_fibonacci(sb.Statement(r[1], r[2]), g, trace_kind=sb.TRACE_SEEDED,
+                                                 trace_seed=r[3])

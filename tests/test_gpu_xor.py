@@ -1,0 +1,62 @@
+"""LogUp XOR-lookup AIR proofs on the GPU, checked by the independent verifier (the AIR has no
+reference counterpart, so the verifier's transcript replay, LogUp cancellation, OODS constraint
+check and PCS/FRI decommitment checks are the parity gate)."""
+import json
+
+import pytest
+
+import oracle
+import verifier
+
+pytestmark = pytest.mark.gpu
+
+
+def _cfg(preset, **over):
+    import stwo_b200 as sb
+    c = oracle.config(preset, **over)
+    return sb.PcsConfig(c.pow_bits, sb.FriConfig(c.log_blowup_factor, c.log_last_layer_degree_bound, c.n_queries))
+
+
+@pytest.mark.parametrize("log_n,log_table,preset,over", [
+    (1, 8, "smoke", {}), (6, 8, "smoke", {}), (9, 8, "functional", {}), (10, 8, "functional", {}),
+    (8, 8, "functional", dict(log_blowup_factor=2, n_queries=5, log_last_layer_degree_bound=1)),
+    (12, 16, "secure", {}), (16, 16, "functional", {}), (18, 16, "secure", {})])
+def test_xor_air_proof_verifies(ctx, log_n, log_table, preset, over):
+    g = _cfg(preset, **over)
+    p = ctx.prove_logup_xor(log_n, g, seed=7 + log_n, log_table=log_table, channel_seed=3)
+    assert verifier.verify_logup_xor(p, log_n, log_table, channel_seed=3)
+    with pytest.raises(verifier.VerificationError):
+        verifier.verify_logup_xor(p, log_n, log_table, channel_seed=4)
+
+
+def test_xor_air_full_size_and_determinism(ctx):
+    g = _cfg("secure")
+    a = ctx.prove_logup_xor(20, g, seed=99)
+    assert verifier.verify_logup_xor(a, 20, 16)
+    assert a == ctx.prove_logup_xor(20, g, seed=99)
+    assert a != ctx.prove_logup_xor(20, g, seed=100)
+
+
+@pytest.mark.parametrize("field", ["claimed", "sampled", "queried"])
+def test_xor_air_tampering_rejected(ctx, field):
+    p = ctx.prove_logup_xor(9, _cfg("functional"), seed=5, log_table=8)
+    d = json.loads(p)
+    if field == "claimed":
+        d["claimed_sums"][0][0] = (d["claimed_sums"][0][0] + 1) % (2**31 - 1)
+        d["claimed_sums"][1][0] = (d["claimed_sums"][1][0] - 1) % (2**31 - 1)  # still cancelling
+    elif field == "sampled":
+        d["sampled_values"][2][3][0][1] = (d["sampled_values"][2][3][0][1] + 1) % (2**31 - 1)
+    else:
+        d["queried_values"][1][2][0] ^= 1
+    with pytest.raises(verifier.VerificationError):
+        verifier.verify_logup_xor(json.dumps(d, separators=(",", ":")).encode(), 9, 8)
+
+
+def test_xor_air_bad_arguments(ctx):
+    import stwo_b200 as sb
+    with pytest.raises(sb.StwoError) as e:
+        ctx.prove_logup_xor(23, _cfg("smoke"), log_table=16)
+    assert e.value.status == sb.E_INVALID
+    with pytest.raises(sb.StwoError) as e:
+        ctx.prove_logup_xor(10, _cfg("smoke"), log_table=12)
+    assert e.value.status == sb.E_INVALID
