@@ -180,6 +180,12 @@ int32_t stwo_b200_server_submit_xor(stwo_b200_server* server, const stwo_b200_xo
  * *proof_len and keeps the result for another call. */
 int32_t stwo_b200_server_wait(stwo_b200_server* server, uint64_t ticket, uint8_t* proof_out, size_t proof_cap,
                               size_t* proof_len, stwo_b200_request_stats* stats);
+/* Sizes every slot for the largest shapes it will serve (the reference's warmup / initializeRuntime
+ * hooks, src/prover/engine.zig): persistent workspaces grow to 2^max_log_n_rows x max_sequence_len
+ * (within the memory budget), and the stream-ordered pool is pre-grown for transient workspaces and
+ * XOR-lookup proofs of up to 2^max_xor_log_n rows (0: none). Call while the server is idle. */
+int32_t stwo_b200_server_warmup(stwo_b200_server* server, uint32_t max_log_n_rows, uint32_t max_sequence_len,
+                                uint32_t log_blowup, uint32_t max_xor_log_n);
 int32_t stwo_b200_server_snapshot_get(stwo_b200_server* server, stwo_b200_server_snapshot* out);
 /* Finishes every queued and running request, then releases the slots. */
 int32_t stwo_b200_server_destroy(stwo_b200_server* server);

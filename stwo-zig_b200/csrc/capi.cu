@@ -478,6 +478,16 @@ int32_t stwo_b200_server_wait(stwo_b200_server* server, uint64_t ticket, uint8_t
   return rc == STWO_B200_OK ? rc : set_error(rc, err);
 }
 
+int32_t stwo_b200_server_warmup(stwo_b200_server* server, uint32_t max_log_n_rows, uint32_t max_sequence_len,
+                                uint32_t log_blowup, uint32_t max_xor_log_n) {
+  if (!server || max_log_n_rows > 22 || max_xor_log_n > 22 || log_blowup < 1 || log_blowup > 4 ||
+      (max_log_n_rows && (max_sequence_len < 2 || max_sequence_len > 1000)))
+    return set_error(STWO_B200_E_INVALID, "bad warmup arguments");
+  std::string err;
+  int32_t rc = server->server->warmup(max_log_n_rows, max_sequence_len, log_blowup, max_xor_log_n, &err);
+  return rc == STWO_B200_OK ? rc : set_error(rc, err);
+}
+
 int32_t stwo_b200_server_snapshot_get(stwo_b200_server* server, stwo_b200_server_snapshot* out) {
   if (!server || !out) return set_error(STWO_B200_E_INVALID, "null server argument");
   sb::ServerSnapshot s = server->server->snapshot();

@@ -210,6 +210,16 @@ void WideFibProver::set_transient(bool on) {
   transient_ = on;
 }
 
+int32_t WideFibProver::reserve(uint32_t log_n, uint32_t W, uint32_t B, size_t* held) {
+  if (!transient_) {
+    cudaSetDevice(ctx_->device);
+    int32_t rc = ensure_workspace(log_n, W, B);
+    if (rc != OK) return rc;
+  }
+  if (held) *held = transient_ ? 0 : arena_size_;
+  return OK;
+}
+
 int32_t WideFibProver::ensure_workspace(uint32_t log_n, uint32_t W, uint32_t B) {
   if (!pinned_) {
     pinned_size_ = GATHER_SCRATCH + (1 << 20);

@@ -65,6 +65,9 @@ class WideFibProver {
   // each proof and returned at its end, so the device memory a prover holds between proofs is
   // only its pinned staging. Used by the serving loop, which admits by in-flight workspace bytes.
   void set_transient(bool on);
+  // Grows the persistent workspace to a shape ahead of use (no-op in transient mode); returns the
+  // bytes the prover holds afterwards in *held.
+  int32_t reserve(uint32_t log_n, uint32_t W, uint32_t B, size_t* held);
 
  private:
   int32_t ensure_workspace(uint32_t log_n, uint32_t W, uint32_t B);

@@ -32,7 +32,7 @@ int32_t Server::start() {
     p->set_transient(!(flags_ & SERVER_PERSISTENT_WORKSPACES));
     provers_.push_back(p);
   }
-  xor_provers_.assign(n_slots_, nullptr);
+  for (uint32_t i = 0; i < n_slots_; ++i) xor_provers_.push_back(new LogupXorProver(ctx_));
   for (uint32_t i = 0; i < n_slots_; ++i) threads_.emplace_back(&Server::worker, this, i);
   return OK;
 }
@@ -118,8 +118,9 @@ void Server::worker(uint32_t slot) {
     // workspaces count while their proof runs; persistent ones count for as long as a slot holds
     // them (a slot grows its workspace to the largest proof it has run).
     const bool persistent = flags_ & SERVER_PERSISTENT_WORKSPACES;
+    // XOR-lookup proofs always take their workspace from the pool for the proof's duration.
     auto extra = [&](const Entry* h) -> uint64_t {
-      if (!persistent) return h->workspace;
+      if (!persistent || h->is_xor) return h->workspace;
       return h->workspace > held_[slot] ? h->workspace - held_[slot] : 0;
     };
     cv_work_.wait(lk, [&] {
@@ -130,7 +131,7 @@ void Server::worker(uint32_t slot) {
     queue_.pop_front();
     const uint64_t added = extra(e);
     in_use_ += added;
-    if (persistent) held_[slot] += added;
+    if (persistent && !e->is_xor) held_[slot] += added;
     ++in_flight_;
     snap_.peak_in_flight = std::max(snap_.peak_in_flight, in_flight_);
     snap_.peak_workspace_bytes = std::max<uint64_t>(snap_.peak_workspace_bytes, in_use_);
@@ -142,7 +143,6 @@ void Server::worker(uint32_t slot) {
     std::string proof, xerr;
     int32_t rc;
     if (e->is_xor) {
-      if (!xor_provers_[slot]) xor_provers_[slot] = new LogupXorProver(ctx_);
       rc = xor_provers_[slot]->prove(e->xreq, proof);
       if (rc != OK) xerr = xor_provers_[slot]->error();
     } else {
@@ -151,7 +151,7 @@ void Server::worker(uint32_t slot) {
     }
     auto t_end = std::chrono::steady_clock::now();
     lk.lock();
-    if (!persistent) in_use_ -= e->workspace;
+    if (!persistent || e->is_xor) in_use_ -= e->workspace;
     --in_flight_;
     e->status = rc;
     if (rc == OK) {
@@ -194,6 +194,51 @@ int32_t Server::wait(uint64_t ticket, uint8_t* out, size_t cap, size_t* len, Req
   std::memcpy(out, e->proof.data(), e->proof.size());
   table_.erase(it);
   delete e;
+  return OK;
+}
+
+int32_t Server::warmup(uint32_t max_log_n_rows, uint32_t max_sequence_len, uint32_t log_blowup,
+                       uint32_t max_xor_log_n, std::string* err) {
+  std::lock_guard<std::mutex> g(mu_);
+  if (in_flight_ != 0 || !queue_.empty()) {
+    *err = "warmup needs an idle server";
+    return E_INVALID;
+  }
+  cudaSetDevice(ctx_->device);
+  const bool persistent = flags_ & SERVER_PERSISTENT_WORKSPACES;
+  size_t wf = max_log_n_rows ? WideFibProver::workspace_bytes(max_log_n_rows, max_sequence_len, log_blowup) : 0;
+  size_t xr = max_xor_log_n ? LogupXorProver::workspace_bytes(max_xor_log_n, 16, log_blowup, 0) : 0;
+  if (persistent && wf) {
+    for (uint32_t slot = 0; slot < n_slots_; ++slot) {
+      if (held_[slot] >= wf) continue;
+      if (in_use_ - held_[slot] + wf > budget_) break;  // slots beyond the budget stay small
+      size_t held = 0;
+      int32_t rc = provers_[slot]->reserve(max_log_n_rows, max_sequence_len, log_blowup, &held);
+      if (rc != OK) {
+        *err = provers_[slot]->error();
+        return rc;
+      }
+      in_use_ = in_use_ - held_[slot] + held;
+      held_[slot] = held;
+    }
+  }
+  // Pre-grow the stream-ordered pool (kept: release threshold = unlimited) by what the transient
+  // workspaces of a full set of slots can take at once.
+  size_t per_slot = std::max(xr, persistent ? (size_t)0 : wf);
+  uint64_t pool = std::min<uint64_t>((uint64_t)per_slot * n_slots_, persistent ? budget_ - std::min(budget_, in_use_)
+                                                                               : budget_);
+  if (pool) {
+    void* p = nullptr;
+    cudaStream_t s = ctx_->stream;
+    if (cudaMallocAsync(&p, pool, s) != cudaSuccess) {
+      cudaGetLastError();
+      *err = "pool pre-growth failed";
+      return E_OOM;
+    }
+    cudaFreeAsync(p, s);
+    cudaStreamSynchronize(s);
+  }
+  snap_.peak_workspace_bytes = std::max<uint64_t>(snap_.peak_workspace_bytes, in_use_);
   return OK;
 }
 

@@ -51,6 +51,12 @@ class Server {
   int32_t start();
   int32_t submit(const ProveRequest& r, uint64_t* ticket, std::string* err);
   int32_t submit_xor(const XorRequest& r, uint64_t* ticket, std::string* err);
+  // Sizes every slot for the largest shapes it will serve before traffic arrives (the reference's
+  // warmup / initializeRuntime hooks): persistent workspaces grow to the largest wide-Fibonacci
+  // shape, and the stream-ordered pool is pre-grown for transient workspaces and XOR proofs. Call
+  // it while the server is idle.
+  int32_t warmup(uint32_t max_log_n_rows, uint32_t max_sequence_len, uint32_t log_blowup, uint32_t max_xor_log_n,
+                 std::string* err);
   // Blocks until the request is done. E_BUFFER_TOO_SMALL keeps the result for another call.
   int32_t wait(uint64_t ticket, uint8_t* out, size_t cap, size_t* len, RequestStats* stats, std::string* err);
   ServerSnapshot snapshot();

@@ -116,6 +116,7 @@ _SIGS = {
     "stwo_b200_server_submit_xor": [_vp, ctypes.POINTER(XorRequestC), ctypes.POINTER(_u64)],
     "stwo_b200_server_wait": [_vp, _u64, _vp, ctypes.c_size_t, ctypes.POINTER(ctypes.c_size_t),
                               ctypes.POINTER(RequestStatsC)],
+    "stwo_b200_server_warmup": [_vp, _u32, _u32, _u32, _u32],
     "stwo_b200_server_snapshot_get": [_vp, ctypes.POINTER(ServerSnapshotC)],
     "stwo_b200_server_destroy": [_vp],
     "stwo_b200_xor_lookup_trace": [_vp, _u32, _u64, _vp, _vp, _vp, _vp],
@@ -475,6 +476,11 @@ class Server:
         stats = {name: getattr(st, name) for name, _ in RequestStatsC._fields_ if name != "stages"}
         stats["stages"] = {name: getattr(st.stages, name) for name, _ in StageTimesC._fields_}
         return buf.raw[: n.value], stats
+
+    def warmup(self, max_log_n_rows: int = 0, max_sequence_len: int = 100, log_blowup: int = 1,
+               max_xor_log_n: int = 0) -> None:
+        """Sizes every slot for the largest shapes before traffic (call while idle)."""
+        _check(_lib.stwo_b200_server_warmup(self._h, max_log_n_rows, max_sequence_len, log_blowup, max_xor_log_n))
 
     def snapshot(self) -> dict:
         s = ServerSnapshotC()

@@ -129,3 +129,17 @@ def test_served_mix_with_xor_lookups(ctx):
         else:
             assert p == ctx.prove_wide_fibonacci(sb.Statement(r[1], r[2]), g, trace_kind=sb.TRACE_SEEDED,
                                                  trace_seed=r[3])
+
+
+def test_warmup_presizes_slots(ctx):
+    import stwo_b200 as sb
+    g = _cfg("functional")
+    with sb.Server(ctx, slots=3, profile=1, persistent_workspaces=True) as srv:
+        srv.warmup(16, 32, 1, 12)
+        held = srv.snapshot()["peak_workspace_bytes"]
+        assert held > 0
+        ts = [srv.submit(sb.Statement(16, 32), g, trace_kind=sb.TRACE_SEEDED, trace_seed=i) for i in range(3)]
+        ts.append(srv.submit_xor(12, g, seed=1))
+        out = [srv.wait(t)[0] for t in ts]
+    assert out[0] == ctx.prove_wide_fibonacci(sb.Statement(16, 32), g, trace_kind=sb.TRACE_SEEDED, trace_seed=0)
+    assert out[3] == ctx.prove_logup_xor(12, g, seed=1)
