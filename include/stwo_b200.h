@@ -137,6 +137,18 @@ typedef struct {
 int32_t stwo_b200_prove_logup_xor(stwo_b200_context* ctx, const stwo_b200_xor_request* req, uint8_t* proof_out,
                                   size_t proof_cap, size_t* proof_len);
 
+/* ---- Verifier (host) ------------------------------------------------------------------------------ */
+
+/* Verifies a proof from its bytes on the calling host thread (no device use): the reference verifier
+ * (src/examples/wide_fibonacci.zig:360-433, src/core/verifier.zig, src/core/pcs/verifier.zig,
+ * src/core/fri.zig, src/core/vcs_lifted/verifier.zig). STWO_B200_OK, or STWO_B200_E_CONSTRAINTS with
+ * the failed check in stwo_b200_last_error(). has_channel_seed mirrors the prover's optional mix. */
+int32_t stwo_b200_verify_wide_fibonacci(const uint8_t* proof, size_t proof_len, uint32_t log_n_rows,
+                                        uint32_t sequence_len, uint32_t has_channel_seed, uint64_t channel_seed);
+/* The same for LogUp XOR-lookup AIR proofs (additionally: the claimed sums cancel). */
+int32_t stwo_b200_verify_logup_xor(const uint8_t* proof, size_t proof_len, uint32_t log_n, uint32_t log_table,
+                                   uint32_t has_channel_seed, uint64_t channel_seed);
+
 /* ---- Serving loop ------------------------------------------------------------------------------- */
 
 /* Continuous batching of wide-Fibonacci proofs on one device: `slots` proofs in flight (each a host
@@ -148,6 +160,7 @@ int32_t stwo_b200_prove_logup_xor(stwo_b200_context* ctx, const stwo_b200_xor_re
  * stwo_b200_prove_wide_fibonacci for the same request. The reference has no serving loop; the
  * admission limits are its resource profiles. */
 typedef struct stwo_b200_server stwo_b200_server;
+#define STWO_B200_SERVER_VERIFY 2u /* every proof is verified on its slot's host thread before it is returned */
 #define STWO_B200_SERVER_PERSISTENT_WORKSPACES 1u /* slots keep their workspace between proofs (counted
                                                   * against the budget while held) instead of taking it
                                                   * from the stream-ordered pool per proof */

@@ -10,6 +10,7 @@
 #include "context.hpp"
 #include "prover.hpp"
 #include "server.hpp"
+#include "verifier.hpp"
 
 namespace sb {
 static std::atomic<uint64_t> g_launches(0);
@@ -381,6 +382,24 @@ int32_t stwo_b200_pow_grind(stwo_b200_context* ctx, const uint8_t prefix_digest[
   return STWO_B200_OK;
 }
 
+int32_t stwo_b200_verify_wide_fibonacci(const uint8_t* proof, size_t proof_len, uint32_t log_n_rows,
+                                        uint32_t sequence_len, uint32_t has_channel_seed, uint64_t channel_seed) {
+  if (!proof) return set_error(STWO_B200_E_INVALID, "null proof");
+  std::string err;
+  int32_t rc = sb::verify_wide_fib_json(std::string(reinterpret_cast<const char*>(proof), proof_len), log_n_rows,
+                                        sequence_len, has_channel_seed != 0, channel_seed, err);
+  return rc == STWO_B200_OK ? rc : set_error(rc, err);
+}
+
+int32_t stwo_b200_verify_logup_xor(const uint8_t* proof, size_t proof_len, uint32_t log_n, uint32_t log_table,
+                                   uint32_t has_channel_seed, uint64_t channel_seed) {
+  if (!proof) return set_error(STWO_B200_E_INVALID, "null proof");
+  std::string err;
+  int32_t rc = sb::verify_logup_xor_json(std::string(reinterpret_cast<const char*>(proof), proof_len), log_n,
+                                         log_table, has_channel_seed != 0, channel_seed, err);
+  return rc == STWO_B200_OK ? rc : set_error(rc, err);
+}
+
 int32_t stwo_b200_prove_logup_xor(stwo_b200_context* ctx, const stwo_b200_xor_request* req, uint8_t* proof_out,
                                   size_t proof_cap, size_t* proof_len) {
   CK_CTX(ctx);
@@ -415,7 +434,7 @@ struct stwo_b200_server {
 int32_t stwo_b200_server_create(stwo_b200_context* ctx, const stwo_b200_server_config* cfg,
                                 stwo_b200_server** out) {
   CK_CTX(ctx);
-  if (!cfg || !out || cfg->profile > 2 || cfg->slots > 64 || cfg->flags > 1)
+  if (!cfg || !out || cfg->profile > 2 || cfg->slots > 64 || cfg->flags > 3)
     return set_error(STWO_B200_E_INVALID, "bad server config");
   uint64_t budget = cfg->memory_budget;
   if (budget == 0) {

@@ -1,6 +1,8 @@
 // Serving loop (continuous batching) over WideFibProver slots; see server.hpp.
 #include "server.hpp"
 
+#include "verifier.hpp"
+
 #include <algorithm>
 #include <cstring>
 
@@ -148,6 +150,18 @@ void Server::worker(uint32_t slot) {
     } else {
       rc = prover->prove(e->req, proof, &e->stats.stages);
       if (rc != OK) xerr = prover->error();
+    }
+    if (rc == OK && (flags_ & SERVER_VERIFY)) {
+      // The device keeps serving the other slots meanwhile.
+      std::string verr;
+      int32_t vrc = e->is_xor ? verify_logup_xor_json(proof, e->xreq.log_n, e->xreq.log_table,
+                                                      e->xreq.has_channel_seed, e->xreq.channel_seed, verr)
+                              : verify_wide_fib_json(proof, e->req.log_n_rows, e->req.sequence_len,
+                                                     e->req.has_channel_seed, e->req.channel_seed, verr);
+      if (vrc != OK) {
+        rc = vrc;
+        xerr = "served proof failed verification: " + verr;
+      }
     }
     auto t_end = std::chrono::steady_clock::now();
     lk.lock();

@@ -38,6 +38,7 @@ struct RequestStats {
 
 // Server flags.
 constexpr uint32_t SERVER_PERSISTENT_WORKSPACES = 1;  // slots keep their workspace between proofs
+constexpr uint32_t SERVER_VERIFY = 2;                 // verify every proof on the slot's host thread
 
 struct ServerSnapshot {
   uint64_t submitted = 0, completed = 0, failed = 0, rejected = 0;

@@ -111,6 +111,8 @@ _SIGS = {
     "stwo_b200_telemetry_snapshot": [ctypes.POINTER(_u64)],
     "stwo_b200_prove_logup_xor": [_vp, ctypes.POINTER(XorRequestC), _vp, ctypes.c_size_t,
                                   ctypes.POINTER(ctypes.c_size_t)],
+    "stwo_b200_verify_wide_fibonacci": [ctypes.c_char_p, ctypes.c_size_t, _u32, _u32, _u32, _u64],
+    "stwo_b200_verify_logup_xor": [ctypes.c_char_p, ctypes.c_size_t, _u32, _u32, _u32, _u64],
     "stwo_b200_server_create": [_vp, ctypes.POINTER(ServerConfigC), ctypes.POINTER(_vp)],
     "stwo_b200_server_submit": [_vp, ctypes.POINTER(RequestC), ctypes.POINTER(_u64)],
     "stwo_b200_server_submit_xor": [_vp, ctypes.POINTER(XorRequestC), ctypes.POINTER(_u64)],
@@ -193,6 +195,21 @@ class PcsConfig:
 class Statement:
     log_n_rows: int
     sequence_len: int
+
+
+def verify_wide_fibonacci(proof: bytes, log_n_rows: int, sequence_len: int, channel_seed: int | None = None) -> bool:
+    """Host verification of a wide-Fibonacci proof by the library's C++ verifier (no device use);
+    raises StwoError(E_CONSTRAINTS) naming the failed check."""
+    _check(_lib.stwo_b200_verify_wide_fibonacci(proof, len(proof), log_n_rows, sequence_len,
+                                                int(channel_seed is not None), channel_seed or 0))
+    return True
+
+
+def verify_logup_xor(proof: bytes, log_n: int, log_table: int = 16, channel_seed: int | None = None) -> bool:
+    """Host verification of a LogUp XOR-lookup AIR proof (see verify_wide_fibonacci)."""
+    _check(_lib.stwo_b200_verify_logup_xor(proof, len(proof), log_n, log_table, int(channel_seed is not None),
+                                           channel_seed or 0))
+    return True
 
 
 TRACE_REFERENCE = 0   # (1, row) seeds of the reference's trace generator
@@ -439,9 +456,9 @@ class Server:
     free device memory) and the reference's resource profile (0 standard, 1 large, 2 extreme)."""
 
     def __init__(self, ctx: Context, slots: int = 8, profile: int = 1, memory_budget: int = 0,
-                 persistent_workspaces: bool = False):
+                 persistent_workspaces: bool = False, verify: bool = False):
         h = _vp()
-        cfg = ServerConfigC(slots, profile, memory_budget, int(persistent_workspaces))
+        cfg = ServerConfigC(slots, profile, memory_budget, int(persistent_workspaces) | (2 if verify else 0))
         _check(_lib.stwo_b200_server_create(ctx._h, ctypes.byref(cfg), ctypes.byref(h)))
         self._h = h
         self._ctx = ctx

@@ -107,6 +107,7 @@ def test_gpu_proofs_verify(ctx, log_n, W, preset):
     p = ctx.prove_wide_fibonacci(sb.Statement(log_n, W), g, trace_kind=sb.TRACE_SEEDED, trace_seed=42,
                                  channel_seed=9)
     assert verifier.verify_wide_fib(p, log_n, W, channel_seed=9)
+    assert sb.verify_wide_fibonacci(p, log_n, W, channel_seed=9)  # the library's own verifier
 
 
 def mixed_requests(master_seed=2026, count=48):

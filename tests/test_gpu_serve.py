@@ -143,3 +143,15 @@ def test_warmup_presizes_slots(ctx):
         out = [srv.wait(t)[0] for t in ts]
     assert out[0] == ctx.prove_wide_fibonacci(sb.Statement(16, 32), g, trace_kind=sb.TRACE_SEEDED, trace_seed=0)
     assert out[3] == ctx.prove_logup_xor(12, g, seed=1)
+
+
+def test_server_verifies_every_proof(ctx):
+    import stwo_b200 as sb
+    g = _cfg("functional")
+    with sb.Server(ctx, slots=3, profile=2, verify=True) as srv:
+        ts = [srv.submit(sb.Statement(12 + i, 16), g, trace_kind=sb.TRACE_SEEDED, trace_seed=i) for i in range(4)]
+        ts.append(srv.submit_xor(12, g, seed=9))
+        outs = [srv.wait(t)[0] for t in ts]
+    for i in range(4):
+        assert sb.verify_wide_fibonacci(outs[i], 12 + i, 16)
+    assert sb.verify_logup_xor(outs[4], 12)

@@ -60,3 +60,16 @@ def test_xor_air_bad_arguments(ctx):
     with pytest.raises(sb.StwoError) as e:
         ctx.prove_logup_xor(10, _cfg("smoke"), log_table=12)
     assert e.value.status == sb.E_INVALID
+
+
+def test_native_verifier_agrees_on_xor_proofs(ctx):
+    import stwo_b200 as sb
+    for log_n, lt, seed in ((7, 8, None), (14, 16, 12)):
+        p = ctx.prove_logup_xor(log_n, _cfg("functional"), seed=3, log_table=lt, channel_seed=seed)
+        assert sb.verify_logup_xor(p, log_n, lt, channel_seed=seed)
+        with pytest.raises(sb.StwoError):
+            sb.verify_logup_xor(p, log_n, lt, channel_seed=(seed or 0) + 1)
+        d = json.loads(p)
+        d["sampled_values"][1][0][0][0] = (d["sampled_values"][1][0][0][0] + 1) % (2**31 - 1)
+        with pytest.raises(sb.StwoError):
+            sb.verify_logup_xor(json.dumps(d, separators=(",", ":")).encode(), log_n, lt, channel_seed=seed)
