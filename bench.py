@@ -214,7 +214,10 @@ def main():
         return replicas.max_over_ranks(x, device=dev)
 
     # Device-resident traces, a distinct seed per proof (generated untimed by the library's kernel).
-    seeds = [1_000_003 * (rank + 1) + i for i in range(K + W)]
+    # The warm-up batch has at least as many proofs as are in flight, so every prover slot
+    # (stream, pinned staging, workspace) exists before the timed region.
+    WB = max(W, args.in_flight)
+    seeds = [1_000_003 * (rank + 1) + i for i in range(K + WB)]
     traces = []
     for s in seeds:
         t = torch.empty(n_words, dtype=torch.int32, device=dev)
@@ -230,7 +233,7 @@ def main():
         return out
 
     # ---- warmup (both paths)
-    ctx.prove_wide_fibonacci_batch(requests(range(K, K + W)), max_in_flight=args.in_flight)
+    ctx.prove_wide_fibonacci_batch(requests(range(K, K + WB)), max_in_flight=args.in_flight)
     for i in range(K, K + W):
         ctx.prove_wide_fibonacci(st, cfg, trace=traces[i])
     torch.cuda.synchronize()
@@ -403,7 +406,12 @@ def run_mixed48(args, ctx):
     stmts = mixed_statements(2026, 48, 14, 20)
     reqs = [dict(statement=sb.Statement(r["log_n"], r["W"]), config=cfg, trace_kind=sb.TRACE_SEEDED,
                  trace_seed=r["trace_seed"], channel_seed=r["channel_seed"]) for r in stmts]
-    ctx.prove_wide_fibonacci_batch(reqs[:16], max_in_flight=args.in_flight)  # warm-up: every workspace size
+    # warm-up: every prover slot grows its workspace to the largest shape first
+    big = max(stmts, key=lambda r: r["W"] << r["log_n"])
+    ctx.prove_wide_fibonacci_batch([dict(statement=sb.Statement(big["log_n"], big["W"]), config=cfg,
+                                         trace_kind=sb.TRACE_SEEDED, trace_seed=7 + i) for i in range(args.in_flight)],
+                                   max_in_flight=args.in_flight)
+    ctx.prove_wide_fibonacci_batch(reqs[:16], max_in_flight=args.in_flight)
     torch.cuda.synchronize()
     launches0 = sb.kernel_launches()
     with ClockSampler(0) as clocks:

@@ -428,7 +428,7 @@ int32_t WideFibProver::prove(const ProveRequest& req, std::string& out, StageTim
 
   // Wire encoding (src/interop/proof_wire.zig:19-77).
   Json j;
-  j.s.reserve(1 << 16);
+  j.s.reserve(3 << 20);
   j.s += "{\"config\":{\"pow_bits\":"; j.u(cfg.pow_bits);
   j.s += ",\"fri_config\":{\"log_blowup_factor\":"; j.u(B);
   j.s += ",\"log_last_layer_degree_bound\":"; j.u(cfg.log_last_layer_degree_bound);

@@ -5,6 +5,7 @@
 #include <cuda_runtime.h>
 
 #include <array>
+#include <cstdio>
 #include <cstring>
 #include <stdexcept>
 #include <string>
@@ -91,11 +92,69 @@ inline const PointTable& host_points() {
   return pt;
 }
 
+// Proof JSON writer. A proof holds hundreds of thousands of decimal numbers (hash bytes
+// above all), so digits are produced two at a time from a table and appended to a
+// buffer that grows geometrically; a hash is written from per-byte strings.
 struct Json {
   std::string s;
-  void u(uint64_t v) { s += std::to_string(v); }
-  void hash(const uint8_t* h) { s += '['; for (int i = 0; i < 32; ++i) { if (i) s += ','; u(h[i]); } s += ']'; }
-  void qm(QM31 q) { uint32_t w[4]; qstore4(q, w); s += '['; for (int i = 0; i < 4; ++i) { if (i) s += ','; u(w[i]); } s += ']'; }
+  void u(uint64_t v) {
+    static const char* kPairs =
+        "00010203040506070809101112131415161718192021222324252627282930313233343536373839"
+        "40414243444546474849505152535455565758596061626364656667686970717273747576777879"
+        "8081828384858687888990919293949596979899";
+    char buf[24];
+    char* e = buf + sizeof(buf);
+    char* p = e;
+    while (v >= 100) {
+      const unsigned r = (unsigned)(v % 100);
+      v /= 100;
+      p -= 2;
+      p[0] = kPairs[2 * r];
+      p[1] = kPairs[2 * r + 1];
+    }
+    if (v >= 10) {
+      p -= 2;
+      p[0] = kPairs[2 * v];
+      p[1] = kPairs[2 * v + 1];
+    } else {
+      *--p = (char)('0' + v);
+    }
+    s.append(p, e - p);
+  }
+  void hash(const uint8_t* h) {
+    struct Bytes {  // decimal text of every byte value followed by ',', and its length
+      char txt[256][4];
+      uint8_t len[256];
+      Bytes() {
+        for (int b = 0; b < 256; ++b) {
+          char t[8];
+          int n = std::snprintf(t, sizeof(t), "%d,", b);
+          std::memcpy(txt[b], t, 4);
+          len[b] = (uint8_t)n;
+        }
+      }
+    };
+    static const Bytes bytes;
+    char buf[1 + 32 * 4 + 4];
+    size_t n = 0;
+    buf[n++] = '[';
+    for (int i = 0; i < 32; ++i) {
+      std::memcpy(buf + n, bytes.txt[h[i]], 4);  // fixed-size copy; only len bytes are kept
+      n += bytes.len[h[i]];
+    }
+    buf[n - 1] = ']';  // the last ',' closes the list
+    s.append(buf, n);
+  }
+  void qm(QM31 q) {
+    uint32_t w[4];
+    qstore4(q, w);
+    s += '[';
+    for (int i = 0; i < 4; ++i) {
+      if (i) s += ',';
+      u(w[i]);
+    }
+    s += ']';
+  }
 };
 
 // Decommitment plan of a lifted tree at sorted unique leaf positions: the nodes

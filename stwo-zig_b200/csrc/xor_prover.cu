@@ -447,7 +447,7 @@ int32_t LogupXorProver::prove(const XorRequest& req, std::string& out) {
   // Wire encoding: the wide-Fibonacci proof layout with four trees, claimed sums and the
   // statement (log_n, log_table).
   Json j;
-  j.s.reserve(1 << 16);
+  j.s.reserve(3 << 20);
   j.s += "{\"config\":{\"pow_bits\":"; j.u(cfg.pow_bits);
   j.s += ",\"fri_config\":{\"log_blowup_factor\":"; j.u(B);
   j.s += ",\"log_last_layer_degree_bound\":"; j.u(cfg.log_last_layer_degree_bound);

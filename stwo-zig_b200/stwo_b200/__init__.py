@@ -298,7 +298,7 @@ class Context:
                                                      ctypes.byref(times))
         _check(rc)
         del keep
-        proof = buf.raw[: n.value]
+        proof = ctypes.string_at(buf, n.value)
         if with_times:
             return proof, {name: getattr(times, name) for name, _ in StageTimesC._fields_}
         return proof
@@ -316,7 +316,7 @@ class Context:
             buf = ctypes.create_string_buffer(cap)
             rc = _lib.stwo_b200_prove_logup_xor(self._h, ctypes.byref(req), buf, cap, ctypes.byref(n))
         _check(rc)
-        return buf.raw[: n.value]
+        return ctypes.string_at(buf, n.value)
 
     def prove_wide_fibonacci_batch(self, requests: list[dict], max_in_flight: int = 4, with_times: bool = False,
                                    proof_cap: int = 1 << 21):
@@ -339,7 +339,7 @@ class Context:
         _check(_lib.stwo_b200_prove_wide_fibonacci_batch(self._h, arr, n, outs, caps, lens, statuses, max_in_flight,
                                                          times))
         del keeps
-        proofs = [bufs[i].raw[: lens[i]] for i in range(n)]
+        proofs = [ctypes.string_at(bufs[i], lens[i]) for i in range(n)]
         if with_times:
             return proofs, [{k: getattr(times[i], k) for k, _ in StageTimesC._fields_} for i in range(n)]
         return proofs
@@ -492,7 +492,7 @@ class Server:
         _check(rc)
         stats = {name: getattr(st, name) for name, _ in RequestStatsC._fields_ if name != "stages"}
         stats["stages"] = {name: getattr(st.stages, name) for name, _ in StageTimesC._fields_}
-        return buf.raw[: n.value], stats
+        return ctypes.string_at(buf, n.value), stats
 
     def warmup(self, max_log_n_rows: int = 0, max_sequence_len: int = 100, log_blowup: int = 1,
                max_xor_log_n: int = 0) -> None:
