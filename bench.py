@@ -165,7 +165,10 @@ def run_reference(args, rank, world):
 def config_block(args):
     return {"workload": f"wide-Fibonacci 2^{args.log_n}x{args.width}, {args.preset} preset, one proof per step",
             "log_n_rows": args.log_n, "sequence_len": args.width, "protocol": args.preset,
-            "in_flight": args.in_flight, "l2": "inputs larger than L2 (400 MB trace per proof)",
+            "in_flight": args.in_flight,
+            "l2": (f"inputs larger than L2 ({(4 * args.width << args.log_n) / 1e6:.0f} MB trace per proof)"
+                   if (4 * args.width << args.log_n) > 126e6 else
+                   f"{(4 * args.width << args.log_n) / 1e6:.1f} MB trace per proof (fits L2)"),
             "parallelism": "replicas"}
 
 
