@@ -291,9 +291,15 @@ int32_t WideFibProver::prove(const ProveRequest& req, std::string& out, StageTim
   if (req.trace_device) {
     trace = req.trace_device;
   } else if (req.trace_host) {
+    // Host uploads go one at a time (FIFO on the context's lock, each held until its copy has
+    // landed): concurrent copies of several proofs would share the host link and all finish
+    // late, while one after the other each proof starts computing as soon as its own trace is in.
+    std::lock_guard<std::mutex> g(ctx_->h2d_mu);
     SB_CK(cudaMemcpyAsync(b.trace, req.trace_host, (size_t)W * l.N * 4, cudaMemcpyHostToDevice, s));
+    SB_CK(cudaEventRecord(ev_[1], s));
+    SB_CK(cudaEventSynchronize(ev_[1]));
   }
-  SB_CK(cudaEventRecord(ev_[1], s));
+  if (!req.trace_host) SB_CK(cudaEventRecord(ev_[1], s));
   if (!req.trace_device && !req.trace_host) SB_CK(wide_fib_trace(n, W, req.trace_kind, req.trace_seed, b.trace, l.N, s));
   SB_CK(cudaEventRecord(ev_[2], s));
 

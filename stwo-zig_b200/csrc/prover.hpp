@@ -129,6 +129,7 @@ struct Context {
   std::vector<LogupXorProver*> xor_pool;
   cudaStream_t stream = nullptr;
   uint32_t* small = nullptr;  // 256 bytes of device scratch for single-value results (PoW nonce)
+  std::mutex h2d_mu;          // serialises host-to-device trace uploads of concurrent proofs
   std::mutex small_mu;
   ~Context();
   int32_t init(int device, uint32_t tower_log);

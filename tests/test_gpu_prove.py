@@ -135,3 +135,19 @@ def test_mixed_batch_of_48_matches_single_runs(ctx):
     for r, p in list(zip(reqs, batch))[:3]:
         assert verifier.verify_wide_fib(p, r["statement"].log_n_rows, r["statement"].sequence_len,
                                         channel_seed=r["channel_seed"])
+
+
+@pytest.mark.parametrize("log_n,W,over", [
+    (4, 2, dict(log_blowup_factor=1, n_queries=3)),                                   # minimum width
+    (7, 9, dict(log_blowup_factor=3, n_queries=9, log_last_layer_degree_bound=2)),   # blowup 8
+    (8, 5, dict(log_blowup_factor=4, n_queries=4, log_last_layer_degree_bound=0)),   # blowup 16
+    (10, 12, dict(n_queries=120, log_last_layer_degree_bound=3)),                     # many queries
+    (9, 3, dict(pow_bits=14, n_queries=2))])
+def test_protocol_variants_match_oracle(ctx, log_n, W, over):
+    import stwo_b200 as sb
+    o, g = cfg_pair("functional", **over)
+    ref = oracle.prove_wide_fib(log_n, W, o, trace_kind=1, trace_seed=31 * log_n + W, channel_seed=0)
+    got = ctx.prove_wide_fibonacci(sb.Statement(log_n, W), g, trace_kind=sb.TRACE_SEEDED,
+                                   trace_seed=31 * log_n + W, channel_seed=0)
+    assert got == ref
+    assert sb.verify_wide_fibonacci(got, log_n, W, channel_seed=0)

@@ -65,3 +65,16 @@ def test_rejects_malformed_input(bad):
     with pytest.raises(sb.StwoError) as e:
         sb.verify_wide_fibonacci(bad, 5, 8)
     assert e.value.status == sb.E_CONSTRAINTS
+
+
+@pytest.mark.parametrize("log_n,W,over", [
+    (4, 2, dict(n_queries=3)), (7, 9, dict(log_blowup_factor=3, n_queries=9, log_last_layer_degree_bound=2)),
+    (8, 5, dict(log_blowup_factor=4, n_queries=4)), (10, 12, dict(n_queries=120, log_last_layer_degree_bound=3)),
+    (9, 3, dict(pow_bits=14, n_queries=2))])
+def test_protocol_variants_verify_in_both_verifiers(log_n, W, over):
+    import verifier
+    sb = _sb()
+    p = oracle.prove_wide_fib(log_n, W, oracle.config("functional", **over), trace_kind=1, trace_seed=31 * log_n + W,
+                              channel_seed=0)
+    assert verifier.verify_wide_fib(p, log_n, W, channel_seed=0)
+    assert sb.verify_wide_fibonacci(p, log_n, W, channel_seed=0)
