@@ -69,7 +69,9 @@ __device__ void fold_levels(uint32_t* sm, uint32_t count, uint32_t levels, uint8
   }
 }
 
-__global__ void __launch_bounds__(LEAF_THREADS) k_merkle_leaves(uint32_t log_size, uint32_t n_cols,
+// Six CTAs per SM (40 registers, a few spilled to L1): measured 11% faster than the
+// unconstrained 62-register build (0.847 vs 0.953 ms for a 2^21 x 100 commit).
+__global__ void __launch_bounds__(LEAF_THREADS, 6) k_merkle_leaves(uint32_t log_size, uint32_t n_cols,
                                                                  const uint32_t* __restrict__ cols, uint64_t stride,
                                                                  uint8_t* layers, Seeds seeds, uint32_t levels,
                                                                  uint32_t one) {
