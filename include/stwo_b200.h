@@ -75,9 +75,11 @@ typedef struct {
   uint64_t channel_seed;
 } stwo_b200_wide_fib_request;
 
-/* Device time per proving stage, in milliseconds. */
+/* Device time per proving stage, in milliseconds; host_encode is the host time after the last device
+ * stage (JSON wire encoding and the OODS self-check). */
 typedef struct {
   float upload, trace, main_commit, composition, composition_commit, oods, quotients, fri, pow, decommit, total;
+  float host_encode;
 } stwo_b200_stage_times;
 
 /* ---- Runtime --------------------------------------------------------------------------------- */

@@ -18,6 +18,8 @@ void note_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
 uint64_t launch_count() { return g_launches.load(std::memory_order_relaxed); }
 }  // namespace sb
 
+static_assert(sizeof(sb::StageTimes) == sizeof(stwo_b200_stage_times), "stage times layout");
+
 namespace {
 
 thread_local std::string g_last_error;

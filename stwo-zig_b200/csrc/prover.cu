@@ -10,6 +10,7 @@
 // PoW, decommit), src/prover/fri.zig:163-850 (FRI layers and decommitment).
 #include <algorithm>
 #include <array>
+#include <chrono>
 #include <cstring>
 #include <stdexcept>
 
@@ -432,6 +433,7 @@ int32_t WideFibProver::prove(const ProveRequest& req, std::string& out, StageTim
     if (grc != OK) return fail(grc, gerr);
   }
 
+  const auto t_encode = std::chrono::steady_clock::now();
   // Wire encoding (src/interop/proof_wire.zig:19-77).
   Json j;
   j.s.reserve(3 << 20);
@@ -495,6 +497,8 @@ int32_t WideFibProver::prove(const ProveRequest& req, std::string& out, StageTim
     times->pow = el(8, 9);
     times->decommit = el(9, 10);
     times->total = el(0, 10);
+    times->host_encode =
+        std::chrono::duration<float, std::milli>(std::chrono::steady_clock::now() - t_encode).count();
   }
   out.swap(j.s);
   return OK;

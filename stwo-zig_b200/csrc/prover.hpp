@@ -29,10 +29,11 @@ struct ProveRequest {
   uint64_t channel_seed = 0;
 };
 
-// Stage timings of one proof (milliseconds of device time between events).
+// Stage timings of one proof (milliseconds of device time between events), and the host time
+// spent after the last device stage (proof encoding and the OODS self-check).
 struct StageTimes {
   float upload = 0, trace = 0, main_commit = 0, composition = 0, composition_commit = 0, oods = 0,
-        quotients = 0, fri = 0, pow = 0, decommit = 0, total = 0;
+        quotients = 0, fri = 0, pow = 0, decommit = 0, total = 0, host_encode = 0;
 };
 
 // Status codes shared with the C ABI.

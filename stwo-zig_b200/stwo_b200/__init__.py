@@ -77,7 +77,8 @@ class ServerSnapshotC(ctypes.Structure):
 
 class StageTimesC(ctypes.Structure):
     _fields_ = [(n, ctypes.c_float) for n in ("upload", "trace", "main_commit", "composition", "composition_commit",
-                                              "oods", "quotients", "fri", "pow", "decommit", "total")]
+                                              "oods", "quotients", "fri", "pow", "decommit", "total",
+                                              "host_encode")]
 
 
 class RequestStatsC(ctypes.Structure):
