@@ -436,25 +436,25 @@ int32_t WideFibProver::prove(const ProveRequest& req, std::string& out, StageTim
   const auto t_encode = std::chrono::steady_clock::now();
   // Wire encoding (src/interop/proof_wire.zig:19-77).
   Json j;
-  j.s.reserve(3 << 20);
-  j.s += "{\"config\":{\"pow_bits\":"; j.u(cfg.pow_bits);
-  j.s += ",\"fri_config\":{\"log_blowup_factor\":"; j.u(B);
-  j.s += ",\"log_last_layer_degree_bound\":"; j.u(cfg.log_last_layer_degree_bound);
-  j.s += ",\"n_queries\":"; j.u(cfg.n_queries);
-  j.s += ",\"fold_step\":1},\"lifting_log_size\":null},\"commitments\":[";
-  j.hash(root0); j.s += ','; j.hash(root1); j.s += ','; j.hash(root2);
-  j.s += "],\"sampled_values\":[[],[";
-  for (uint32_t c = 0; c < W; ++c) { if (c) j.s += ','; j.s += '['; j.qm(sampled[c]); j.s += ']'; }
-  j.s += "],[";
-  for (uint32_t c = 0; c < 8; ++c) { if (c) j.s += ','; j.s += '['; j.qm(sampled[W + c]); j.s += ']'; }
-  j.s += "]],\"decommitments\":[";
-  for (size_t t = 0; t < 3; ++t) { if (t) j.s += ','; j.s += "{\"hash_witness\":"; plan.json_witness(j, t); j.s += '}'; }
-  j.s += "],\"queried_values\":[";
-  for (size_t t = 0; t < 3; ++t) { if (t) j.s += ','; plan.json_queried(j, t); }
-  j.s += "],\"proof_of_work\":"; j.u(fr.nonce);
-  j.s += ",\"fri_proof\":";
+  j.reserve(3 << 20);
+  j.lit("{\"config\":{\"pow_bits\":"); j.u(cfg.pow_bits);
+  j.lit(",\"fri_config\":{\"log_blowup_factor\":"); j.u(B);
+  j.lit(",\"log_last_layer_degree_bound\":"); j.u(cfg.log_last_layer_degree_bound);
+  j.lit(",\"n_queries\":"); j.u(cfg.n_queries);
+  j.lit(",\"fold_step\":1},\"lifting_log_size\":null},\"commitments\":[");
+  j.hash(root0); j.ch(','); j.hash(root1); j.ch(','); j.hash(root2);
+  j.lit("],\"sampled_values\":[[],[");
+  for (uint32_t c = 0; c < W; ++c) { if (c) j.ch(','); j.ch('['); j.qm(sampled[c]); j.ch(']'); }
+  j.lit("],[");
+  for (uint32_t c = 0; c < 8; ++c) { if (c) j.ch(','); j.ch('['); j.qm(sampled[W + c]); j.ch(']'); }
+  j.lit("]],\"decommitments\":[");
+  for (size_t t = 0; t < 3; ++t) { if (t) j.ch(','); j.lit("{\"hash_witness\":"); plan.json_witness(j, t); j.ch('}'); }
+  j.lit("],\"queried_values\":[");
+  for (size_t t = 0; t < 3; ++t) { if (t) j.ch(','); plan.json_queried(j, t); }
+  j.lit("],\"proof_of_work\":"); j.u(fr.nonce);
+  j.lit(",\"fri_proof\":");
   plan.json_fri(j, fr);
-  j.s += '}';
+  j.ch('}');
 
   // Prover self-check of the composition OODS value (src/prover/prove.zig:366-386).
   {
@@ -500,7 +500,7 @@ int32_t WideFibProver::prove(const ProveRequest& req, std::string& out, StageTim
     times->host_encode =
         std::chrono::duration<float, std::milli>(std::chrono::steady_clock::now() - t_encode).count();
   }
-  out.swap(j.s);
+  out = j.str();
   return OK;
 }
 

@@ -214,9 +214,9 @@ int32_t DecommitPlan::gather(uint8_t* scratch, size_t scratch_bytes, uint8_t* pi
 }
 
 void DecommitPlan::hash_list(Json& j, size_t first, size_t count) const {
-  j.s += '[';
-  for (size_t i = 0; i < count; ++i) { if (i) j.s += ','; j.hash(gh_ + (first + i) * 32); }
-  j.s += ']';
+  j.ch('[');
+  for (size_t i = 0; i < count; ++i) { if (i) j.ch(','); j.hash(gh_ + (first + i) * 32); }
+  j.ch(']');
 }
 
 void DecommitPlan::json_witness(Json& j, size_t tree) const {
@@ -225,38 +225,38 @@ void DecommitPlan::json_witness(Json& j, size_t tree) const {
 
 void DecommitPlan::json_queried(Json& j, size_t tree) const {
   const TreePlan& tp = trees_[tree];
-  j.s += '[';
+  j.ch('[');
   for (size_t c = 0; c < tp.n_cols; ++c) {
-    if (c) j.s += ',';
-    j.s += '[';
-    for (size_t q = 0; q < n_queries_; ++q) { if (q) j.s += ','; j.u(gw_[tp.word0 + c * n_queries_ + q]); }
-    j.s += ']';
+    if (c) j.ch(',');
+    j.ch('[');
+    for (size_t q = 0; q < n_queries_; ++q) { if (q) j.ch(','); j.u(gw_[tp.word0 + c * n_queries_ + q]); }
+    j.ch(']');
   }
-  j.s += ']';
+  j.ch(']');
 }
 
 void DecommitPlan::json_fri(Json& j, const FriResult& fr) const {
   auto layer = [&](size_t k) {
     const LayerPlan& lp = fri_[k];
-    j.s += "{\"fri_witness\":[";
+    j.lit("{\"fri_witness\":[");
     for (size_t i = 0; i < lp.n_wit; ++i) {
-      if (i) j.s += ',';
+      if (i) j.ch(',');
       const uint32_t* w = gw_ + lp.wit_word0 + 4 * i;
       j.qm(qmake(w[0], w[1], w[2], w[3]));
     }
-    j.s += "],\"decommitment\":{\"hash_witness\":";
+    j.lit("],\"decommitment\":{\"hash_witness\":");
     hash_list(j, lp.hash0, lp.n_hash);
-    j.s += "},\"commitment\":";
+    j.lit("},\"commitment\":");
     j.hash(fr.roots[k].data());
-    j.s += '}';
+    j.ch('}');
   };
-  j.s += "{\"first_layer\":";
+  j.lit("{\"first_layer\":");
   layer(0);
-  j.s += ",\"inner_layers\":[";
-  for (size_t k = 1; k < fri_.size(); ++k) { if (k > 1) j.s += ','; layer(k); }
-  j.s += "],\"last_layer_poly\":[";
-  for (size_t i = 0; i < fr.last_coeffs.size(); ++i) { if (i) j.s += ','; j.qm(fr.last_coeffs[i]); }
-  j.s += "]}";
+  j.lit(",\"inner_layers\":[");
+  for (size_t k = 1; k < fri_.size(); ++k) { if (k > 1) j.ch(','); layer(k); }
+  j.lit("],\"last_layer_poly\":[");
+  for (size_t i = 0; i < fr.last_coeffs.size(); ++i) { if (i) j.ch(','); j.qm(fr.last_coeffs[i]); }
+  j.lit("]}");
 }
 
 }  // namespace sb

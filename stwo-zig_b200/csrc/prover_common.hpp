@@ -4,8 +4,11 @@
 #pragma once
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <array>
 #include <cstdio>
+#include <cstdlib>
+#include <new>
 #include <cstring>
 #include <stdexcept>
 #include <string>
@@ -93,68 +96,110 @@ inline const PointTable& host_points() {
 }
 
 // Proof JSON writer. A proof holds hundreds of thousands of decimal numbers (hash bytes
-// above all), so digits are produced two at a time from a table and appended to a
-// buffer that grows geometrically; a hash is written from per-byte strings.
-struct Json {
-  std::string s;
+// above all), so the text goes straight into a growable byte buffer: digits two at a time
+// from a table, hashes from per-byte strings, one bounds check per item.
+class Json {
+ public:
+  Json() = default;
+  Json(const Json&) = delete;
+  Json& operator=(const Json&) = delete;
+  ~Json() { std::free(buf_); }
+  void reserve(size_t k) { grow(k); }
+  void ch(char c) {
+    grow(1);
+    buf_[n_++] = c;
+  }
+  template <size_t K>
+  void lit(const char (&text)[K]) {  // a string literal, without its terminator
+    grow(K - 1);
+    std::memcpy(buf_ + n_, text, K - 1);
+    n_ += K - 1;
+  }
   void u(uint64_t v) {
-    static const char* kPairs =
-        "00010203040506070809101112131415161718192021222324252627282930313233343536373839"
-        "40414243444546474849505152535455565758596061626364656667686970717273747576777879"
-        "8081828384858687888990919293949596979899";
-    char buf[24];
-    char* e = buf + sizeof(buf);
-    char* p = e;
-    while (v >= 100) {
-      const unsigned r = (unsigned)(v % 100);
-      v /= 100;
-      p -= 2;
-      p[0] = kPairs[2 * r];
-      p[1] = kPairs[2 * r + 1];
-    }
-    if (v >= 10) {
-      p -= 2;
-      p[0] = kPairs[2 * v];
-      p[1] = kPairs[2 * v + 1];
-    } else {
-      *--p = (char)('0' + v);
-    }
-    s.append(p, e - p);
+    grow(20);
+    n_ += digits(v, buf_ + n_);
   }
   void hash(const uint8_t* h) {
-    struct Bytes {  // decimal text of every byte value followed by ',', and its length
-      char txt[256][4];
-      uint8_t len[256];
-      Bytes() {
-        for (int b = 0; b < 256; ++b) {
-          char t[8];
-          int n = std::snprintf(t, sizeof(t), "%d,", b);
-          std::memcpy(txt[b], t, 4);
-          len[b] = (uint8_t)n;
-        }
-      }
-    };
-    static const Bytes bytes;
-    char buf[1 + 32 * 4 + 4];
-    size_t n = 0;
-    buf[n++] = '[';
+    const Bytes& t = bytes();
+    grow(1 + 32 * 4);
+    char* p = buf_ + n_;
+    *p++ = '[';
     for (int i = 0; i < 32; ++i) {
-      std::memcpy(buf + n, bytes.txt[h[i]], 4);  // fixed-size copy; only len bytes are kept
-      n += bytes.len[h[i]];
+      std::memcpy(p, t.txt[h[i]], 4);  // fixed-size copy; only len bytes are kept
+      p += t.len[h[i]];
     }
-    buf[n - 1] = ']';  // the last ',' closes the list
-    s.append(buf, n);
+    p[-1] = ']';  // the last ',' closes the list
+    n_ = p - buf_;
   }
   void qm(QM31 q) {
     uint32_t w[4];
     qstore4(q, w);
-    s += '[';
+    grow(4 * 11 + 2);
+    char* p = buf_ + n_;
+    *p++ = '[';
     for (int i = 0; i < 4; ++i) {
-      if (i) s += ',';
-      u(w[i]);
+      if (i) *p++ = ',';
+      p += digits(w[i], p);
     }
-    s += ']';
+    *p++ = ']';
+    n_ = p - buf_;
   }
+  std::string str() const { return std::string(buf_ ? buf_ : "", n_); }
+
+ private:
+  struct Bytes {  // decimal text of every byte value followed by ',', and its length
+    char txt[256][4];
+    uint8_t len[256];
+    Bytes() {
+      for (int b = 0; b < 256; ++b) {
+        char t[8];
+        int n = std::snprintf(t, sizeof(t), "%d,", b);
+        std::memcpy(txt[b], t, 4);
+        len[b] = (uint8_t)n;
+      }
+    }
+  };
+  static const Bytes& bytes() {
+    static const Bytes b;
+    return b;
+  }
+  // Writes v in decimal at p; returns the number of characters.
+  static size_t digits(uint64_t v, char* p) {
+    static const char* kPairs =
+        "00010203040506070809101112131415161718192021222324252627282930313233343536373839"
+        "40414243444546474849505152535455565758596061626364656667686970717273747576777879"
+        "8081828384858687888990919293949596979899";
+    char tmp[24];
+    char* e = tmp + sizeof(tmp);
+    char* q = e;
+    while (v >= 100) {
+      const unsigned r = (unsigned)(v % 100);
+      v /= 100;
+      q -= 2;
+      q[0] = kPairs[2 * r];
+      q[1] = kPairs[2 * r + 1];
+    }
+    if (v >= 10) {
+      q -= 2;
+      q[0] = kPairs[2 * v];
+      q[1] = kPairs[2 * v + 1];
+    } else {
+      *--q = (char)('0' + v);
+    }
+    const size_t k = e - q;
+    std::memcpy(p, q, k);
+    return k;
+  }
+  void grow(size_t k) {
+    if (n_ + k <= cap_) return;
+    size_t cap = std::max(cap_ * 2, n_ + k + 4096);
+    char* nb = static_cast<char*>(std::realloc(buf_, cap));
+    if (!nb) throw std::bad_alloc();
+    buf_ = nb;
+    cap_ = cap;
+  }
+  char* buf_ = nullptr;
+  size_t n_ = 0, cap_ = 0;
 };
 
 // Decommitment plan of a lifted tree at sorted unique leaf positions: the nodes

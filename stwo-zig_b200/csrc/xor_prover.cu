@@ -447,35 +447,35 @@ int32_t LogupXorProver::prove(const XorRequest& req, std::string& out) {
   // Wire encoding: the wide-Fibonacci proof layout with four trees, claimed sums and the
   // statement (log_n, log_table).
   Json j;
-  j.s.reserve(3 << 20);
-  j.s += "{\"config\":{\"pow_bits\":"; j.u(cfg.pow_bits);
-  j.s += ",\"fri_config\":{\"log_blowup_factor\":"; j.u(B);
-  j.s += ",\"log_last_layer_degree_bound\":"; j.u(cfg.log_last_layer_degree_bound);
-  j.s += ",\"n_queries\":"; j.u(cfg.n_queries);
-  j.s += ",\"fold_step\":1},\"lifting_log_size\":null},\"statement\":{\"log_n\":"; j.u(req.log_n);
-  j.s += ",\"log_table\":"; j.u(req.log_table);
-  j.s += "},\"commitments\":[";
-  for (int t = 0; t < 4; ++t) { if (t) j.s += ','; j.hash(roots[t]); }
-  j.s += "],\"claimed_sums\":["; j.qm(claimed[0]); j.s += ','; j.qm(claimed[1]);
-  j.s += "],\"sampled_values\":[[";
-  for (int c = 0; c < 4; ++c) { if (c) j.s += ','; j.s += '['; j.qm(at_p[c]); j.s += ']'; }
-  j.s += "],[";
-  for (int c = 0; c < 4; ++c) { if (c) j.s += ','; j.s += '['; j.qm(at_p[4 + c]); j.s += ']'; }
-  j.s += "],[";
+  j.reserve(3 << 20);
+  j.lit("{\"config\":{\"pow_bits\":"); j.u(cfg.pow_bits);
+  j.lit(",\"fri_config\":{\"log_blowup_factor\":"); j.u(B);
+  j.lit(",\"log_last_layer_degree_bound\":"); j.u(cfg.log_last_layer_degree_bound);
+  j.lit(",\"n_queries\":"); j.u(cfg.n_queries);
+  j.lit(",\"fold_step\":1},\"lifting_log_size\":null},\"statement\":{\"log_n\":"); j.u(req.log_n);
+  j.lit(",\"log_table\":"); j.u(req.log_table);
+  j.lit("},\"commitments\":[");
+  for (int t = 0; t < 4; ++t) { if (t) j.ch(','); j.hash(roots[t]); }
+  j.lit("],\"claimed_sums\":["); j.qm(claimed[0]); j.ch(','); j.qm(claimed[1]);
+  j.lit("],\"sampled_values\":[[");
+  for (int c = 0; c < 4; ++c) { if (c) j.ch(','); j.ch('['); j.qm(at_p[c]); j.ch(']'); }
+  j.lit("],[");
+  for (int c = 0; c < 4; ++c) { if (c) j.ch(','); j.ch('['); j.qm(at_p[4 + c]); j.ch(']'); }
+  j.lit("],[");
   for (int c = 0; c < 8; ++c) {
-    if (c) j.s += ',';
-    j.s += '['; j.qm(at_p[16 + c]); j.s += ','; j.qm(at_p[8 + c]); j.s += ']';
+    if (c) j.ch(',');
+    j.ch('['); j.qm(at_p[16 + c]); j.ch(','); j.qm(at_p[8 + c]); j.ch(']');
   }
-  j.s += "],[";
-  for (int c = 0; c < 8; ++c) { if (c) j.s += ','; j.s += '['; j.qm(at_p[24 + c]); j.s += ']'; }
-  j.s += "]],\"decommitments\":[";
-  for (size_t t = 0; t < 4; ++t) { if (t) j.s += ','; j.s += "{\"hash_witness\":"; plan.json_witness(j, t); j.s += '}'; }
-  j.s += "],\"queried_values\":[";
-  for (size_t t = 0; t < 4; ++t) { if (t) j.s += ','; plan.json_queried(j, t); }
-  j.s += "],\"proof_of_work\":"; j.u(fr.nonce);
-  j.s += ",\"fri_proof\":";
+  j.lit("],[");
+  for (int c = 0; c < 8; ++c) { if (c) j.ch(','); j.ch('['); j.qm(at_p[24 + c]); j.ch(']'); }
+  j.lit("]],\"decommitments\":[");
+  for (size_t t = 0; t < 4; ++t) { if (t) j.ch(','); j.lit("{\"hash_witness\":"); plan.json_witness(j, t); j.ch('}'); }
+  j.lit("],\"queried_values\":[");
+  for (size_t t = 0; t < 4; ++t) { if (t) j.ch(','); plan.json_queried(j, t); }
+  j.lit("],\"proof_of_work\":"); j.u(fr.nonce);
+  j.lit(",\"fri_proof\":");
   plan.json_fri(j, fr);
-  j.s += '}';
+  j.ch('}');
 
   // Self-checks: the lookup balances and the composition matches the constraints at P.
   if (!qiszero(qadd(claimed[0], claimed[1]))) return fail(E_CONSTRAINTS, "LogUp claimed sums do not cancel");
@@ -509,7 +509,7 @@ int32_t LogupXorProver::prove(const XorRequest& req, std::string& out) {
     const QM31 expect = qmul(qadd(qmul(random_coeff, c_main), c_table), qinv(x));
     if (!qeq(expect, comp_oods)) return fail(E_CONSTRAINTS, "constraints not satisfied at the OODS point");
   }
-  out.swap(j.s);
+  out = j.str();
   return OK;
 }
 
