@@ -1,13 +1,16 @@
 """Benchmark of the B200 wide-Fibonacci prover (one JSON line on rank 0).
 
 Workload: wide-Fibonacci AIR, 2^20 rows x 100 columns, `secure` preset (pow 26,
-70 queries, blowup 2, FRI to a constant), seeded uniform col0/col1 traces (a
-distinct seed per proof), every proof byte-identical to the CPU oracle's.
-A step is one proof. `value` is the batched throughput (proofs in flight on
-separate streams) with traces already resident in HBM; the single-proof path
-(one proof at a time) is reported beside it with its p50/p99 latency; `e2e`
-goes through the C ABI with pinned host traces (host-to-device copy of every
-trace and device-to-host of every proof inside the timed region).
+70 queries, blowup 2, FRI to a constant), seeded uniform col0/col1 traces, every
+proof byte-identical to the CPU oracle's. A step is one batch of `--batch` proofs
+(default 8). `value` is the batched throughput: the K * batch proofs of the timed
+region run back to back through the in-flight queue (proofs on separate streams)
+with traces already resident in HBM. The single-proof path (one proof at a time)
+is reported beside it with its p50/p99 latency. `e2e` goes through the C ABI from
+pinned host memory: each proof's col0/col1 uploaded and the rest of its trace
+derived on the device (the column source the reference's accelerated backend
+uses), proofs back on the host; `e2e_full_trace` uploads every trace column.
+The reference arm times the CPU prover, one proof per step (a bounded sample).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
     python bench.py --workload mixed48      # 48 mixed-shape proofs in one submission
@@ -17,7 +20,8 @@ trace and device-to-host of every proof inside the timed region).
                                             # fold_circle_into_line 2^21 and fold_line to 2^4
 
 N > 1 runs under torchrun as independent replicas (proofs do not shard): each
-rank proves its own K proofs; value = N*K / max over ranks of the timed region.
+rank proves its own K * batch proofs; value = N*K*batch / max over ranks of the
+timed region.
 """
 from __future__ import annotations
 
@@ -36,6 +40,8 @@ sys.path.insert(0, os.path.join(ROOT, "stwo-zig_b200"))
 METRIC = "proofs/s & p99 ms: batched vs single-proof on 1 B200, wide-Fib 2^20x100, exact"
 LOG_N, WIDTH = 20, 100
 IN_FLIGHT = 8
+BATCH = 8
+MAX_RESIDENT_TRACES = 48
 
 
 def parse():
@@ -48,6 +54,7 @@ def parse():
     ap.add_argument("--width", type=int, default=WIDTH)
     ap.add_argument("--preset", default="secure")
     ap.add_argument("--in-flight", type=int, default=IN_FLIGHT)
+    ap.add_argument("--batch", type=int, default=BATCH, help="proofs per step (headline workload)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--workload", default="headline", choices=["headline", "mixed48", "serve", "kernels128"])
     ap.add_argument("--rates", default="25,50,100,200")
@@ -162,9 +169,11 @@ def run_reference(args, rank, world):
     print(json.dumps(out), flush=True)
 
 
-def config_block(args):
-    return {"workload": f"wide-Fibonacci 2^{args.log_n}x{args.width}, {args.preset} preset, one proof per step",
+def config_block(args, batch=1):
+    per_step = "one proof per step" if batch == 1 else f"one batch of {batch} proofs per step"
+    return {"workload": f"wide-Fibonacci 2^{args.log_n}x{args.width}, {args.preset} preset, {per_step}",
             "log_n_rows": args.log_n, "sequence_len": args.width, "protocol": args.preset,
+            "proofs_per_step": batch,
             "in_flight": args.in_flight,
             "l2": (f"inputs larger than L2 ({(4 * args.width << args.log_n) / 1e6:.0f} MB trace per proof)"
                    if (4 * args.width << args.log_n) > 126e6 else
@@ -216,11 +225,14 @@ def main():
     def max_over_ranks(x: float) -> float:
         return replicas.max_over_ranks(x, device=dev)
 
-    # Device-resident traces, a distinct seed per proof (generated untimed by the library's kernel).
-    # The warm-up batch has at least as many proofs as are in flight, so every prover slot
-    # (stream, pinned staging, workspace) exists before the timed region.
-    WB = max(W, args.in_flight)
-    seeds = [1_000_003 * (rank + 1) + i for i in range(K + WB)]
+    # Device-resident traces (generated untimed by the library's kernel). A step is one batch of
+    # `--batch` proofs; the K * batch proofs of the timed region go through the in-flight queue
+    # back to back. Up to 48 distinct traces are kept resident; proof i uses trace i % 48 and, from
+    # its second use on, a channel seed of its own, so every proof is a distinct statement proven
+    # in full (nothing is reused between proofs but the input columns).
+    NB = K * args.batch
+    n_traces = min(NB, MAX_RESIDENT_TRACES)
+    seeds = [1_000_003 * (rank + 1) + i for i in range(n_traces)]
     traces = []
     for s in seeds:
         t = torch.empty(n_words, dtype=torch.int32, device=dev)
@@ -228,47 +240,60 @@ def main():
         traces.append(t)
     torch.cuda.synchronize()
 
-    def requests(idx, host=None):
+    def requests(idx, source=None, salt=0):
+        n_inputs = len(host_full) if source == "full_host" else n_traces
         out = []
         for i in idx:
-            tr = host[i % len(host)] if host is not None else traces[i]
-            out.append(dict(statement=st, config=cfg, trace=tr))
+            j = i % n_inputs
+            cs = None if i < n_inputs and not salt else salt * 1_000_000 + i
+            if source == "first_columns":
+                r = dict(statement=st, config=cfg, trace=host_two[j], trace_kind=sb.TRACE_FIRST_COLUMNS)
+            elif source == "full_host":
+                r = dict(statement=st, config=cfg, trace=host_full[j])
+            else:
+                r = dict(statement=st, config=cfg, trace=traces[j])
+            if cs is not None:
+                r["channel_seed"] = cs
+            out.append(r)
         return out
 
-    # ---- warmup (both paths)
-    ctx.prove_wide_fibonacci_batch(requests(range(K, K + WB)), max_in_flight=args.in_flight)
-    for i in range(K, K + W):
-        ctx.prove_wide_fibonacci(st, cfg, trace=traces[i])
+    # ---- warmup (both paths): at least one proof per in-flight slot, so every prover slot
+    # (stream, pinned staging, workspace) exists before the timed region
+    WB = max(W, args.in_flight)
+    ctx.prove_wide_fibonacci_batch(requests(range(WB), salt=1), max_in_flight=args.in_flight)
+    for r in requests(range(W), salt=2):
+        ctx.prove_wide_fibonacci(**r)
     torch.cuda.synchronize()
 
     stream = torch.cuda.current_stream()
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
 
-    # ---- batched path: the headline value (clocks sampled over all three timed regions)
+    # ---- batched path: the headline value (clocks sampled over all timed regions)
     launches0 = sb.kernel_launches()
     clocks = ClockSampler(local).__enter__()
+    reqs_b = requests(range(NB))
     barrier()
     torch.cuda.synchronize()
     ev0.record(stream)
-    proofs_b, times_b = ctx.prove_wide_fibonacci_batch(requests(range(K)), max_in_flight=args.in_flight,
-                                                       with_times=True)
+    proofs_b, times_b = ctx.prove_wide_fibonacci_batch(reqs_b, max_in_flight=args.in_flight, with_times=True)
     ev1.record(stream)
     torch.cuda.synchronize()
     barrier()
     batched_ms = max_over_ranks(ev0.elapsed_time(ev1))
     launches = sb.kernel_launches() - launches0
-    value = world * K / (batched_ms / 1e3)
+    value = world * NB / (batched_ms / 1e3)
 
-    # ---- single-proof path
+    # ---- single-proof path: one proof at a time
+    n_single = min(NB, 32)
     lat = []
     barrier()
     torch.cuda.synchronize()
     e_start, e_end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e_start.record(stream)
-    for i in range(K):
+    for i in range(n_single):
         a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         a.record(stream)
-        p = ctx.prove_wide_fibonacci(st, cfg, trace=traces[i])
+        p = ctx.prove_wide_fibonacci(**reqs_b[i])
         b.record(stream)
         b.synchronize()
         lat.append(a.elapsed_time(b))
@@ -278,31 +303,52 @@ def main():
     barrier()
     single_ms = max_over_ranks(e_start.elapsed_time(e_end))
 
-    # ---- end to end through the C ABI: pinned host traces, proofs back to the host
-    host_traces = []
-    for i in range(min(K, 3)):
-        h = torch.empty(n_words, dtype=torch.int32, pin_memory=True)
-        h.copy_(traces[i])
-        host_traces.append(h.numpy().view("uint32"))  # same pinned pages, the ABI's uint32 type
+    # ---- end to end through the C ABI from pinned host memory, proofs back on the host.
+    # Headline: the wide-Fibonacci column source the reference's accelerated backend uses (the
+    # trace materialised on the device from its recurrence): col0/col1 of every proof uploaded
+    # (8 B per row), the other columns derived on the device inside the timed region.
+    host_two, host_full = [], []
+    for t in traces:
+        h = torch.empty(2 << args.log_n, dtype=torch.int32, pin_memory=True)
+        h.copy_(t[: 2 << args.log_n])
+        host_two.append(h.numpy().view("uint32").reshape(2, -1))
     torch.cuda.synchronize()
     barrier()
     ev0.record(stream)
-    proofs_e = ctx.prove_wide_fibonacci_batch(requests(range(K), host=host_traces), max_in_flight=args.in_flight)
+    proofs_e = ctx.prove_wide_fibonacci_batch(requests(range(NB), source="first_columns"),
+                                              max_in_flight=args.in_flight)
     ev1.record(stream)
     torch.cuda.synchronize()
     barrier()
     e2e_ms = max_over_ranks(ev0.elapsed_time(ev1))
-    clocks.__exit__(None, None, None)
-    for i in range(len(host_traces)):
-        assert proofs_e[i] == proofs_b[i], "host-trace and device-trace proofs differ"
+    assert proofs_e == proofs_b, "first-column-source and device-trace proofs differ"
     proof_bytes = statistics.mean(len(p) for p in proofs_e)
+
+    # Also: every trace column uploaded (4 B per cell; the host link bounds this one).
+    n_full = min(NB, 16)
+    for i in range(min(n_full, 3)):
+        h = torch.empty(n_words, dtype=torch.int32, pin_memory=True)
+        h.copy_(traces[i])
+        host_full.append(h.numpy().view("uint32"))  # same pinned pages, the ABI's uint32 type
+    torch.cuda.synchronize()
+    barrier()
+    ev0.record(stream)
+    proofs_f = ctx.prove_wide_fibonacci_batch(requests(range(n_full), source="full_host"),
+                                              max_in_flight=args.in_flight)
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    barrier()
+    e2e_full_ms = max_over_ranks(ev0.elapsed_time(ev1))
+    clocks.__exit__(None, None, None)
+    for i in range(len(host_full)):
+        assert proofs_f[i] == proofs_b[i], "host-trace and device-trace proofs differ"
 
     # ---- the reference's published shape: one functional-preset proof (pow 10, 3 queries) at a time
     fcfg = sb.PcsConfig.preset("functional")
     for i in range(2):
         ctx.prove_wide_fibonacci(st, fcfg, trace=traces[i])
     flat = []
-    for i in range(min(K, 8)):
+    for i in range(min(n_traces, 8)):
         a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         a.record(stream)
         ctx.prove_wide_fibonacci(st, fcfg, trace=traces[i])
@@ -345,11 +391,13 @@ def main():
     out = {
         "metric": METRIC, "value": value, "unit": "proofs/s", "n_gpus": world, "steps": K, "warmup": W,
         "ms_per_step": batched_ms / K, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-        "dtype": "u32", "data": "synthetic: seeded uniform col0/col1 wide-Fibonacci traces, a distinct seed per proof",
-        "config": config_block(args),
+        "dtype": "u32", "data": (f"synthetic: seeded uniform col0/col1 wide-Fibonacci traces, {n_traces} resident; "
+                                 "a distinct (trace, channel seed) pair per proof"),
+        "config": config_block(args, args.batch),
         "batched": {"proofs_per_s": value, "in_flight": args.in_flight,
                     "p50_ms": pct([t["total"] for t in times_b], 50), "p99_ms": pct([t["total"] for t in times_b], 99)},
-        "single": {"proofs_per_s": world * K / (single_ms / 1e3), "p50_ms": pct(lat, 50), "p99_ms": pct(lat, 99)},
+        "single": {"proofs_per_s": world * n_single / (single_ms / 1e3), "proofs": n_single,
+                   "p50_ms": pct(lat, 50), "p99_ms": pct(lat, 99)},
         "p99_ms": pct(lat, 99),
         "functional_single": {"p50_ms": pct(flat, 50), "p99_ms": pct(flat, 99), "proofs": len(flat),
                               "reference_published_ms": {"apple_m5_max_cpu_simd": [870.1, 332.8],
@@ -357,8 +405,14 @@ def main():
                               "note": "the reference's own published shape and preset (functional, 2^20x100); "
                                       "its numbers are from other hardware"},
         "stage_ms_p50": {k: pct([t[k] for t in times_b], 50) for k in times_b[0]},
-        "e2e": {"value": world * K / (e2e_ms / 1e3), "unit": "proofs/s", "h2d_bytes_per_step": 4 * n_words,
-                "d2h_bytes_per_step": int(proof_bytes)},
+        "e2e": {"value": world * NB / (e2e_ms / 1e3), "unit": "proofs/s",
+                "h2d_bytes_per_step": args.batch * (8 << args.log_n),
+                "d2h_bytes_per_step": int(args.batch * proof_bytes),
+                "input": "col0/col1 of each proof from pinned host memory (TRACE_FIRST_COLUMNS); the device "
+                         "derives the other columns; proof bytes back on the host"},
+        "e2e_full_trace": {"value": world * n_full / (e2e_full_ms / 1e3), "unit": "proofs/s", "proofs": n_full,
+                           "h2d_bytes_per_proof": 4 * n_words,
+                           "input": "every trace column from pinned host memory (host-link bound)"},
         "roofline": {"bound": "hbm", "kernel": "circle FFT pass: interpolate + blow-up extend (k_fft_low<1>, "
                      "k_fft_high, k_fft_low<0>)", "achieved": fft_gbs, "peak": hbm_peak, "unit": "GB/s",
                      "frac": fft_gbs / hbm_peak, "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)",
@@ -375,7 +429,7 @@ def main():
     ri = out["roofline_int32"]
     ri["frac"] = ri["achieved"] / ri["peak"]
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        n_cpu = min(3, K)
+        n_cpu = min(3, n_traces)
         total, same = 0.0, True
         for i in range(n_cpu):
             dt, ref = cpu_oracle_prove(args.log_n, args.width, args.preset, seeds[i])

@@ -61,8 +61,16 @@ typedef struct {
 /* Wide-Fibonacci proving request: the Statement (src/examples/wide_fibonacci/trace.zig:18-21)
  * plus the prepared trace. Exactly one trace source is used, in this order: trace_device,
  * trace_host, generated (trace_kind 0 = the reference's (1, row) seeds, 1 = seeded uniform
- * col0/col1 in [0, p-1)). has_channel_seed mixes channel_seed (mixU64) right after the
- * statement; 0 keeps the reference transcript. */
+ * col0/col1 in [0, p-1)). With trace_kind 2 (STWO_B200_TRACE_FIRST_COLUMNS) trace_device or
+ * trace_host holds only col0 then col1 (2 x 2^log_n_rows canonical words, bit-reversed circle
+ * order) and the device derives col_k = col_{k-2}^2 + col_{k-1}^2: the deferred quadratic-
+ * recurrence column source the Metal backend materialises on the device
+ * (src/examples/wide_fibonacci/trace.zig:221-265, materializeColumnSource at
+ * src/prover/pcs/scheme.zig:271-278). has_channel_seed mixes channel_seed (mixU64) right after
+ * the statement; 0 keeps the reference transcript. */
+#define STWO_B200_TRACE_REFERENCE 0
+#define STWO_B200_TRACE_SEEDED 1
+#define STWO_B200_TRACE_FIRST_COLUMNS 2
 typedef struct {
   uint32_t log_n_rows;
   uint32_t sequence_len;
@@ -301,7 +309,8 @@ int32_t stwo_b200_accumulate_quotients(stwo_b200_context* ctx, uint32_t log_size
 /* ---- Wide-Fibonacci AIR -------------------------------------------------------------------------- */
 
 /* Trace generation in bit-reversed circle order (fillQuadraticRecurrenceTrace hook,
- * src/examples/wide_fibonacci/trace.zig:63-74; generate_wide_fibonacci_trace, ffi.zig:263). */
+ * src/examples/wide_fibonacci/trace.zig:63-74; generate_wide_fibonacci_trace, ffi.zig:263).
+ * trace_kind 2 derives columns 2.. from the col0/col1 already in `out`. */
 int32_t stwo_b200_wide_fib_trace(stwo_b200_context* ctx, uint32_t log_n_rows, uint32_t sequence_len,
                                  uint32_t trace_kind, uint64_t seed, uint32_t* out, uint64_t stride, void* stream);
 /* Composition evaluation on CanonicCoset(log_n_rows+1): out (4 columns) = sum_k coeffs[k] *

@@ -338,7 +338,7 @@ int32_t stwo_b200_accumulate_quotients(stwo_b200_context* ctx, uint32_t log_size
 int32_t stwo_b200_wide_fib_trace(stwo_b200_context* ctx, uint32_t log_n_rows, uint32_t sequence_len,
                                  uint32_t trace_kind, uint64_t seed, uint32_t* out, uint64_t stride, void* stream) {
   CK_CTX(ctx);
-  if (log_n_rows == 0 || log_n_rows > 28 || sequence_len < 2 || !out || trace_kind > 1)
+  if (log_n_rows == 0 || log_n_rows > 28 || sequence_len < 2 || !out || trace_kind > 2)
     return set_error(STWO_B200_E_INVALID, "bad trace arguments");
   return cuda_status(sb::wide_fib_trace(log_n_rows, sequence_len, (int)trace_kind, seed, out, stride, st(stream)),
                      "wide_fib_trace");

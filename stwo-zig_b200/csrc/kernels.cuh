@@ -103,10 +103,28 @@ cudaError_t fold_line(const DeviceTables& t, uint32_t src_log, const uint32_t* s
 // FRI fold (circle -> line when `circle`, else line -> line with the source line
 // domain halfOdds(src_log)) fused with the commitment of the folded layer: when
 // `layers` is non-null the folded values are hashed as leaves (4 words each) and
-// the whole tree of 2^(src_log-1) leaves is built.
+// the whole tree of 2^(src_log-1) leaves is built. `alpha` is device memory (written
+// by fri_channel_step earlier on the same stream).
 cudaError_t fri_fold_commit(const DeviceTables& t, bool circle, uint32_t src_log, const uint32_t* src,
-                            uint64_t src_stride, QM31 alpha, uint32_t* dst, uint64_t dst_stride, uint8_t* layers,
-                            cudaStream_t stream);
+                            uint64_t src_stride, const QM31* alpha, uint32_t* dst, uint64_t dst_stride,
+                            uint8_t* layers, cudaStream_t stream);
+
+// Blake2s Fiat-Shamir channel state on the device for the FRI commit phase
+// (src/prover/fri.zig:314-592: per layer mixRoot, then drawSecureFelt for its alpha), so
+// the layers follow one another without a host round trip. The host uploads its channel
+// state first and replays the same steps from `roots` afterwards.
+constexpr uint32_t FRI_MAX_LAYERS = 32;
+struct FriChannelDev {
+  uint32_t digest[8];
+  uint32_t n_draws;
+  uint32_t status;  // nonzero: a draw was rejected FRI_DRAW_TRIES times in a row
+  uint32_t pad[2];
+  QM31 alpha[FRI_MAX_LAYERS];
+  uint32_t roots[FRI_MAX_LAYERS][8];
+};
+// mixRoot(root) (src/core/vcs_lifted/blake2_merkle.zig:236-247), then drawSecureFelt
+// (src/core/channel/blake2s.zig:52-112,260-279) into alpha[slot]; the root is kept in roots[slot].
+cudaError_t fri_channel_step(FriChannelDev* c, const uint8_t* root, uint32_t slot, cudaStream_t stream);
 
 // ---- Proof of work (src/core/channel/blake2s.zig:135-240) ------------------
 // Bounded rounds of the same search (the form the prover uses, so the grind

@@ -205,13 +205,14 @@ __device__ __forceinline__ void fri_ibfly(QM31& f0, QM31& f1, uint32_t it) {
 template <bool CIRCLE>
 __global__ void __launch_bounds__(LEAF_THREADS) k_fri_fold_commit(TwiddleView itv, uint32_t dst_log,
                                                                    const uint32_t* __restrict__ src, uint64_t ss,
-                                                                   QM31 alpha, uint32_t* dst, uint64_t ds,
+                                                                   const QM31* alpha_p, uint32_t* dst, uint64_t ds,
                                                                    uint8_t* layers, Seeds seeds, uint32_t levels,
                                                                    uint32_t one) {
   __shared__ uint32_t sm[LEAF_THREADS * 8];
   const uint64_t n = 1ull << dst_log;
   const uint64_t i = (uint64_t)blockIdx.x * LEAF_THREADS + threadIdx.x;
   if (i < n) {
+    const QM31 alpha = *alpha_p;
     uint2 w0 = *reinterpret_cast<const uint2*>(src + 2 * i);
     uint2 w1 = *reinterpret_cast<const uint2*>(src + ss + 2 * i);
     uint2 w2 = *reinterpret_cast<const uint2*>(src + 2 * ss + 2 * i);
@@ -234,6 +235,47 @@ __global__ void __launch_bounds__(LEAF_THREADS) k_fri_fold_commit(TwiddleView it
   __syncthreads();
   uint32_t count = n < LEAF_THREADS ? (uint32_t)n : LEAF_THREADS;
   fold_levels(sm, count, levels, layers, dst_log, dst_log, (uint64_t)blockIdx.x * LEAF_THREADS, seeds.node, one);
+}
+
+constexpr int FRI_DRAW_TRIES = 64;
+
+// One thread: the channel steps of one FRI layer (see fri_channel_step).
+__global__ void k_fri_channel(FriChannelDev* c, const uint8_t* root, uint32_t slot) {
+  uint32_t m[16], h[8];
+  const uint32_t* r = reinterpret_cast<const uint32_t*>(root);
+#pragma unroll
+  for (int k = 0; k < 8; ++k) {
+    m[k] = c->digest[k];
+    m[8 + k] = r[k];
+    c->roots[slot][k] = r[k];
+  }
+  b2s_init(h);
+  b2s_compress(h, m, 64, true);  // digest' = H(digest || root), one final 64-byte block
+  uint32_t n_draws = 0;
+  // drawSecureFelt: words of H(digest || LE32 n_draws || 0), all below 2p, else draw again.
+  for (int tries = 0; tries < FRI_DRAW_TRIES; ++tries) {
+    uint32_t w[8];
+#pragma unroll
+    for (int k = 0; k < 8; ++k) m[k] = h[k];
+    m[8] = n_draws;
+#pragma unroll
+    for (int k = 9; k < 16; ++k) m[k] = 0;
+    b2s_init(w);
+    b2s_compress(w, m, 37, true);
+    ++n_draws;
+    bool ok = true;
+#pragma unroll
+    for (int k = 0; k < 8; ++k) ok &= w[k] < 2 * P;
+    if (ok) {
+#pragma unroll
+      for (int k = 0; k < 8; ++k) c->digest[k] = h[k];
+      c->n_draws = n_draws;
+      c->alpha[slot] = qmake(mreduce64(w[0]), mreduce64(w[1]), mreduce64(w[2]), mreduce64(w[3]));
+      return;
+    }
+  }
+  c->status = 1;
+  c->alpha[slot] = qmake(0, 0, 0, 0);
 }
 
 __global__ void k_empty_root(uint8_t* layers, Seeds seeds) {
@@ -278,9 +320,15 @@ static cudaError_t merkle_finish(uint8_t* layers, uint32_t max_log, uint32_t chi
   return cudaSuccess;
 }
 
+cudaError_t fri_channel_step(FriChannelDev* c, const uint8_t* root, uint32_t slot, cudaStream_t stream) {
+  if (slot >= FRI_MAX_LAYERS) return cudaErrorInvalidValue;
+  k_fri_channel<<<1, 1, 0, stream>>>(c, root, slot); note_launch();
+  return cudaGetLastError();
+}
+
 cudaError_t fri_fold_commit(const DeviceTables& t, bool circle, uint32_t src_log, const uint32_t* src,
-                            uint64_t src_stride, QM31 alpha, uint32_t* dst, uint64_t dst_stride, uint8_t* layers,
-                            cudaStream_t stream) {
+                            uint64_t src_stride, const QM31* alpha, uint32_t* dst, uint64_t dst_stride,
+                            uint8_t* layers, cudaStream_t stream) {
   const Seeds& seeds = seeds_once();
   const uint32_t dst_log = src_log - 1;
   const uint64_t n = 1ull << dst_log;

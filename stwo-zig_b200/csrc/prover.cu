@@ -46,6 +46,7 @@ struct Buffers {
   const uint32_t** col_ptrs;
   QuotientBatchDev* batch;
   uint32_t* pow_result;
+  FriChannelDev* chan;
   uint8_t* scratch;  // gathers
   size_t scratch_bytes;
 };
@@ -75,6 +76,7 @@ Buffers carve(Arena& a, const Layout& l) {
   b.col_ptrs = a.take<const uint32_t*>(l.W + 8);
   b.batch = a.take<QuotientBatchDev>(1);
   b.pow_result = a.take<uint32_t>(4);
+  b.chan = a.take<FriChannelDev>(1);
   b.scratch = a.take<uint8_t>(GATHER_SCRATCH);
   b.scratch_bytes = GATHER_SCRATCH;
   return b;
@@ -257,6 +259,10 @@ int32_t WideFibProver::prove(const ProveRequest& req, std::string& out, StageTim
       n + 1 > ctx_->tables.tower_log + 1 || cfg.n_queries == 0 || cfg.n_queries > 4096 || cfg.pow_bits > 64)
     return fail(E_INVALID, "unsupported proof shape or configuration");
   if (n + B < cfg.log_last_layer_degree_bound + B + 1) return fail(E_INVALID, "last layer larger than the domain");
+  if (req.trace_kind < 0 || req.trace_kind > TRACE_FIRST_COLUMNS)
+    return fail(E_INVALID, "unknown trace kind");
+  if (req.trace_kind == TRACE_FIRST_COLUMNS && !req.trace_host && !req.trace_device)
+    return fail(E_INVALID, "the first two trace columns are missing");
   cudaSetDevice(ctx_->device);
   int32_t rc = ensure_workspace(n, W, B);
   if (rc != OK) return rc;
@@ -288,20 +294,26 @@ int32_t WideFibProver::prove(const ProveRequest& req, std::string& out, StageTim
   Channel ch;
   SB_CK(cudaEventRecord(ev_[0], s));
   // Trace in HBM.
+  // A full trace is used where it lies (device) or uploaded (host); with TRACE_FIRST_COLUMNS only
+  // col0/col1 are given and the device derives the other columns.
   const uint32_t* trace = b.trace;
+  const bool first_two = req.trace_kind == TRACE_FIRST_COLUMNS;
   if (req.trace_device) {
-    trace = req.trace_device;
+    if (first_two) SB_CK(cudaMemcpyAsync(b.trace, req.trace_device, 2 * l.N * 4, cudaMemcpyDeviceToDevice, s));
+    else trace = req.trace_device;
   } else if (req.trace_host) {
     // Host uploads go one at a time (FIFO on the context's lock, each held until its copy has
     // landed): concurrent copies of several proofs would share the host link and all finish
     // late, while one after the other each proof starts computing as soon as its own trace is in.
     std::lock_guard<std::mutex> g(ctx_->h2d_mu);
-    SB_CK(cudaMemcpyAsync(b.trace, req.trace_host, (size_t)W * l.N * 4, cudaMemcpyHostToDevice, s));
+    const size_t cols = first_two ? 2 : W;
+    SB_CK(cudaMemcpyAsync(b.trace, req.trace_host, cols * l.N * 4, cudaMemcpyHostToDevice, s));
     SB_CK(cudaEventRecord(ev_[1], s));
     SB_CK(cudaEventSynchronize(ev_[1]));
   }
   if (!req.trace_host) SB_CK(cudaEventRecord(ev_[1], s));
-  if (!req.trace_device && !req.trace_host) SB_CK(wide_fib_trace(n, W, req.trace_kind, req.trace_seed, b.trace, l.N, s));
+  if (first_two || (!req.trace_device && !req.trace_host))
+    SB_CK(wide_fib_trace(n, W, req.trace_kind, req.trace_seed, b.trace, l.N, s));
   SB_CK(cudaEventRecord(ev_[2], s));
 
   // PcsConfig.mixInto (src/core/pcs/mod.zig:32-52).
@@ -408,7 +420,7 @@ int32_t WideFibProver::prove(const ProveRequest& req, std::string& out, StageTim
   SB_CK(cudaEventRecord(ev_[7], fs));
 
   // FRI, last layer, proof of work and queries.
-  FriBuffers fbuf{b.quot, b.tree_q, b.line, b.line_tree, b.pow_result};
+  FriBuffers fbuf{b.quot, b.tree_q, b.line, b.line_tree, b.pow_result, b.chan};
   FriResult fr;
   {
     std::string ferr;

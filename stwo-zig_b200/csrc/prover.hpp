@@ -18,12 +18,16 @@ struct PcsConfig {
   uint32_t n_queries = 3;
 };
 
+constexpr int TRACE_FIRST_COLUMNS = 2;
+
 struct ProveRequest {
   uint32_t log_n_rows = 0, sequence_len = 0;
   PcsConfig config;
   const uint32_t* trace_host = nullptr;    // column-major, bit-reversed circle order
   const uint32_t* trace_device = nullptr;  // same layout, device memory
-  int trace_kind = 0;                      // when neither pointer is given: 0 (1,row), 1 seeded
+  // Without a trace pointer: 0 (1,row), 1 seeded. TRACE_FIRST_COLUMNS: the pointer holds only
+  // col0 and col1 and the device derives the rest of the trace.
+  int trace_kind = 0;
   uint64_t trace_seed = 0;
   bool has_channel_seed = false;
   uint64_t channel_seed = 0;

@@ -18,41 +18,55 @@ int32_t fri_pow_queries(const DeviceTables& T, int sm_count, Channel& ch, const 
                         uint32_t n_inner, uint32_t last_log, const FriBuffers& fb, uint8_t* pin, cudaStream_t s,
                         cudaStream_t fs, cudaEvent_t ev_fri, cudaEvent_t ev_pow, FriResult& out, std::string& err) {
   const uint64_t NL = 1ull << L;
-  // FRI: first layer, then inner layers each committed before its fold.
+  // FRI: first layer, then inner layers each committed before its fold. The channel steps
+  // between them (mix the layer's root, draw its alpha) run on the device, so the layers
+  // follow one another on `fs` without a host round trip.
   std::vector<std::array<uint8_t, 32>>& fri_roots = out.roots;
+  if (n_inner + 1 > FRI_MAX_LAYERS) { err = "too many FRI layers"; return E_INVALID; }
+  const size_t m_last = 1ull << last_log;
+  constexpr size_t LAST_OFF = (sizeof(FriChannelDev) + 255) & ~size_t(255);
   {
+    uint32_t* up = reinterpret_cast<uint32_t*>(pin);
+    std::memcpy(up, ch.digest, 32);
+    up[8] = ch.n_draws;
+    up[9] = 0;  // status
+    SB_CKE(cudaMemcpyAsync(fb.chan, up, 40, cudaMemcpyHostToDevice, fs));
     SB_CKE(merkle_commit(L, 4, fb.quot, NL, fb.tree_q, fs));
-    SB_CKE(cudaMemcpyAsync(pin, fb.tree_q + (2 * NL - 2) * 32, 32, cudaMemcpyDeviceToHost, fs));
-    SB_CKE(cudaStreamSynchronize(fs));
-    std::array<uint8_t, 32> r;
-    std::memcpy(r.data(), pin, 32);
-    fri_roots.push_back(r);
-    ch.mix_root(r.data());
-    QM31 alpha = ch.draw_secure_felt();
+    SB_CKE(fri_channel_step(fb.chan, fb.tree_q + (2 * NL - 2) * 32, 0, fs));
     // Each fold writes the next line layer and, unless it is the last layer,
     // commits it in the same launch sequence.
-    SB_CKE(fri_fold_commit(T, true, L, fb.quot, NL, alpha, fb.line[0], 1ull << (L - 1),
+    SB_CKE(fri_fold_commit(T, true, L, fb.quot, NL, &fb.chan->alpha[0], fb.line[0], 1ull << (L - 1),
                           n_inner > 0 ? fb.line_tree[0] : nullptr, fs));
     for (uint32_t k = 0; k < n_inner; ++k) {
       uint32_t lg = L - 1 - k;
       size_t sz = 1ull << lg;
-      SB_CKE(cudaMemcpyAsync(pin, fb.line_tree[k] + (2 * sz - 2) * 32, 32, cudaMemcpyDeviceToHost, fs));
-      SB_CKE(cudaStreamSynchronize(fs));
-      std::memcpy(r.data(), pin, 32);
+      SB_CKE(fri_channel_step(fb.chan, fb.line_tree[k] + (2 * sz - 2) * 32, k + 1, fs));
+      SB_CKE(fri_fold_commit(T, false, lg, fb.line[k], sz, &fb.chan->alpha[k + 1], fb.line[k + 1], sz / 2,
+                            k + 1 < n_inner ? fb.line_tree[k + 1] : nullptr, fs));
+    }
+    // One copy back: the device channel (roots, alphas) and the last layer's values.
+    SB_CKE(cudaMemcpyAsync(pin, fb.chan, sizeof(FriChannelDev), cudaMemcpyDeviceToHost, fs));
+    SB_CKE(cudaMemcpyAsync(pin + LAST_OFF, fb.line[n_inner], 4 * m_last * 4, cudaMemcpyDeviceToHost, fs));
+    SB_CKE(cudaStreamSynchronize(fs));
+    FriChannelDev dc;
+    std::memcpy(&dc, pin, sizeof(dc));
+    for (uint32_t k = 0; k <= n_inner; ++k) {
+      std::array<uint8_t, 32> r;
+      std::memcpy(r.data(), dc.roots[k], 32);
       fri_roots.push_back(r);
       ch.mix_root(r.data());
       QM31 a = ch.draw_secure_felt();
-      SB_CKE(fri_fold_commit(T, false, lg, fb.line[k], sz, a, fb.line[k + 1], sz / 2,
-                            k + 1 < n_inner ? fb.line_tree[k + 1] : nullptr, fs));
+      if (dc.status != 0 || !qeq(a, dc.alpha[k])) {
+        err = "device FRI channel diverged from the host transcript";
+        return E_CUDA;
+      }
     }
   }
   // Last layer: line IFFT of 2^last_log values (src/backend/line_evaluation.zig:97-145).
   std::vector<QM31>& last_coeffs = out.last_coeffs;
   {
-    size_t m = 1ull << last_log;
-    SB_CKE(cudaMemcpyAsync(pin, fb.line[n_inner], 4 * m * 4, cudaMemcpyDeviceToHost, fs));
-    SB_CKE(cudaStreamSynchronize(fs));
-    const uint32_t* w = reinterpret_cast<const uint32_t*>(pin);
+    const size_t m = m_last;
+    const uint32_t* w = reinterpret_cast<const uint32_t*>(pin + LAST_OFF);
     std::vector<QM31> v(m);
     for (size_t i = 0; i < m; ++i) v[i] = qmake(w[i], w[m + i], w[2 * m + i], w[3 * m + i]);
     auto brev = [&](std::vector<QM31>& x) {

@@ -249,6 +249,7 @@ struct FriBuffers {
   std::vector<uint32_t*> line;      // line layers 0..n_inner (the last one is the last layer)
   std::vector<uint8_t*> line_tree;  // trees of line layers 0..n_inner-1
   uint32_t* pow_result;             // 2 words of device scratch
+  FriChannelDev* chan;              // device channel of the FRI commit phase
 };
 struct FriResult {
   std::vector<std::array<uint8_t, 32>> roots;  // first layer, then inner layers
@@ -256,7 +257,9 @@ struct FriResult {
   uint64_t nonce = 0;
   std::vector<uint64_t> queries;  // sorted, unique
 };
-// Runs on `fs` (FRI, latency-bound) and `s` (proof of work); `pin` is pinned host staging.
+// Runs on `fs` (FRI, latency-bound) and `s` (proof of work); `pin` is pinned host staging
+// (at least 64 KB). The FRI layers draw their alphas on the device (FriChannelDev); the
+// host replays the same channel steps from the returned roots and checks every alpha.
 // ev_fri and ev_pow (nullable) are recorded after the last layer and after the grind.
 int32_t fri_pow_queries(const DeviceTables& T, int sm_count, Channel& ch, const PcsConfig& cfg, uint32_t L,
                         uint32_t n_inner, uint32_t last_log, const FriBuffers& fb, uint8_t* pin, cudaStream_t s,

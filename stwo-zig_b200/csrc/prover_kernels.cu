@@ -35,16 +35,23 @@ __device__ __forceinline__ uint32_t seeded_value(uint64_t seed, uint32_t column,
   return 0;  // probability 2^-1984: unreachable in practice
 }
 
+// Wide-Fibonacci trace in bit-reversed circle order: col0/col1 are the reference's (1, row) for
+// kind 0, seeded uniform for kind 1, or already in `out` for kind 2; col_k = col_{k-2}^2 + col_{k-1}^2.
 __global__ void k_wide_fib_trace(uint32_t log_n, uint32_t W, int kind, uint64_t seed, uint32_t* out, uint64_t stride) {
   const uint32_t n = 1u << log_n;
   for (uint32_t s = blockIdx.x * blockDim.x + threadIdx.x; s < n; s += gridDim.x * blockDim.x) {
     uint32_t ci = bitrev(s, log_n);
     uint32_t row = ci < n / 2 ? ci * 2 : (n - 1 - ci) * 2 + 1;
     uint32_t a, b;
-    if (kind == 0) { a = 1; b = row % P; }
-    else { a = seeded_value(seed, 0, row); b = seeded_value(seed, 1, row); }
-    out[s] = a;
-    out[stride + s] = b;
+    if (kind == 2) {  // the first two columns are given: derive the rest
+      a = out[s];
+      b = out[stride + s];
+    } else {
+      if (kind == 0) { a = 1; b = row % P; }
+      else { a = seeded_value(seed, 0, row); b = seeded_value(seed, 1, row); }
+      out[s] = a;
+      out[stride + s] = b;
+    }
     for (uint32_t k = 2; k < W; ++k) {
       uint32_t c = madd(mmul(a, a), mmul(b, b));
       out[k * stride + s] = c;

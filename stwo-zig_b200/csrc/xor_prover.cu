@@ -135,6 +135,7 @@ struct XorBufs {
   const uint32_t** col_ptrs;
   QuotientBatchDev* batch;
   uint32_t *pow_result, *zero_flag;
+  FriChannelDev* chan;
 };
 XorBufs xor_carve(Arena& a, const XorShape& sh) {
   const uint64_t N = 1ull << sh.L, NL = N << sh.B, NC = N << 1;
@@ -163,6 +164,7 @@ XorBufs xor_carve(Arena& a, const XorShape& sh) {
   b.claimed = a.take<QM31>(2);
   b.logup_scratch = a.take<QM31>(logup_scratch_count(sh.L));
   b.pow_result = a.take<uint32_t>(4);
+  b.chan = a.take<FriChannelDev>(1);
   b.zero_flag = a.take<uint32_t>(4);
   b.scratch = a.take<uint8_t>(GATHER_SCRATCH);
   return b;
@@ -421,7 +423,7 @@ int32_t LogupXorProver::prove(const XorRequest& req, std::string& out) {
   }
 
   // Tail: FRI, proof of work, queries, decommitment.
-  FriBuffers fbuf{b.quot, b.tree_q, b.line, b.line_tree, b.pow_result};
+  FriBuffers fbuf{b.quot, b.tree_q, b.line, b.line_tree, b.pow_result, b.chan};
   FriResult fr;
   {
     std::string ferr;

@@ -215,6 +215,7 @@ def verify_logup_xor(proof: bytes, log_n: int, log_table: int = 16, channel_seed
 
 TRACE_REFERENCE = 0   # (1, row) seeds of the reference's trace generator
 TRACE_SEEDED = 1      # seeded uniform col0/col1 in [0, p-1)
+TRACE_FIRST_COLUMNS = 2  # the trace argument holds only col0 and col1; the device derives the rest
 
 
 def _qm(v) -> QM31C:

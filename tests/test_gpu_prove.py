@@ -61,6 +61,47 @@ def test_host_and_device_traces(ctx):
     assert ctx.prove_wide_fibonacci(sb.Statement(10, 20), g, trace=dtrace) == ref
 
 
+def _recurrence_trace(first_two, W):
+    P = 2**31 - 1
+    full = np.empty((W, first_two.shape[1]), dtype=np.uint32)
+    full[:2] = first_two
+    for k in range(2, W):
+        a, b = full[k - 2].astype(np.uint64), full[k - 1].astype(np.uint64)
+        full[k] = ((a * a + b * b) % P).astype(np.uint32)
+    return full
+
+
+def test_first_two_columns_source(ctx):
+    """TRACE_FIRST_COLUMNS: only col0/col1 are given (host or device); the device derives the rest."""
+    import stwo_b200 as sb
+    import torch
+    o, g = cfg_pair("functional")
+    rng = np.random.default_rng(8)
+    two = rng.integers(0, 2**31 - 1, size=(2, 1 << 11), dtype=np.uint32)  # arbitrary canonical values
+    full = _recurrence_trace(two, 24)
+    ref = oracle.prove_wide_fib(11, 24, o, trace=full)
+    st = sb.Statement(11, 24)
+    assert ctx.prove_wide_fibonacci(st, g, trace=two, trace_kind=sb.TRACE_FIRST_COLUMNS) == ref
+    dtwo = torch.from_numpy(two.view(np.int32)).cuda()
+    assert ctx.prove_wide_fibonacci(st, g, trace=dtwo, trace_kind=sb.TRACE_FIRST_COLUMNS) == ref
+    # In place: the kernel fills columns 2.. from the two already in the buffer.
+    out = torch.zeros(24 << 11, dtype=torch.int32, device="cuda")
+    out[: 2 << 11] = dtwo.reshape(-1)
+    ctx.wide_fib_trace(out, 11, 24, sb.TRACE_FIRST_COLUMNS)
+    assert np.array_equal(out.cpu().numpy().view(np.uint32).reshape(24, -1), full)
+    # The seeded source and its own first two columns prove the same statement identically.
+    o2, g2 = cfg_pair("secure")
+    seeded = oracle.gen_trace(12, 100, trace_kind=1, seed=41)
+    want = ctx.prove_wide_fibonacci(sb.Statement(12, 100), g2, trace_kind=sb.TRACE_SEEDED, trace_seed=41)
+    got = ctx.prove_wide_fibonacci(sb.Statement(12, 100), g2, trace=np.ascontiguousarray(seeded[:2]),
+                                   trace_kind=sb.TRACE_FIRST_COLUMNS)
+    assert got == want
+    for bad in (dict(trace_kind=sb.TRACE_FIRST_COLUMNS), dict(trace_kind=3, trace_seed=1)):
+        with pytest.raises(sb.StwoError) as e:
+            ctx.prove_wide_fibonacci(st, g, **bad)
+        assert e.value.status == sb.E_INVALID
+
+
 def test_channel_seed_and_blowup(ctx):
     import stwo_b200 as sb
     o, g = cfg_pair("functional", log_blowup_factor=2, n_queries=5, log_last_layer_degree_bound=1)
