@@ -257,9 +257,10 @@ def main():
             out.append(r)
         return out
 
-    # ---- warmup (both paths): at least one proof per in-flight slot, so every prover slot
-    # (stream, pinned staging, workspace) exists before the timed region
-    WB = max(W, args.in_flight)
+    # ---- warmup (both paths): W steps of the batched workload (W * batch proofs, and at least one
+    # per in-flight slot, so every prover slot's stream, pinned staging and workspace exists before
+    # the timed region), then W single proofs
+    WB = max(W * args.batch, args.in_flight)
     ctx.prove_wide_fibonacci_batch(requests(range(WB), salt=1), max_in_flight=args.in_flight)
     for r in requests(range(W), salt=2):
         ctx.prove_wide_fibonacci(**r)

@@ -12,6 +12,7 @@ values are < 2^31); torch is used for device memory and streams only.
 from __future__ import annotations
 
 import ctypes
+import threading
 import os
 from dataclasses import dataclass, field
 
@@ -246,6 +247,20 @@ class Context:
         self._h = h
         self.device = device
         self._cap = 1 << 21
+        self._buffers: list = []  # host output buffers of batch calls, reused across calls
+        self._buffers_lock = threading.Lock()
+
+    def _take_buffer(self, nbytes: int):
+        import numpy as np
+        with self._buffers_lock:
+            for i, b in enumerate(self._buffers):
+                if b.size >= nbytes:
+                    return self._buffers.pop(i)
+        return np.empty(nbytes, dtype=np.uint8)
+
+    def _give_buffer(self, buf) -> None:
+        with self._buffers_lock:
+            self._buffers.append(buf)
 
     def close(self) -> None:
         if self._h:
@@ -332,16 +347,22 @@ class Context:
             arr[i] = req
             keeps.append(keep)
         cap = proof_cap
-        bufs = [ctypes.create_string_buffer(cap) for _ in range(n)]
-        outs = (_vp * n)(*[ctypes.cast(b, _vp) for b in bufs])
-        caps = (ctypes.c_size_t * n)(*([cap] * n))
-        lens = (ctypes.c_size_t * n)()
-        statuses = (_i32 * n)()
-        times = (StageTimesC * n)()
-        _check(_lib.stwo_b200_prove_wide_fibonacci_batch(self._h, arr, n, outs, caps, lens, statuses, max_in_flight,
-                                                         times))
+        # Proof output space: one host buffer of n * cap bytes, taken from a pool kept on the
+        # context and reused across calls (neither zero-filled nor page-faulted again per call).
+        buf = self._take_buffer(n * cap)
+        try:
+            base = buf.ctypes.data
+            outs = (_vp * n)(*[base + i * cap for i in range(n)])
+            caps = (ctypes.c_size_t * n)(*([cap] * n))
+            lens = (ctypes.c_size_t * n)()
+            statuses = (_i32 * n)()
+            times = (StageTimesC * n)()
+            _check(_lib.stwo_b200_prove_wide_fibonacci_batch(self._h, arr, n, outs, caps, lens, statuses,
+                                                             max_in_flight, times))
+            proofs = [ctypes.string_at(base + i * cap, lens[i]) for i in range(n)]
+        finally:
+            self._give_buffer(buf)
         del keeps
-        proofs = [ctypes.string_at(bufs[i], lens[i]) for i in range(n)]
         if with_times:
             return proofs, [{k: getattr(times[i], k) for k, _ in StageTimesC._fields_} for i in range(n)]
         return proofs
