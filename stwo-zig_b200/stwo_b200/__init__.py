@@ -262,6 +262,26 @@ class Context:
         with self._buffers_lock:
             self._buffers.append(buf)
 
+    def _with_output(self, call) -> bytes:
+        """Runs call(out_ptr, cap, n) with a pooled host buffer of self._cap bytes and returns the
+        n bytes written; on E_BUFFER_TOO_SMALL the capacity grows to what was reported and the call
+        is repeated once."""
+        n = ctypes.c_size_t(0)
+        for _ in range(2):
+            cap = self._cap
+            buf = self._take_buffer(cap)
+            try:
+                rc = call(buf.ctypes.data, cap, n)
+                if rc == OK:
+                    return ctypes.string_at(buf.ctypes.data, n.value)
+            finally:
+                self._give_buffer(buf)
+            if rc != E_BUFFER_TOO_SMALL:
+                break
+            self._cap = max(2 * cap, n.value)
+        _check(rc)
+        raise StwoError(rc, "output buffer too small")
+
     def close(self) -> None:
         if self._h:
             _lib.stwo_b200_context_destroy(self._h)
@@ -302,20 +322,10 @@ class Context:
                              with_times: bool = False):
         """Proves the wide-Fibonacci AIR; returns the JSON wire proof bytes (and stage times)."""
         req, keep = self._request(statement, config, trace, trace_kind, trace_seed, channel_seed)
-        cap = self._cap
-        buf = ctypes.create_string_buffer(cap)
-        n = ctypes.c_size_t(0)
         times = StageTimesC()
-        rc = _lib.stwo_b200_prove_wide_fibonacci(self._h, ctypes.byref(req), buf, cap, ctypes.byref(n),
-                                                 ctypes.byref(times))
-        if rc == E_BUFFER_TOO_SMALL:
-            self._cap = cap = max(2 * cap, n.value)
-            buf = ctypes.create_string_buffer(cap)
-            rc = _lib.stwo_b200_prove_wide_fibonacci(self._h, ctypes.byref(req), buf, cap, ctypes.byref(n),
-                                                     ctypes.byref(times))
-        _check(rc)
+        proof = self._with_output(lambda out, cap, n: _lib.stwo_b200_prove_wide_fibonacci(
+            self._h, ctypes.byref(req), out, cap, ctypes.byref(n), ctypes.byref(times)))
         del keep
-        proof = ctypes.string_at(buf, n.value)
         if with_times:
             return proof, {name: getattr(times, name) for name, _ in StageTimesC._fields_}
         return proof
@@ -324,16 +334,8 @@ class Context:
                         channel_seed: int | None = None) -> bytes:
         """Proves the LogUp XOR-lookup AIR (2^log_n seeded lookups into the 2^log_table XOR table)."""
         req = XorRequestC(log_n, log_table, config._c(), seed, int(channel_seed is not None), 0, channel_seed or 0)
-        n = ctypes.c_size_t(0)
-        cap = self._cap
-        buf = ctypes.create_string_buffer(cap)
-        rc = _lib.stwo_b200_prove_logup_xor(self._h, ctypes.byref(req), buf, cap, ctypes.byref(n))
-        if rc == E_BUFFER_TOO_SMALL:
-            self._cap = cap = max(2 * cap, n.value)
-            buf = ctypes.create_string_buffer(cap)
-            rc = _lib.stwo_b200_prove_logup_xor(self._h, ctypes.byref(req), buf, cap, ctypes.byref(n))
-        _check(rc)
-        return ctypes.string_at(buf, n.value)
+        return self._with_output(lambda out, cap, n: _lib.stwo_b200_prove_logup_xor(
+            self._h, ctypes.byref(req), out, cap, ctypes.byref(n)))
 
     def prove_wide_fibonacci_batch(self, requests: list[dict], max_in_flight: int = 4, with_times: bool = False,
                                    proof_cap: int = 1 << 21):
@@ -503,19 +505,15 @@ class Server:
         return ticket.value
 
     def wait(self, ticket: int) -> tuple[bytes, dict]:
-        cap = 1 << 21
-        n = ctypes.c_size_t(0)
         st = RequestStatsC()
-        buf = ctypes.create_string_buffer(cap)
-        rc = _lib.stwo_b200_server_wait(self._h, ticket, buf, cap, ctypes.byref(n), ctypes.byref(st))
-        if rc == E_BUFFER_TOO_SMALL:
-            buf = ctypes.create_string_buffer(n.value)
-            rc = _lib.stwo_b200_server_wait(self._h, ticket, buf, n.value, ctypes.byref(n), ctypes.byref(st))
-        self._keep.pop(ticket, None)
-        _check(rc)
+        try:
+            proof = self._ctx._with_output(lambda out, cap, n: _lib.stwo_b200_server_wait(
+                self._h, ticket, out, cap, ctypes.byref(n), ctypes.byref(st)))
+        finally:
+            self._keep.pop(ticket, None)
         stats = {name: getattr(st, name) for name, _ in RequestStatsC._fields_ if name != "stages"}
         stats["stages"] = {name: getattr(st.stages, name) for name, _ in StageTimesC._fields_}
-        return ctypes.string_at(buf, n.value), stats
+        return proof, stats
 
     def warmup(self, max_log_n_rows: int = 0, max_sequence_len: int = 100, log_blowup: int = 1,
                max_xor_log_n: int = 0) -> None:
