@@ -204,19 +204,21 @@ def pow_ok(digest: bytes, bits: int, nonce: int) -> bool:
     return tz >= bits
 
 
-def merkle_verify(root, max_log, positions, columns, witness):
-    """Lifted Merkle verification for equal-size columns (src/core/vcs_lifted/verifier.zig:94-250).
-    positions: queried leaf indices (any order, duplicates allowed); columns[c][j] value of column c
-    at positions[j]."""
+def merkle_verify(root, max_log, positions, columns, witness, col_logs=None):
+    """Lifted Merkle verification (src/core/vcs_lifted/verifier.zig:94-250). positions: queried leaf
+    indices (any order, duplicates allowed); columns[c][j] value of column c at positions[j] (for a
+    column smaller than the tree, its value at the lifted index). A leaf hashes the row of values in
+    column order stably sorted by log size (col_logs; equal sizes when omitted)."""
     if not columns:
         if witness:
             raise VerificationError("witness for an empty tree")
         return
+    corder = sorted(range(len(columns)), key=lambda c: ((col_logs[c] if col_logs else 0), c))
     order = sorted(range(len(positions)), key=lambda j: (positions[j], j))
     leaves = {}
     for j in order:
         pos = positions[j]
-        row = b"".join(struct.pack("<I", col[j]) for col in columns)
+        row = b"".join(struct.pack("<I", columns[c][j]) for c in corder)
         h = b2s(LEAF + row)
         if pos in leaves and leaves[pos] != h:
             raise VerificationError("duplicate query mismatch")
@@ -318,11 +320,14 @@ def verify_wide_fib(proof_bytes: bytes, log_n_rows: int, sequence_len: int, chan
     return _verify_pcs_tail(pr, ch, roots, [0, W, 8], [(oods, entries)], n + B, B, pow_bits, log_last, n_queries)
 
 
-def _verify_pcs_tail(pr, ch, roots, tree_cols, batches, L, B, pow_bits, log_last, n_queries):
+def _verify_pcs_tail(pr, ch, roots, tree_cols, batches, L, B, pow_bits, log_last, n_queries, tree_logs=None):
     """FRI commitments and alphas, last layer, proof of work, queries, the trees' Merkle
     decommitments and the FRI decommitment, for a proof whose trees hold tree_cols[t] columns on
-    the lifting domain of log size L. batches: [(point, [(flat column, value, random power)])]
-    (src/core/pcs/quotients/fri_answers.zig, src/core/fri.zig)."""
+    the lifting domain of log size L. tree_logs[t] (optional): the committed log sizes of tree t's
+    columns; a tree's depth is its largest column, and the preprocessed tree (tree 0), when smaller
+    than L, is queried at the positions mapped down (src/core/pcs/utils.zig:292-314). batches:
+    [(point, [(flat column, value, random power)])] (src/core/pcs/quotients/fri_answers.zig,
+    src/core/fri.zig)."""
     fri = pr["fri_proof"]
     ch.mix_root(bytes(fri["first_layer"]["commitment"]))
     alphas = [ch.draw_secure_felt()]
@@ -362,7 +367,15 @@ def _verify_pcs_tail(pr, ch, roots, tree_cols, batches, L, B, pow_bits, log_last
             if dec[t_idx]["hash_witness"]:
                 raise VerificationError("preprocessed tree shape")
             continue
-        merkle_verify(roots[t_idx], L, queries, tcols, [bytes(h) for h in dec[t_idx]["hash_witness"]])
+        logs = tree_logs[t_idx] if tree_logs else None
+        depth = max(logs) if logs else L
+        positions = queries
+        if depth != L:
+            if t_idx != 0 or depth > L:
+                raise VerificationError("tree size")
+            sh = L - depth + 1
+            positions = [((p >> sh) << 1) + (p & 1) for p in queries]
+        merkle_verify(roots[t_idx], depth, positions, tcols, [bytes(h) for h in dec[t_idx]["hash_witness"]], logs)
         cols.extend(tcols)
 
     # quotient answers at the queries (src/core/pcs/quotients/fri_answers.zig, row_evaluation.zig)
@@ -469,9 +482,11 @@ def _verify_pcs_tail(pr, ch, roots, tree_cols, batches, L, B, pow_bits, log_last
 
 def verify_logup_xor(proof_bytes: bytes, log_n: int, log_table: int = 16, channel_seed: int | None = None):
     """Verifier of the LogUp XOR-lookup AIR proofs of the B200 prover (the AIR is described in
-    stwo-zig_b200/csrc/xor_prover.cu; it has no reference counterpart). Checks the transcript, the
-    cancellation of the two LogUp claimed sums, both LogUp transition constraints and the
-    composition at the OODS point, and the PCS / FRI decommitments."""
+    stwo-zig_b200/csrc/xor_prover.cu; it has no reference counterpart): a main component of 2^log_n
+    rows and a table component of 2^log_table rows under the reference's lifted PCS. Checks the
+    transcript, the cancellation of the two LogUp claimed sums, both LogUp transition constraints
+    and the composition at the OODS point (each component at the point doubled to its size, with
+    its own vanishing polynomial), and the PCS / FRI decommitments with lifted trees."""
     pr = json.loads(proof_bytes)
     cfg = pr["config"]
     fc = cfg["fri_config"]
@@ -481,8 +496,8 @@ def verify_logup_xor(proof_bytes: bytes, log_n: int, log_table: int = 16, channe
         raise VerificationError("unsupported config")
     if pr["statement"] != {"log_n": log_n, "log_table": log_table}:
         raise VerificationError("statement mismatch")
-    L = max(log_n, log_table)
-    N = 1 << L
+    n, t = log_n, log_table
+    L = max(n, t)
     roots = [bytes(c) for c in pr["commitments"]]
     if len(roots) != 4:
         raise VerificationError("expected 4 commitments")
@@ -505,20 +520,25 @@ def verify_logup_xor(proof_bytes: bytes, log_n: int, log_table: int = 16, channe
         raise VerificationError("LogUp claimed sums do not cancel")
     random_coeff = ch.draw_secure_felt()
     ch.mix_root(roots[3])
-    t = ch.draw_secure_felt()
-    t2 = qmul(t, t)
+    t_ = ch.draw_secure_felt()
+    t2 = qmul(t_, t_)
     inv = qinv(qadd(t2, q(1)))
-    oods = (qmul(qsub(q(1), t2), inv), qmul(qadd(t, t), inv))
+    oods = (qmul(qsub(q(1), t2), inv), qmul(qadd(t_, t_), inv))
     g = index_point(subgroup_gen(L))
-    prev = qpadd(oods, (q(g[0]), q(-g[1])))
+    prev = qpadd(oods, (q(g[0]), q(-g[1])))  # the previous row at the maximal size
+
+    def doubled(pt, k):  # a point of the 2^L-row domain seen by a column of 2^k rows
+        for _ in range(L - k):
+            pt = qpadd(pt, pt)
+        return pt
 
     sv = pr["sampled_values"]
-    if [len(x) for x in sv] != [4, 4, 8, 8] or any(len(c) != 1 for t_ in (0, 1, 3) for c in sv[t_]) or \
+    if [len(x) for x in sv] != [3, 4, 8, 8] or any(len(c) != 1 for tr in (0, 1, 3) for c in sv[tr]) or \
             any(len(c) != 2 for c in sv[2]):
         raise VerificationError("sampled values shape")
-    pre = [qfrom(c[0]) for c in sv[0]]
-    main = [qfrom(c[0]) for c in sv[1]]
-    inter_prev = [qfrom(c[0]) for c in sv[2]]
+    pre = [qfrom(c[0]) for c in sv[0]]           # ta, tb, tc (table size)
+    main = [qfrom(c[0]) for c in sv[1]]          # a, b, c (main size), m (table size)
+    inter_prev = [qfrom(c[0]) for c in sv[2]]    # S_M (main size), S_T (table size)
     inter_cur = [qfrom(c[1]) for c in sv[2]]
     comp = [qfrom(c[0]) for c in sv[3]]
     basis = [q(1), q(0, 1), q(0, 0, 1), q(0, 0, 0, 1)]
@@ -533,15 +553,15 @@ def verify_logup_xor(proof_bytes: bytes, log_n: int, log_table: int = 16, channe
     for _ in range(L + 1 - 2):
         pt = qpadd(pt, pt)
     comp_eval = qadd(left, qmul(pt[0], right))
-    inv_n = pow(N, P - 2, P)
     sm, sm_prev = secure(inter_cur[:4]), secure(inter_prev[:4])
     st, st_prev = secure(inter_cur[4:]), secure(inter_prev[4:])
     d_main = qsub(qadd(qadd(main[0], qmul(alpha, main[1])), qmul(alpha2, main[2])), z)
     d_table = qsub(qadd(qadd(pre[0], qmul(alpha, pre[1])), qmul(alpha2, pre[2])), z)
-    c_main = qsub(qmul(qadd(qsub(sm, sm_prev), qmulm(claimed[0], inv_n)), d_main), pre[3])
-    c_table = qadd(qmul(qadd(qsub(st, st_prev), qmulm(claimed[1], inv_n)), d_table), main[3])
-    dinv = qinv(coset_vanishing_q(L, subgroup_gen(L + 1), subgroup_gen(L), oods))
-    if qmul(qadd(qmul(random_coeff, c_main), c_table), dinv) != comp_eval:
+    c_main = qsub(qmul(qadd(qsub(sm, sm_prev), qmulm(claimed[0], pow(1 << n, P - 2, P))), d_main), q(1))
+    c_table = qadd(qmul(qadd(qsub(st, st_prev), qmulm(claimed[1], pow(1 << t, P - 2, P))), d_table), main[3])
+    z_main = coset_vanishing_q(n, subgroup_gen(n + 1), subgroup_gen(n), doubled(oods, n))
+    z_table = coset_vanishing_q(t, subgroup_gen(t + 1), subgroup_gen(t), doubled(oods, t))
+    if qadd(qmul(qmul(random_coeff, c_main), qinv(z_main)), qmul(c_table, qinv(z_table))) != comp_eval:
         raise VerificationError("OODS mismatch")
 
     flat = pre + main
@@ -550,25 +570,39 @@ def verify_logup_xor(proof_bytes: bytes, log_n: int, log_table: int = 16, channe
     flat += comp
     ch.mix_felts(flat)
     quot_coeff = ch.draw_secure_felt()
-    # samples with random powers over (tree, column, sample), a two-sample column's periodicity
-    # sample (at P, the lifting generator doubled to the column's log size being the identity)
-    # first; batches by point in order of first appearance: P, then P - g
+    # samples with random powers over (tree, column, sample); a two-sample column's periodicity
+    # sample first, at its current point plus the lifting generator (order 2^(L+B)) doubled to the
+    # column's log size (the identity for a full-size column); batches by point in order of first
+    # appearance (src/core/pcs/quotients/samples.zig:163-300)
     rp = [q(1)]
 
     def nxt():
         r = rp[0]
         rp[0] = qmul(r, quot_coeff)
         return r
-    b_p, b_prev = [], []
+    batches = []
+
+    def add(point, entry):
+        for bp, entries in batches:
+            if bp == point:
+                entries.append(entry)
+                return
+        batches.append((point, [entry]))
+    logs = [[t + B] * 3, [n + B] * 3 + [t + B], [n + B] * 4 + [t + B] * 4, [L + B] * 8]
+    for c in range(3):
+        add(oods, (c, pre[c], nxt()))
     for c in range(4):
-        b_p.append((c, pre[c], nxt()))
-    for c in range(4):
-        b_p.append((4 + c, main[c], nxt()))
+        add(oods, (3 + c, main[c], nxt()))
     for c in range(8):
-        b_p.append((8 + c, inter_cur[c], nxt()))
-        b_prev.append((8 + c, inter_prev[c], nxt()))
-        b_p.append((8 + c, inter_cur[c], nxt()))
+        k = n if c < 4 else t
+        per = oods
+        if k < L:
+            h = index_point(1 << (31 - L + k))
+            per = qpadd(oods, (q(h[0]), q(h[1])))
+        add(per, (7 + c, inter_cur[c], nxt()))
+        add(prev, (7 + c, inter_prev[c], nxt()))
+        add(oods, (7 + c, inter_cur[c], nxt()))
     for c in range(8):
-        b_p.append((16 + c, comp[c], nxt()))
-    return _verify_pcs_tail(pr, ch, roots, [4, 4, 8, 8], [(oods, b_p), (prev, b_prev)], L + B, B, pow_bits,
-                            log_last, n_queries)
+        add(oods, (15 + c, comp[c], nxt()))
+    return _verify_pcs_tail(pr, ch, roots, [3, 4, 8, 8], batches, L + B, B, pow_bits, log_last, n_queries,
+                            tree_logs=logs)

@@ -159,7 +159,10 @@ void DecommitPlan::add_tree(const uint8_t* layers, uint32_t max_log, const std::
     for (uint64_t q : queries) words_.push_back({c, q});
   tp.hash0 = hashes_.size();
   if (!cols.empty()) {
-    for (uint64_t nd : witness_nodes(max_log, queries)) hashes_.push_back({layers, nd});
+    std::vector<uint64_t> uniq(queries);
+    std::sort(uniq.begin(), uniq.end());
+    uniq.erase(std::unique(uniq.begin(), uniq.end()), uniq.end());
+    for (uint64_t nd : witness_nodes(max_log, uniq)) hashes_.push_back({layers, nd});
   }
   tp.n_hash = hashes_.size() - tp.hash0;
   trees_.push_back(tp);

@@ -272,8 +272,10 @@ int32_t fri_pow_queries(const DeviceTables& T, int sm_count, Channel& ch, const 
 // ---------------------------------------------------------------------------
 class DecommitPlan {
  public:
-  // A trace tree of `cols` columns (each 2^max_log words) at the queried leaf positions;
-  // a tree without columns contributes nothing.
+  // A trace tree of `cols` columns (each 2^max_log words): their values at `queries` (one
+  // position per query, in query order; repeats allowed, as when a smaller preprocessed tree
+  // takes the lifting domain's positions mapped down) and the witness of the sorted unique
+  // positions. A tree without columns contributes nothing.
   void add_tree(const uint8_t* layers, uint32_t max_log, const std::vector<const uint32_t*>& cols,
                 const std::vector<uint64_t>& queries);
   void add_fri(const FriBuffers& fb, uint32_t L, uint32_t n_inner, const std::vector<uint64_t>& queries);

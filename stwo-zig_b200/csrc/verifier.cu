@@ -158,16 +158,23 @@ Hash node_hash(const Hash& l, const Hash& r) {
 
 // Equal-size columns at `positions` (any order, duplicates allowed): cols[c][j] is column c at
 // positions[j] (src/core/vcs_lifted/verifier.zig:94-250).
+// A leaf hashes its row of values in column order stably sorted by log size (`col_logs`; equal
+// sizes when empty), a smaller column's value being the one at the lifted index.
 void merkle_verify(const Hash& root, uint32_t max_log, const std::vector<uint64_t>& positions,
-                   const std::vector<std::vector<uint32_t>>& cols, const std::vector<Hash>& witness) {
+                   const std::vector<std::vector<uint32_t>>& cols, const std::vector<Hash>& witness,
+                   const std::vector<uint32_t>& col_logs = {}) {
   if (cols.empty()) {
     if (!witness.empty()) throw Fail("witness for an empty tree");
     return;
   }
+  std::vector<size_t> corder(cols.size());
+  for (size_t c = 0; c < cols.size(); ++c) corder[c] = c;
+  if (!col_logs.empty())
+    std::stable_sort(corder.begin(), corder.end(), [&](size_t x, size_t y) { return col_logs[x] < col_logs[y]; });
   std::map<uint64_t, Hash> leaves;
   for (size_t j = 0; j < positions.size(); ++j) {
     std::vector<uint32_t> row(cols.size());
-    for (size_t c = 0; c < cols.size(); ++c) row[c] = cols[c][j];
+    for (size_t c = 0; c < cols.size(); ++c) row[c] = cols[corder[c]][j];
     Hash h = leaf_hash(row);
     auto it = leaves.find(positions[j]);
     if (it != leaves.end() && it->second != h) throw Fail("duplicate query mismatch");
@@ -268,8 +275,12 @@ struct Batch {
 
 // FRI commitments and alphas, last layer, PoW, queries, tree decommitments and quotient answers,
 // FRI decommitment (the verifier's PCS tail).
+// tree_logs (optional): the committed log sizes of each tree's columns. A tree's depth is its largest
+// column; the preprocessed tree (tree 0), when smaller than the lifting domain, is queried at the
+// positions mapped down (preparePreprocessedQueryPositions, src/core/pcs/utils.zig:292-314).
 void pcs_tail(const JV& pr, Channel& ch, const std::vector<Hash>& roots, const std::vector<uint32_t>& tree_cols,
-              const std::vector<Batch>& batches, uint32_t L, const Cfg& cfg) {
+              const std::vector<Batch>& batches, uint32_t L, const Cfg& cfg,
+              const std::vector<std::vector<uint32_t>>& tree_logs = {}) {
   const JV& fri = pr["fri_proof"];
   ch.mix_root(hash_of(fri["first_layer"]["commitment"]).data());
   std::vector<QM31> alphas{ch.draw_secure_felt()};
@@ -319,7 +330,15 @@ void pcs_tail(const JV& pr, Channel& ch, const std::vector<Hash>& roots, const s
       if (!wit.empty()) throw Fail("preprocessed tree shape");
       continue;
     }
-    merkle_verify(roots[t], L, queries, tc, wit);
+    const std::vector<uint32_t> logs = tree_logs.empty() ? std::vector<uint32_t>{} : tree_logs[t];
+    const uint32_t depth = logs.empty() ? L : *std::max_element(logs.begin(), logs.end());
+    std::vector<uint64_t> positions = queries;
+    if (depth != L) {
+      if (t != 0 || depth > L) throw Fail("tree size");
+      const uint32_t sh = L - depth + 1;
+      for (uint64_t& p : positions) p = ((p >> sh) << 1) + (p & 1);
+    }
+    merkle_verify(roots[t], depth, positions, tc, wit, logs);
     for (auto& c : tc) cols.push_back(std::move(c));
   }
   // quotient answers at the queries
@@ -513,7 +532,7 @@ int32_t verify_logup_xor_json(const std::string& proof, uint32_t log_n, uint32_t
     const Cfg cfg = read_config(pr);
     const JV& stm = pr["statement"];
     if (stm["log_n"].u() != log_n || stm["log_table"].u() != log_table) throw Fail("statement mismatch");
-    const uint32_t L = std::max(log_n, log_table);
+    const uint32_t n = log_n, t = log_table, L = std::max(n, t), B = cfg.B;
     std::vector<Hash> roots;
     for (const JV& c : pr["commitments"].arr) roots.push_back(hash_of(c));
     if (roots.size() != 4) throw Fail("expected 4 commitments");
@@ -539,51 +558,75 @@ int32_t verify_logup_xor_json(const std::string& proof, uint32_t log_n, uint32_t
     ch.mix_root(roots[3].data());
     const PointQ oods = oods_point(ch);
     PointM g = index_point(1u << (31 - L));
-    const PointQ prev = qpadd(oods, PointQ{qbase(g.x), qneg(qbase(g.y))});
+    const PointQ prev = qpadd(oods, PointQ{qbase(g.x), qneg(qbase(g.y))});  // previous row at the maximal size
+    auto doubled = [&](PointQ p, uint32_t k) {  // the point seen by a column of 2^k rows
+      for (uint32_t i = k; i < L; ++i) p = qpadd(p, p);
+      return p;
+    };
     const JV& sv = pr["sampled_values"];
-    const size_t shape[4] = {4, 4, 8, 8};
+    const size_t shape[4] = {3, 4, 8, 8};
     if (sv.size() != 4) throw Fail("sampled values shape");
     std::vector<QM31> pre, mainv, ic, ip, comp;
-    for (size_t t = 0; t < 4; ++t) {
-      if (sv.at(t).size() != shape[t]) throw Fail("sampled values shape");
-      for (const JV& c : sv.at(t).arr) {
-        if (c.size() != (t == 2 ? 2u : 1u)) throw Fail("sampled values shape");
-        if (t == 0) pre.push_back(qm(c.at(0)));
-        if (t == 1) mainv.push_back(qm(c.at(0)));
-        if (t == 2) { ip.push_back(qm(c.at(0))); ic.push_back(qm(c.at(1))); }
-        if (t == 3) comp.push_back(qm(c.at(0)));
+    for (size_t tr = 0; tr < 4; ++tr) {
+      if (sv.at(tr).size() != shape[tr]) throw Fail("sampled values shape");
+      for (const JV& c : sv.at(tr).arr) {
+        if (c.size() != (tr == 2 ? 2u : 1u)) throw Fail("sampled values shape");
+        if (tr == 0) pre.push_back(qm(c.at(0)));
+        if (tr == 1) mainv.push_back(qm(c.at(0)));
+        if (tr == 2) { ip.push_back(qm(c.at(0))); ic.push_back(qm(c.at(1))); }
+        if (tr == 3) comp.push_back(qm(c.at(0)));
       }
     }
     const QM31 left = secure_of(&comp[0]), right = secure_of(&comp[4]);
     PointQ pt = oods;
     for (uint32_t i = 0; i + 1 < L; ++i) pt = qpadd(pt, pt);
     const QM31 comp_eval = qadd(left, qmul(pt.x, right));
-    const uint32_t inv_n = minv((uint32_t)((1ull << L) % P));
     const QM31 sm = secure_of(&ic[0]), smp = secure_of(&ip[0]), st = secure_of(&ic[4]), stp = secure_of(&ip[4]);
     const QM31 d_main = qsub(qadd(qadd(mainv[0], qmul(alpha, mainv[1])), qmul(alpha2, mainv[2])), z);
     const QM31 d_table = qsub(qadd(qadd(pre[0], qmul(alpha, pre[1])), qmul(alpha2, pre[2])), z);
-    const QM31 c_main = qsub(qmul(qadd(qsub(sm, smp), qmulm(claimed[0], inv_n)), d_main), pre[3]);
-    const QM31 c_table = qadd(qmul(qadd(qsub(st, stp), qmulm(claimed[1], inv_n)), d_table), mainv[3]);
-    const QM31 dinv = qinv(coset_vanishing_q(L, 1u << (31 - (L + 1)), 1u << (31 - L), oods));
-    if (!qeq(qmul(qadd(qmul(random_coeff, c_main), c_table), dinv), comp_eval)) throw Fail("OODS mismatch");
+    const QM31 c_main =
+        qsub(qmul(qadd(qsub(sm, smp), qmulm(claimed[0], minv((uint32_t)((1ull << n) % P)))), d_main), qone());
+    const QM31 c_table =
+        qadd(qmul(qadd(qsub(st, stp), qmulm(claimed[1], minv((uint32_t)((1ull << t) % P)))), d_table), mainv[3]);
+    const QM31 z_main = coset_vanishing_q(n, 1u << (31 - (n + 1)), 1u << (31 - n), doubled(oods, n));
+    const QM31 z_table = coset_vanishing_q(t, 1u << (31 - (t + 1)), 1u << (31 - t), doubled(oods, t));
+    if (!qeq(qadd(qmul(qmul(random_coeff, c_main), qinv(z_main)), qmul(c_table, qinv(z_table))), comp_eval))
+      throw Fail("OODS mismatch");
     std::vector<QM31> flat(pre);
     flat.insert(flat.end(), mainv.begin(), mainv.end());
     for (int c = 0; c < 8; ++c) { flat.push_back(ip[c]); flat.push_back(ic[c]); }
     flat.insert(flat.end(), comp.begin(), comp.end());
     ch.mix_felts(flat.data(), flat.size());
     const QM31 quot_coeff = ch.draw_secure_felt();
+    // random powers over (tree, column, sample), a two-sample column's periodicity sample first;
+    // batches by point in order of first appearance (src/core/pcs/quotients/samples.zig:163-300)
     QM31 rp = qone();
     auto nxt = [&]() { QM31 r = rp; rp = qmul(rp, quot_coeff); return r; };
-    Batch bp{oods, {}}, bprev{prev, {}};
-    for (int c = 0; c < 4; ++c) bp.entries.push_back({(size_t)c, pre[c], nxt()});
-    for (int c = 0; c < 4; ++c) bp.entries.push_back({(size_t)(4 + c), mainv[c], nxt()});
+    std::vector<Batch> batches;
+    auto add = [&](const PointQ& p, size_t col, QM31 v) {
+      for (Batch& bt : batches)
+        if (qeq(bt.point.x, p.x) && qeq(bt.point.y, p.y)) { bt.entries.push_back({col, v, nxt()}); return; }
+      batches.push_back(Batch{p, {}});
+      batches.back().entries.push_back({col, v, nxt()});
+    };
+    for (int c = 0; c < 3; ++c) add(oods, (size_t)c, pre[c]);
+    for (int c = 0; c < 4; ++c) add(oods, (size_t)(3 + c), mainv[c]);
     for (int c = 0; c < 8; ++c) {
-      bp.entries.push_back({(size_t)(8 + c), ic[c], nxt()});
-      bprev.entries.push_back({(size_t)(8 + c), ip[c], nxt()});
-      bp.entries.push_back({(size_t)(8 + c), ic[c], nxt()});
+      const uint32_t k = c < 4 ? n : t;
+      PointQ per = oods;
+      if (k < L) {
+        PointM h = index_point(1u << (31 - L + k));
+        per = qpadd(oods, PointQ{qbase(h.x), qbase(h.y)});
+      }
+      add(per, (size_t)(7 + c), ic[c]);
+      add(prev, (size_t)(7 + c), ip[c]);
+      add(oods, (size_t)(7 + c), ic[c]);
     }
-    for (int c = 0; c < 8; ++c) bp.entries.push_back({(size_t)(16 + c), comp[c], nxt()});
-    pcs_tail(pr, ch, roots, {4, 4, 8, 8}, {bp, bprev}, L + cfg.B, cfg);
+    for (int c = 0; c < 8; ++c) add(oods, (size_t)(15 + c), comp[c]);
+    const std::vector<std::vector<uint32_t>> logs = {
+        {t + B, t + B, t + B}, {n + B, n + B, n + B, t + B}, {n + B, n + B, n + B, n + B, t + B, t + B, t + B, t + B},
+        std::vector<uint32_t>(8, L + B)};
+    pcs_tail(pr, ch, roots, {3, 4, 8, 8}, batches, L + B, cfg, logs);
     return OK;
   } catch (const std::exception& e) {
     err = e.what();

@@ -1,6 +1,8 @@
 """LogUp XOR-lookup AIR proofs on the GPU, checked by the independent verifier (the AIR has no
 reference counterpart, so the verifier's transcript replay, LogUp cancellation, OODS constraint
-check and PCS/FRI decommitment checks are the parity gate)."""
+check and PCS/FRI decommitment checks are the parity gate). The main and table components keep
+their own sizes (2^log_n and 2^log_table rows) under the lifted PCS: cases cover the lookups
+smaller than, equal to and larger than the table."""
 import json
 
 import pytest
@@ -37,19 +39,29 @@ def test_xor_air_full_size_and_determinism(ctx):
     assert a != ctx.prove_logup_xor(20, g, seed=100)
 
 
-@pytest.mark.parametrize("field", ["claimed", "sampled", "queried"])
-def test_xor_air_tampering_rejected(ctx, field):
-    p = ctx.prove_logup_xor(9, _cfg("functional"), seed=5, log_table=8)
+@pytest.mark.parametrize("log_n", [12, 6])
+@pytest.mark.parametrize("field", ["claimed", "sampled", "queried", "sampled_table", "queried_table",
+                                   "preprocessed"])
+def test_xor_air_tampering_rejected(ctx, field, log_n):
+    # log_n 12 > log_table 8: the table component is the smaller, lifted one; log_n 6: the lookups are.
+    p = ctx.prove_logup_xor(log_n, _cfg("functional"), seed=5, log_table=8)
+    assert verifier.verify_logup_xor(p, log_n, 8)
     d = json.loads(p)
     if field == "claimed":
         d["claimed_sums"][0][0] = (d["claimed_sums"][0][0] + 1) % (2**31 - 1)
         d["claimed_sums"][1][0] = (d["claimed_sums"][1][0] - 1) % (2**31 - 1)  # still cancelling
     elif field == "sampled":
         d["sampled_values"][2][3][0][1] = (d["sampled_values"][2][3][0][1] + 1) % (2**31 - 1)
-    else:
+    elif field == "queried":
         d["queried_values"][1][2][0] ^= 1
+    elif field == "sampled_table":  # S_T, previous row
+        d["sampled_values"][2][5][0][2] = (d["sampled_values"][2][5][0][2] + 1) % (2**31 - 1)
+    elif field == "queried_table":  # the multiplicity column m
+        d["queried_values"][1][3][1] ^= 1
+    else:  # the preprocessed table tree
+        d["queried_values"][0][1][0] ^= 1
     with pytest.raises(verifier.VerificationError):
-        verifier.verify_logup_xor(json.dumps(d, separators=(",", ":")).encode(), 9, 8)
+        verifier.verify_logup_xor(json.dumps(d, separators=(",", ":")).encode(), log_n, 8)
 
 
 def test_xor_air_bad_arguments(ctx):
@@ -64,7 +76,7 @@ def test_xor_air_bad_arguments(ctx):
 
 def test_native_verifier_agrees_on_xor_proofs(ctx):
     import stwo_b200 as sb
-    for log_n, lt, seed in ((7, 8, None), (14, 16, 12)):
+    for log_n, lt, seed in ((7, 8, None), (14, 16, 12), (12, 8, 3), (16, 16, None)):
         p = ctx.prove_logup_xor(log_n, _cfg("functional"), seed=3, log_table=lt, channel_seed=seed)
         assert sb.verify_logup_xor(p, log_n, lt, channel_seed=seed)
         with pytest.raises(sb.StwoError):
