@@ -130,9 +130,11 @@ int32_t stwo_b200_prove_wide_fibonacci_batch(stwo_b200_context* ctx, const stwo_
 
 /* LogUp XOR-lookup AIR request: 2^log_n lookups of seeded w-bit operand pairs (w = log_table / 2;
  * log_table 16 for u8 pairs, 8 for 4-bit pairs) into the 2^log_table-row XOR table. No reference
- * AIR exists; the proof uses the reference's PCS, FRI, channel and wire layout with four trees
- * (preprocessed table and selector, main trace and multiplicities, LogUp interaction, composition)
- * and the two LogUp claimed sums, which the verifier requires to cancel. */
+ * AIR exists; the proof uses the reference's lifted PCS, FRI, channel and wire layout, with the
+ * lookups (2^log_n rows) and the table (2^log_table rows) at their own sizes, four trees
+ * (preprocessed table at its size; main trace and multiplicities, LogUp interaction: lifted trees
+ * over both sizes; composition) and the two LogUp claimed sums, which the verifier requires to
+ * cancel. */
 typedef struct {
   uint32_t log_n;
   uint32_t log_table;
