@@ -125,6 +125,13 @@ struct FriChannelDev {
 // mixRoot(root) (src/core/vcs_lifted/blake2_merkle.zig:236-247), then drawSecureFelt
 // (src/core/channel/blake2s.zig:52-112,260-279) into alpha[slot]; the root is kept in roots[slot].
 cudaError_t fri_channel_step(FriChannelDev* c, const uint8_t* root, uint32_t slot, cudaStream_t stream);
+// The inner FRI layers from line layer fri_tail_first(L, n_inner) on (at most 2^12 values each) in one
+// CTA: per layer the channel step, the fold and the next layer's commitment, in the order and with
+// the outputs of fri_channel_step + fri_fold_commit. line[k]: line layer k (4 coordinate columns of
+// 2^(L-1-k)); trees[k]: its tree; line[n_inner] receives the last layer.
+uint32_t fri_tail_first(uint32_t L, uint32_t n_inner);
+cudaError_t fri_tail(const DeviceTables& t, FriChannelDev* c, uint32_t L, uint32_t k0, uint32_t n_inner,
+                     uint32_t* const* line, uint8_t* const* trees, cudaStream_t stream);
 
 // ---- Proof of work (src/core/channel/blake2s.zig:135-240) ------------------
 // Bounded rounds of the same search (the form the prover uses, so the grind

@@ -248,7 +248,7 @@ __global__ void __launch_bounds__(LEAF_THREADS) k_fri_fold_commit(TwiddleView it
 constexpr int FRI_DRAW_TRIES = 64;
 
 // One thread: the channel steps of one FRI layer (see fri_channel_step).
-__global__ void k_fri_channel(FriChannelDev* c, const uint8_t* root, uint32_t slot) {
+__device__ void fri_channel_body(FriChannelDev* c, const uint8_t* root, uint32_t slot) {
   uint32_t m[16], h[8];
   const uint32_t* r = reinterpret_cast<const uint32_t*>(root);
 #pragma unroll
@@ -284,6 +284,62 @@ __global__ void k_fri_channel(FriChannelDev* c, const uint8_t* root, uint32_t sl
   }
   c->status = 1;
   c->alpha[slot] = qmake(0, 0, 0, 0);
+}
+
+__global__ void k_fri_channel(FriChannelDev* c, const uint8_t* root, uint32_t slot) {
+  fri_channel_body(c, root, slot);
+}
+
+// The small inner FRI layers in one CTA: for line layers k = k0 .. n_inner-1 (2^(L-1-k) values,
+// at most 2^FRI_TAIL_LOG), the channel step on layer k's root (alpha into slot k + 1), the fold
+// into layer k + 1 and, below the last layer, the commitment of layer k + 1: leaf hashes and every
+// node level, folded in shared memory. Same arithmetic, buffers and outputs as the per-layer
+// k_fri_channel + k_fri_fold_commit<false> + merkle_finish sequence.
+constexpr uint32_t FRI_TAIL_LOG = 12, FRI_TAIL_THREADS = 1024;
+struct FriTailParams {
+  uint32_t L, k0, n_inner;
+  uint32_t* line[FRI_MAX_LAYERS + 1];
+  uint8_t* tree[FRI_MAX_LAYERS];
+  TwiddleView tv[FRI_MAX_LAYERS];  // inverse view of line layer k's domain (log L - k)
+  Seeds seeds;
+};
+
+__global__ void __launch_bounds__(FRI_TAIL_THREADS) k_fri_tail(FriChannelDev* c, const __grid_constant__ FriTailParams p,
+                                                               uint32_t one) {
+  extern __shared__ uint32_t tsm[];  // (2^(FRI_TAIL_LOG-1)) hashes, then alpha
+  QM31* s_alpha = reinterpret_cast<QM31*>(tsm + (1u << (FRI_TAIL_LOG - 1)) * 8);
+  const uint32_t t = threadIdx.x;
+  for (uint32_t k = p.k0; k < p.n_inner; ++k) {
+    const uint32_t lg = p.L - 1 - k;
+    const uint64_t sz = 1ull << lg, n = sz >> 1;
+    if (t == 0) {
+      fri_channel_body(c, p.tree[k] + (2 * sz - 2) * 32, k + 1);
+      *s_alpha = c->alpha[k + 1];
+    }
+    __syncthreads();
+    const QM31 alpha = *s_alpha;
+    const uint32_t* src = p.line[k];
+    uint32_t* dst = p.line[k + 1];
+    const bool commit = k + 1 < p.n_inner;
+    for (uint32_t i = t; i < n; i += FRI_TAIL_THREADS) {
+      QM31 f0 = qmake(src[2 * i], src[sz + 2 * i], src[2 * sz + 2 * i], src[3 * sz + 2 * i]);
+      QM31 f1 = qmake(src[2 * i + 1], src[sz + 2 * i + 1], src[2 * sz + 2 * i + 1], src[3 * sz + 2 * i + 1]);
+      fri_ibfly(f0, f1, p.tv[k].line(1, i));
+      const QM31 r = qadd(f0, qmul(alpha, f1));
+      dst[i] = r.c0.a; dst[n + i] = r.c0.b; dst[2 * n + i] = r.c1.a; dst[3 * n + i] = r.c1.b;
+      if (commit) {
+        uint32_t h[8], m[16] = {r.c0.a, r.c0.b, r.c1.a, r.c1.b, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
+#pragma unroll
+        for (int q = 0; q < 8; ++q) h[q] = p.seeds.leaf[q];
+        b2s_compress(h, m, 80, true, one);
+        store_hash(p.tree[k + 1], i, h);
+#pragma unroll
+        for (int q = 0; q < 8; ++q) tsm[i * 8 + q] = h[q];
+      }
+    }
+    __syncthreads();
+    if (commit) fold_levels(tsm, (uint32_t)n, lg - 1, p.tree[k + 1], lg - 1, lg - 1, 0, p.seeds.node, one);
+  }
 }
 
 __global__ void k_empty_root(uint8_t* layers, Seeds seeds) {
@@ -326,6 +382,36 @@ static cudaError_t merkle_finish(uint8_t* layers, uint32_t max_log, uint32_t chi
     child_log -= levels;
   }
   return cudaSuccess;
+}
+
+uint32_t fri_tail_first(uint32_t L, uint32_t n_inner) {
+  for (uint32_t k = 0; k < n_inner; ++k)
+    if (L - 1 - k <= FRI_TAIL_LOG) return k;
+  return n_inner;
+}
+
+cudaError_t fri_tail(const DeviceTables& t, FriChannelDev* c, uint32_t L, uint32_t k0, uint32_t n_inner,
+                     uint32_t* const* line, uint8_t* const* trees, cudaStream_t stream) {
+  if (k0 >= n_inner) return cudaSuccess;
+  if (n_inner > FRI_MAX_LAYERS || L - 1 - k0 > FRI_TAIL_LOG) return cudaErrorInvalidValue;
+  FriTailParams p{};
+  p.L = L;
+  p.k0 = k0;
+  p.n_inner = n_inner;
+  for (uint32_t k = k0; k <= n_inner; ++k) p.line[k] = line[k];
+  for (uint32_t k = k0; k < n_inner; ++k) {
+    p.tree[k] = trees[k];
+    p.tv[k] = t.view(L - k, true);
+  }
+  p.seeds = seeds_once();
+  const size_t smem = (1u << (FRI_TAIL_LOG - 1)) * 32 + 16;
+  static const bool attr = [&] {  // once per process (thread-safe static initialisation)
+    cudaFuncSetAttribute(k_fri_tail, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    return true;
+  }();
+  (void)attr;
+  k_fri_tail<<<1, FRI_TAIL_THREADS, smem, stream>>>(c, p, 1u); note_launch();
+  return cudaGetLastError();
 }
 
 cudaError_t fri_channel_step(FriChannelDev* c, const uint8_t* root, uint32_t slot, cudaStream_t stream) {

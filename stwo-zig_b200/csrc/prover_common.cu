@@ -37,13 +37,16 @@ int32_t fri_pow_queries(const DeviceTables& T, int sm_count, Channel& ch, const 
     // commits it in the same launch sequence.
     SB_CKE(fri_fold_commit(T, true, L, fb.quot, NL, &fb.chan->alpha[0], fb.line[0], 1ull << (L - 1),
                           n_inner > 0 ? fb.line_tree[0] : nullptr, fs));
-    for (uint32_t k = 0; k < n_inner; ++k) {
+    // Large layers one launch sequence each; the small ones (at most 2^12 values) in one CTA.
+    const uint32_t k_tail = fri_tail_first(L, n_inner);
+    for (uint32_t k = 0; k < k_tail; ++k) {
       uint32_t lg = L - 1 - k;
       size_t sz = 1ull << lg;
       SB_CKE(fri_channel_step(fb.chan, fb.line_tree[k] + (2 * sz - 2) * 32, k + 1, fs));
       SB_CKE(fri_fold_commit(T, false, lg, fb.line[k], sz, &fb.chan->alpha[k + 1], fb.line[k + 1], sz / 2,
                             k + 1 < n_inner ? fb.line_tree[k + 1] : nullptr, fs));
     }
+    SB_CKE(fri_tail(T, fb.chan, L, k_tail, n_inner, fb.line.data(), fb.line_tree.data(), fs));
     // One copy back: the device channel (roots, alphas) and the last layer's values.
     SB_CKE(cudaMemcpyAsync(pin, fb.chan, sizeof(FriChannelDev), cudaMemcpyDeviceToHost, fs));
     SB_CKE(cudaMemcpyAsync(pin + LAST_OFF, fb.line[n_inner], 4 * m_last * 4, cudaMemcpyDeviceToHost, fs));
