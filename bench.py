@@ -419,6 +419,16 @@ def main():
                      "frac": fft_gbs / hbm_peak, "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)",
                      "traffic": FFT_TRAFFIC_BYTES.get((args.log_n, args.width)),
                      "algorithmic_bytes": fft_bytes, "ms": fft_ms},
+        "roofline_issue": ({"kernel": "circle FFT pass (k_fft_low12<1>, k_fft_high16, k_fft_low12<0>)",
+                            "unit": "warp instructions/s",
+                            "instructions": FFT_WARP_INSTR_PER_COL_2P20 * args.width,
+                            "achieved": FFT_WARP_INSTR_PER_COL_2P20 * args.width / (fft_ms / 1e3),
+                            "peak": 148 * 4 * 1e6 * (clocks.summary().get("sm_mhz") or 1965.0),
+                            "peak_source": "148 SMs x 4 schedulers x 1 warp instruction per cycle x sampled SM "
+                                           "clock (nominal issue rate)",
+                            "instructions_source": "ncu smsp__inst_executed.sum of the three pass kernels on 40 "
+                                                   "columns of 2^20, per column"}
+                           if args.log_n == 20 else None),
         "roofline_int32": {"kernel": "k_pow_round (Blake2s, 1 compression per nonce)", "hashes_per_s": hashes_per_s,
                            "nonces": nonce + 1, "ms": pow_ms, "unit": "thread instructions/s",
                            "achieved": hashes_per_s * POW_INSTR_PER_NONCE,
@@ -429,6 +439,8 @@ def main():
     }
     ri = out["roofline_int32"]
     ri["frac"] = ri["achieved"] / ri["peak"]
+    if out["roofline_issue"]:
+        out["roofline_issue"]["frac"] = out["roofline_issue"]["achieved"] / out["roofline_issue"]["peak"]
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         n_cpu = min(3, n_traces)
         total, same = 0.0, True
@@ -684,6 +696,9 @@ FFT_TRAFFIC_BYTES: dict = {(20, 100): 1531.5e6 * 100 / 40}
 # Thread instructions per nonce of the grind (one ncu capture of a 26-bit round:
 # 550.2 M warp instructions x 32 / 16,973,824 nonces).
 POW_INSTR_PER_NONCE = 1037
+# Warp instructions of one interpolate + blow-up extend of a 2^20 column (ncu smsp__inst_executed.sum
+# of k_fft_low12<1> + k_fft_high16 + k_fft_low12<0>: 557,465,600 for 40 columns).
+FFT_WARP_INSTR_PER_COL_2P20 = 557_465_600 // 40
 
 if __name__ == "__main__":
     main()
