@@ -14,7 +14,7 @@ The reference arm times the CPU prover, one proof per step (a bounded sample).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
     python bench.py --workload mixed48      # 48 mixed-shape proofs in one submission
-    python bench.py --workload serve [--rates 25,50,100,200] [--requests 64]
+    python bench.py --workload serve [--rates 25,50,100,200,400] [--requests 64]
                                             # Poisson arrivals into the serving loop
     python bench.py --workload kernels128   # kernel-level ops: 128 columns 2^20 -> 2^21, Merkle,
                                             # fold_circle_into_line 2^21 and fold_line to 2^4
@@ -57,7 +57,7 @@ def parse():
     ap.add_argument("--batch", type=int, default=BATCH, help="proofs per step (headline workload)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--workload", default="headline", choices=["headline", "mixed48", "serve", "kernels128"])
-    ap.add_argument("--rates", default="25,50,100,200")
+    ap.add_argument("--rates", default="25,50,100,200,400")
     ap.add_argument("--requests", type=int, default=64)
     ap.add_argument("--slots", type=int, default=8)
     return ap.parse_args()
