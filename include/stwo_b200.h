@@ -308,6 +308,17 @@ int32_t stwo_b200_accumulate_quotients(stwo_b200_context* ctx, uint32_t log_size
                                        stwo_b200_qm31 px, stwo_b200_qm31 py, stwo_b200_qm31 sum_a,
                                        stwo_b200_qm31 sum_b, uint32_t* out, uint64_t out_stride, void* stream);
 
+/* ---- AccumulationOps (src/backend/accumulation_ops.zig) -------------------------------------------- */
+
+/* Lifted accumulation of secure columns: dst (4 coordinate columns of 2^dst_log, stride dst_stride)
+ * += coeff * src (4 coordinate columns of 2^src_log <= 2^dst_log), where row i of dst reads src at
+ * ((i >> (dst_log - src_log + 1)) << 1) + (i & 1), or at i for equal sizes: the accumulate hook and
+ * DomainEvaluationAccumulator.accumulateColumn + finalize (src/prover/air/accumulation.zig:256-347,
+ * liftedValueAt :336-347). Device pointers, async on `stream`. */
+int32_t stwo_b200_accumulate(stwo_b200_context* ctx, uint32_t dst_log, uint32_t* dst, uint64_t dst_stride,
+                             uint32_t src_log, const uint32_t* src, uint64_t src_stride, stwo_b200_qm31 coeff,
+                             void* stream);
+
 /* ---- Wide-Fibonacci AIR -------------------------------------------------------------------------- */
 
 /* Trace generation in bit-reversed circle order (fillQuadraticRecurrenceTrace hook,

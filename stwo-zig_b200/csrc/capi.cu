@@ -357,6 +357,17 @@ int32_t stwo_b200_wide_fib_composition(stwo_b200_context* ctx, uint32_t log_n_ro
                      "wide_fib_composition");
 }
 
+int32_t stwo_b200_accumulate(stwo_b200_context* ctx, uint32_t dst_log, uint32_t* dst, uint64_t dst_stride,
+                             uint32_t src_log, const uint32_t* src, uint64_t src_stride, stwo_b200_qm31 coeff,
+                             void* stream) {
+  CK_CTX(ctx);
+  if (dst_log > 30 || src_log > dst_log || !dst || !src || dst_stride < (1ull << dst_log) ||
+      src_stride < (1ull << src_log))
+    return set_error(STWO_B200_E_INVALID, "bad accumulate arguments");
+  return cuda_status(sb::accumulate_lifted(dst_log, dst, dst_stride, src_log, src, src_stride, q(coeff), st(stream)),
+                     "accumulate");
+}
+
 int32_t stwo_b200_pow_grind(stwo_b200_context* ctx, const uint8_t prefix_digest[32], uint32_t n_bits,
                             uint64_t* nonce_out) {
   CK_CTX(ctx);

@@ -65,6 +65,11 @@ SB_HD uint64_t merkle_layer_offset(uint32_t max_log, uint32_t layer_log) {
   return (1ull << (max_log + 1)) - (1ull << (layer_log + 1));
 }
 
+// ---- Lifted accumulation (DomainEvaluationAccumulator, src/prover/air/accumulation.zig:256-347):
+// dst (4 coordinate columns of 2^dst_log) += coeff * src (4 coordinate columns of 2^src_log) lifted.
+cudaError_t accumulate_lifted(uint32_t dst_log, uint32_t* dst, uint64_t dst_stride, uint32_t src_log,
+                              const uint32_t* src, uint64_t src_stride, QM31 coeff, cudaStream_t stream);
+
 // ---- Wide-Fibonacci composition (src/examples/wide_fibonacci/component.zig:138-236)
 // out: 4 coordinate columns of 2^(log_n+1). `eval` holds the W trace columns on
 // CanonicCoset(log_n + 1). `coeffs` has W-2 QM31 (constraint k uses coeffs[k]).

@@ -561,6 +561,33 @@ cudaError_t wide_fib_composition(uint32_t log_n, uint32_t W, const uint32_t* eva
   return cudaGetLastError();
 }
 
+namespace {
+// dst[i] += coeff * src[lifted i] over 4 coordinate columns (src of 2^src_log <= 2^dst_log rows).
+__global__ void k_accumulate_lifted(uint32_t dst_log, uint32_t* dst, uint64_t ds, uint32_t src_log,
+                                    const uint32_t* __restrict__ src, uint64_t ss, QM31 coeff) {
+  const uint64_t n = 1ull << dst_log;
+  const uint32_t sh = dst_log - src_log + 1;
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+    const uint64_t j = src_log == dst_log ? i : (((i >> sh) << 1) | (i & 1));
+    const QM31 v = qmul(coeff, qmake(src[j], src[ss + j], src[2 * ss + j], src[3 * ss + j]));
+    dst[i] = madd(dst[i], v.c0.a);
+    dst[ds + i] = madd(dst[ds + i], v.c0.b);
+    dst[2 * ds + i] = madd(dst[2 * ds + i], v.c1.a);
+    dst[3 * ds + i] = madd(dst[3 * ds + i], v.c1.b);
+  }
+}
+
+}  // namespace
+
+cudaError_t accumulate_lifted(uint32_t dst_log, uint32_t* dst, uint64_t dst_stride, uint32_t src_log,
+                              const uint32_t* src, uint64_t src_stride, QM31 coeff, cudaStream_t stream) {
+  if (src_log > dst_log) return cudaErrorInvalidValue;
+  k_accumulate_lifted<<<grid_for(1ull << dst_log, 256), 256, 0, stream>>>(dst_log, dst, dst_stride, src_log, src,
+                                                                           src_stride, coeff);
+  note_launch();
+  return cudaGetLastError();
+}
+
 size_t eval_at_point_partial_count(uint32_t log_size, uint32_t n_cols) {
   uint32_t chunk_bits = log_size < OODS_CHUNK_BITS ? log_size : OODS_CHUNK_BITS;
   return (size_t)n_cols << (log_size - chunk_bits);
