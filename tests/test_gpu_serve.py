@@ -131,6 +131,26 @@ def test_served_mix_with_xor_lookups(ctx):
                                                  trace_seed=r[3])
 
 
+def test_served_first_column_traces(ctx):
+    """Requests that hand the server only col0/col1 from host memory (TRACE_FIRST_COLUMNS): the
+    buffers are read when a slot runs the request; proofs equal the seeded single runs."""
+    import stwo_b200 as sb
+    import torch
+    g = _cfg("functional")
+    shapes = [(14, 32, 3), (16, 100, 4), (12, 16, 5), (15, 17, 6)]
+    twos = []
+    for log_n, W, seed in shapes:
+        full = torch.empty(W << log_n, dtype=torch.int32, device="cuda")
+        ctx.wide_fib_trace(full, log_n, W, sb.TRACE_SEEDED, seed)
+        twos.append(full[: 2 << log_n].cpu().numpy().view(np.uint32).reshape(2, -1).copy())
+    with sb.Server(ctx, slots=3, profile=1) as srv:
+        ts = [srv.submit(sb.Statement(n, W), g, trace=two, trace_kind=sb.TRACE_FIRST_COLUMNS)
+              for (n, W, _), two in zip(shapes, twos)]
+        out = [srv.wait(t)[0] for t in ts]
+    for (n, W, seed), p in zip(shapes, out):
+        assert p == ctx.prove_wide_fibonacci(sb.Statement(n, W), g, trace_kind=sb.TRACE_SEEDED, trace_seed=seed)
+
+
 def test_warmup_presizes_slots(ctx):
     import stwo_b200 as sb
     g = _cfg("functional")
