@@ -22,6 +22,8 @@ def _cfg(preset, **over):
 @pytest.mark.parametrize("log_n,log_table,preset,over", [
     (1, 8, "smoke", {}), (6, 8, "smoke", {}), (9, 8, "functional", {}), (10, 8, "functional", {}),
     (8, 8, "functional", dict(log_blowup_factor=2, n_queries=5, log_last_layer_degree_bound=1)),
+    (11, 8, "functional", dict(log_blowup_factor=2, n_queries=5, log_last_layer_degree_bound=1)),
+    (5, 8, "functional", dict(log_blowup_factor=3, n_queries=4)),
     (12, 16, "secure", {}), (16, 16, "functional", {}), (18, 16, "secure", {})])
 def test_xor_air_proof_verifies(ctx, log_n, log_table, preset, over):
     g = _cfg(preset, **over)
