@@ -692,7 +692,7 @@ def run_serve(args, ctx):
 # DRAM bytes (read + write) of one FFT pass (the 3-kernel interpolate+extend chain) from one ncu
 # capture of 2^20 rows x 40 columns (dram__bytes_read.sum + dram__bytes_write.sum = 1531.5 MB),
 # scaled to 100 columns; traffic is linear in the column count.
-FFT_TRAFFIC_BYTES: dict = {(20, 100): 1531.5e6 * 100 / 40}
+FFT_TRAFFIC_BYTES: dict = {(20, 100): 1532.8e6 * 100 / 40}
 # Thread instructions per nonce of the grind (one ncu capture of a 26-bit round:
 # 550.2 M warp instructions x 32 / 16,973,824 nonces).
 POW_INSTR_PER_NONCE = 1037
