@@ -170,9 +170,9 @@ def run_reference(args, rank, world):
 
 
 def config_block(args, batch=1):
-    per_step = "one proof per step" if batch == 1 else f"one batch of {batch} proofs per step"
-    return {"workload": f"wide-Fibonacci 2^{args.log_n}x{args.width}, {args.preset} preset, {per_step}",
-            "log_n_rows": args.log_n, "sequence_len": args.width, "protocol": args.preset,
+    step = "one proof (a bounded sample of the workload)" if batch == 1 else f"one batch of {batch} proofs"
+    return {"workload": f"wide-Fibonacci 2^{args.log_n}x{args.width}, {args.preset} preset",
+            "step": step, "log_n_rows": args.log_n, "sequence_len": args.width, "protocol": args.preset,
             "proofs_per_step": batch,
             "in_flight": args.in_flight,
             "l2": (f"inputs larger than L2 ({(4 * args.width << args.log_n) / 1e6:.0f} MB trace per proof)"
