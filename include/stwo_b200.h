@@ -326,6 +326,13 @@ int32_t stwo_b200_accumulate(stwo_b200_context* ctx, uint32_t dst_log, uint32_t*
  * trace_kind 2 derives columns 2.. from the col0/col1 already in `out`. */
 int32_t stwo_b200_wide_fib_trace(stwo_b200_context* ctx, uint32_t log_n_rows, uint32_t sequence_len,
                                  uint32_t trace_kind, uint64_t seed, uint32_t* out, uint64_t stride, void* stream);
+/* Trace of a seven-word quadratic recurrence in bit-reversed circle order (the
+ * fillQuadraticRecurrenceTrace hook and its recipe ABI, src/examples/wide_fibonacci/trace.zig:13-16,
+ * 63-74): for logical (coset-order) row k, col0 = r0 + r1 k, col1 = r2 + r3 k and
+ * col_j = r4 col_{j-2}^2 + r5 col_{j-1}^2 + r6 in M31. The wide-Fibonacci recipe is
+ * {1, 0, 0, 1, 1, 1, 0}. n_cols >= 2 columns of `stride` words at `out` (device). */
+int32_t stwo_b200_quadratic_recurrence_trace(stwo_b200_context* ctx, uint32_t log_n_rows, uint32_t n_cols,
+                                             const uint32_t recipe[7], uint32_t* out, uint64_t stride, void* stream);
 /* Composition evaluation on CanonicCoset(log_n_rows+1): out (4 columns) = sum_k coeffs[k] *
  * (c_k - a_k^2 - b_k^2) * den_inv[row >> log_n_rows] (computeCompositionEvaluation hook,
  * src/prover/air/component_prover.zig:269; src/examples/wide_fibonacci/component.zig:138-236). */

@@ -344,6 +344,15 @@ int32_t stwo_b200_wide_fib_trace(stwo_b200_context* ctx, uint32_t log_n_rows, ui
                      "wide_fib_trace");
 }
 
+int32_t stwo_b200_quadratic_recurrence_trace(stwo_b200_context* ctx, uint32_t log_n_rows, uint32_t n_cols,
+                                             const uint32_t recipe[7], uint32_t* out, uint64_t stride, void* stream) {
+  CK_CTX(ctx);
+  if (log_n_rows == 0 || log_n_rows > 28 || n_cols < 2 || !recipe || !out || stride < (1ull << log_n_rows))
+    return set_error(STWO_B200_E_INVALID, "bad quadratic recurrence arguments");
+  return cuda_status(sb::quadratic_trace(log_n_rows, n_cols, recipe, out, stride, st(stream)),
+                     "quadratic_recurrence_trace");
+}
+
 int32_t stwo_b200_wide_fib_composition(stwo_b200_context* ctx, uint32_t log_n_rows, uint32_t sequence_len,
                                        const uint32_t* eval, uint64_t stride, const stwo_b200_qm31* coeffs_dev,
                                        uint32_t den_inv0, uint32_t den_inv1, uint32_t* out, uint64_t out_stride,

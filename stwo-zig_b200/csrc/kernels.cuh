@@ -147,6 +147,9 @@ cudaError_t pow_round(const uint32_t prefix_words[8], uint32_t n_bits, uint64_t 
                       int sm_count, cudaStream_t stream);
 
 // ---- Trace generation (src/examples/wide_fibonacci/trace.zig:34-162) -------
+// Seven-word quadratic recurrence (row seeds r0 + r1 k, r2 + r3 k; next = r4 a^2 + r5 b^2 + r6).
+cudaError_t quadratic_trace(uint32_t log_n, uint32_t W, const uint32_t recipe[7], uint32_t* out, uint64_t stride,
+                            cudaStream_t stream);
 cudaError_t wide_fib_trace(uint32_t log_n, uint32_t W, int kind, uint64_t seed, uint32_t* out,
                            uint64_t stride, cudaStream_t stream);
 

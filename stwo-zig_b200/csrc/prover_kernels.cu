@@ -60,6 +60,27 @@ __global__ void k_wide_fib_trace(uint32_t log_n, uint32_t W, int kind, uint64_t 
   }
 }
 
+// Quadratic-recurrence trace of a seven-word recipe (the fillQuadraticRecurrenceTrace column
+// source, src/examples/wide_fibonacci/trace.zig:13-16): for the logical row k of each storage
+// position, col0 = r0 + r1 k, col1 = r2 + r3 k, col_j = r4 col_{j-2}^2 + r5 col_{j-1}^2 + r6 (M31).
+struct QuadRecipe { uint32_t r[7]; };
+__global__ void k_quadratic_trace(uint32_t log_n, uint32_t W, QuadRecipe q, uint32_t* out, uint64_t stride) {
+  const uint32_t n = 1u << log_n;
+  for (uint32_t s = blockIdx.x * blockDim.x + threadIdx.x; s < n; s += gridDim.x * blockDim.x) {
+    const uint32_t ci = bitrev(s, log_n);
+    const uint32_t row = ci < n / 2 ? ci * 2 : (n - 1 - ci) * 2 + 1;
+    uint32_t a = madd(q.r[0], mmul(q.r[1], row)), b = madd(q.r[2], mmul(q.r[3], row));
+    out[s] = a;
+    out[stride + s] = b;
+    for (uint32_t k = 2; k < W; ++k) {
+      const uint32_t c = madd(madd(mmul(q.r[4], mmul(a, a)), mmul(q.r[5], mmul(b, b))), q.r[6]);
+      out[k * stride + s] = c;
+      a = b;
+      b = c;
+    }
+  }
+}
+
 // ---------------------------------------------------------------------------
 // Composition (src/examples/wide_fibonacci/component.zig:138-236): per row of
 // CanonicCoset(n+1), sum_k coeff_k * (c_k - a_k^2 - b_k^2), times the inverse
@@ -533,6 +554,14 @@ inline uint32_t grid_for(uint64_t n, uint32_t threads, uint32_t cap = 148 * 32) 
 }
 
 }  // namespace
+
+cudaError_t quadratic_trace(uint32_t log_n, uint32_t W, const uint32_t recipe[7], uint32_t* out, uint64_t stride,
+                            cudaStream_t stream) {
+  QuadRecipe q;
+  for (int i = 0; i < 7; ++i) q.r[i] = recipe[i] % P;
+  k_quadratic_trace<<<grid_for(1ull << log_n, 256), 256, 0, stream>>>(log_n, W, q, out, stride); note_launch();
+  return cudaGetLastError();
+}
 
 cudaError_t wide_fib_trace(uint32_t log_n, uint32_t W, int kind, uint64_t seed, uint32_t* out, uint64_t stride,
                            cudaStream_t stream) {

@@ -110,6 +110,7 @@ _SIGS = {
     "stwo_b200_wide_fib_trace": [_vp, _u32, _u32, _u32, _u64, _vp, _u64, _vp],
     "stwo_b200_wide_fib_composition": [_vp, _u32, _u32, _vp, _u64, _vp, _u32, _u32, _vp, _u64, _vp],
     "stwo_b200_accumulate": [_vp, _u32, _vp, _u64, _u32, _vp, _u64, QM31C, _vp],
+    "stwo_b200_quadratic_recurrence_trace": [_vp, _u32, _u32, ctypes.POINTER(_u32), _vp, _u64, _vp],
     "stwo_b200_pow_grind": [_vp, ctypes.c_char_p, _u32, ctypes.POINTER(_u64)],
     "stwo_b200_telemetry_snapshot": [ctypes.POINTER(_u64)],
     "stwo_b200_prove_logup_xor": [_vp, ctypes.POINTER(XorRequestC), _vp, ctypes.c_size_t,
@@ -436,6 +437,12 @@ class Context:
         """dst (4 x 2^dst_log coordinate words) += coeff * src (4 x 2^src_log), src lifted to dst's size."""
         _check(_lib.stwo_b200_accumulate(self._h, dst_log, _ptr(dst), 1 << dst_log, src_log, _ptr(src), 1 << src_log,
                                          _qm(coeff), _stream(stream)))
+
+    def quadratic_recurrence_trace(self, out, log_n_rows: int, n_cols: int, recipe, stream=None) -> None:
+        """n_cols columns of the seven-word quadratic recurrence (recipe) in bit-reversed circle order."""
+        r = (_u32 * 7)(*[int(x) for x in recipe])
+        _check(_lib.stwo_b200_quadratic_recurrence_trace(self._h, log_n_rows, n_cols, r, _ptr(out), 1 << log_n_rows,
+                                                         _stream(stream)))
 
     def wide_fib_composition(self, eval_cols, log_n_rows: int, sequence_len: int, coeffs, den0: int, den1: int,
                              out, stream=None) -> None:
