@@ -303,6 +303,31 @@ int32_t stwo_b200_fold_line(stwo_b200_context* ctx, uint32_t src_log, const uint
  * (random-coefficient scaled), sum_a / sum_b the batch's summed a and b line coefficients
  * (src/core/pcs/quotients/row_evaluation.zig:71-101,400-521). Replaces accumulateQuotients and
  * accumulate_quotients (ffi.zig:94). */
+/* One FRI fold fused with the commitment of the folded layer (foldLineAndCommitNext and the first
+ * layer's fold, src/prover/fri.zig:314-592; Metal foldLineAndCommitNext / commitFriLayers): circle != 0
+ * folds a circle evaluation of 2^src_log values into a line (foldCircleIntoLine without accumulation),
+ * else a line of 2^src_log values into its half (foldLine). src: 4 coordinate columns, 8-byte aligned,
+ * even stride; dst: 4 columns of 2^(src_log-1). layers_dev (nullable: fold only) receives the folded
+ * layer's Merkle tree (2^src_log - 1 hashes, leaf = the 4 coordinates); root_host (nullable) its root
+ * after the stream synchronizes. */
+int32_t stwo_b200_fold_and_commit(stwo_b200_context* ctx, int32_t circle, uint32_t src_log, const uint32_t* src,
+                                  uint64_t src_stride, stwo_b200_qm31 alpha, uint32_t* dst, uint64_t dst_stride,
+                                  uint8_t* layers_dev, uint8_t* root_host, void* stream);
+/* Interpolate, extend by 2^log_blowup and commit the extension (prepareAndCommitPolys /
+ * prepareAndCommitOwned, src/backends/metal/commit_backend.zig; src/prover/pcs/commit_polys.zig:10-67):
+ * stwo_b200_interpolate_and_extend followed by stwo_b200_merkle_commit of the n_cols LDE columns. */
+int32_t stwo_b200_commit_columns(stwo_b200_context* ctx, uint32_t log_size, uint32_t log_blowup, uint32_t n_cols,
+                                 const uint32_t* evals, uint64_t evals_stride, uint32_t* coeffs, uint64_t coeffs_stride,
+                                 uint32_t* lde, uint64_t lde_stride, uint8_t* layers_dev, uint8_t* root_host,
+                                 void* stream);
+/* The composition polynomial's interpolation, split and extension (interpolateSecureComposition,
+ * src/prover/poly/circle/secure_poly.zig:77-105,164-226): comp holds the 4 coordinate columns of its
+ * evaluations on CanonicCoset(comp_log) and receives their coefficients; lde receives 8 columns of
+ * 2^(comp_log-1+log_blowup): the extensions of the 4 left halves (first 2^(comp_log-1) coefficients),
+ * then of the 4 right halves. */
+int32_t stwo_b200_interpolate_secure_composition(stwo_b200_context* ctx, uint32_t comp_log, uint32_t* comp,
+                                                 uint64_t comp_stride, uint32_t log_blowup, uint32_t* lde,
+                                                 uint64_t lde_stride, void* stream);
 int32_t stwo_b200_accumulate_quotients(stwo_b200_context* ctx, uint32_t log_size, uint32_t n_cols,
                                        const uint32_t* const* col_ptrs_dev, const stwo_b200_qm31* c_dev,
                                        stwo_b200_qm31 px, stwo_b200_qm31 py, stwo_b200_qm31 sum_a,

@@ -309,6 +309,73 @@ int32_t stwo_b200_fold_line(stwo_b200_context* ctx, uint32_t src_log, const uint
                      "fold_line");
 }
 
+namespace {
+int32_t read_root(uint8_t* root_host, const uint8_t* layers_dev, uint32_t log_size, cudaStream_t s,
+                  const char* what) {
+  if (!root_host) return STWO_B200_OK;
+  const uint64_t root_node = (2ull << log_size) - 2;
+  cudaError_t e = cudaMemcpyAsync(root_host, layers_dev + root_node * 32, 32, cudaMemcpyDeviceToHost, s);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  return cuda_status(e, what);
+}
+}  // namespace
+
+int32_t stwo_b200_fold_and_commit(stwo_b200_context* ctx, int32_t circle, uint32_t src_log, const uint32_t* src,
+                                  uint64_t src_stride, stwo_b200_qm31 alpha, uint32_t* dst, uint64_t dst_stride,
+                                  uint8_t* layers_dev, uint8_t* root_host, void* stream) {
+  CK_CTX(ctx);
+  if (src_log < 2 || !domain_ok(ctx, circle ? src_log : src_log + 1) || !src || !dst ||
+      (reinterpret_cast<uintptr_t>(src) & 7) || (src_stride & 1) || src_stride < (1ull << src_log) ||
+      dst_stride < (1ull << (src_log - 1)) || (root_host && !layers_dev))
+    return set_error(STWO_B200_E_INVALID, "bad fold_and_commit arguments");
+  cudaStream_t s = st(stream);
+  void* a_dev = nullptr;
+  cudaError_t e = cudaMallocAsync(&a_dev, sizeof(sb::QM31), s);
+  if (e != cudaSuccess) return cuda_status(e, "fold_and_commit alpha");
+  const sb::QM31 a = q(alpha);
+  e = cudaMemcpyAsync(a_dev, &a, sizeof(a), cudaMemcpyHostToDevice, s);
+  if (e == cudaSuccess)
+    e = sb::fri_fold_commit(ctx->ctx.tables, circle != 0, src_log, src, src_stride,
+                            static_cast<const sb::QM31*>(a_dev), dst, dst_stride, layers_dev, s);
+  cudaError_t e2 = cudaFreeAsync(a_dev, s);
+  if (e != cudaSuccess) return cuda_status(e, "fold_and_commit");
+  if (e2 != cudaSuccess) return cuda_status(e2, "fold_and_commit alpha free");
+  return read_root(root_host, layers_dev, src_log - 1, s, "fold_and_commit root readback");
+}
+
+int32_t stwo_b200_commit_columns(stwo_b200_context* ctx, uint32_t log_size, uint32_t log_blowup, uint32_t n_cols,
+                                 const uint32_t* evals, uint64_t evals_stride, uint32_t* coeffs, uint64_t coeffs_stride,
+                                 uint32_t* lde, uint64_t lde_stride, uint8_t* layers_dev, uint8_t* root_host,
+                                 void* stream) {
+  CK_CTX(ctx);
+  if (!domain_ok(ctx, log_size + log_blowup) || log_blowup == 0 || log_blowup > 4 || n_cols == 0 || !evals ||
+      !coeffs || !lde || !layers_dev)
+    return set_error(STWO_B200_E_INVALID, "bad commit_columns arguments");
+  cudaStream_t s = st(stream);
+  cudaError_t e = sb::interpolate_extend(ctx->ctx.tables, log_size, log_blowup, n_cols, evals, evals_stride, coeffs,
+                                         coeffs_stride, lde, lde_stride, s);
+  if (e == cudaSuccess) e = sb::merkle_commit(log_size + log_blowup, n_cols, lde, lde_stride, layers_dev, s);
+  if (e != cudaSuccess) return cuda_status(e, "commit_columns");
+  return read_root(root_host, layers_dev, log_size + log_blowup, s, "commit_columns root readback");
+}
+
+int32_t stwo_b200_interpolate_secure_composition(stwo_b200_context* ctx, uint32_t comp_log, uint32_t* comp,
+                                                 uint64_t comp_stride, uint32_t log_blowup, uint32_t* lde,
+                                                 uint64_t lde_stride, void* stream) {
+  CK_CTX(ctx);
+  if (comp_log < 2 || log_blowup == 0 || log_blowup > 4 || !domain_ok(ctx, comp_log - 1 + log_blowup) || !comp ||
+      !lde || comp_stride < (1ull << comp_log))
+    return set_error(STWO_B200_E_INVALID, "bad interpolate_secure_composition arguments");
+  cudaStream_t s = st(stream);
+  const sb::DeviceTables& T = ctx->ctx.tables;
+  const uint32_t half_log = comp_log - 1;
+  cudaError_t e = sb::fft_columns(T, true, comp_log, 4, comp, comp_stride, s);
+  if (e == cudaSuccess) e = sb::extend(T, half_log, log_blowup, 4, comp, comp_stride, lde, lde_stride, s);
+  if (e == cudaSuccess)
+    e = sb::extend(T, half_log, log_blowup, 4, comp + (1ull << half_log), comp_stride, lde + 4 * lde_stride, lde_stride, s);
+  return cuda_status(e, "interpolate_secure_composition");
+}
+
 int32_t stwo_b200_accumulate_quotients(stwo_b200_context* ctx, uint32_t log_size, uint32_t n_cols,
                                        const uint32_t* const* col_ptrs_dev, const stwo_b200_qm31* c_dev,
                                        stwo_b200_qm31 px, stwo_b200_qm31 py, stwo_b200_qm31 sum_a,

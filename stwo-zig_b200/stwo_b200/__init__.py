@@ -110,6 +110,9 @@ _SIGS = {
     "stwo_b200_wide_fib_trace": [_vp, _u32, _u32, _u32, _u64, _vp, _u64, _vp],
     "stwo_b200_wide_fib_composition": [_vp, _u32, _u32, _vp, _u64, _vp, _u32, _u32, _vp, _u64, _vp],
     "stwo_b200_accumulate": [_vp, _u32, _vp, _u64, _u32, _vp, _u64, QM31C, _vp],
+    "stwo_b200_fold_and_commit": [_vp, _i32, _u32, _vp, _u64, QM31C, _vp, _u64, _vp, _vp, _vp],
+    "stwo_b200_commit_columns": [_vp, _u32, _u32, _u32, _vp, _u64, _vp, _u64, _vp, _u64, _vp, _vp, _vp],
+    "stwo_b200_interpolate_secure_composition": [_vp, _u32, _vp, _u64, _u32, _vp, _u64, _vp],
     "stwo_b200_quadratic_recurrence_trace": [_vp, _u32, _u32, ctypes.POINTER(_u32), _vp, _u64, _vp],
     "stwo_b200_pow_grind": [_vp, ctypes.c_char_p, _u32, ctypes.POINTER(_u64)],
     "stwo_b200_telemetry_snapshot": [ctypes.POINTER(_u64)],
@@ -402,6 +405,31 @@ class Context:
         root = ctypes.create_string_buffer(32)
         _check(_lib.stwo_b200_merkle_commit_lifted(self._h, n, ptrs, logs, _ptr(layers), root, _stream(stream)))
         return root.raw
+
+    def fold_and_commit(self, src, dst, src_log: int, alpha, layers=None, circle: bool = False, stream=None):
+        """One FRI fold (circle -> line when circle, else line -> half line) and the Merkle tree of the
+        folded layer in `layers`; returns its root (None without layers)."""
+        root = ctypes.create_string_buffer(32) if layers is not None else None
+        _check(_lib.stwo_b200_fold_and_commit(self._h, int(circle), src_log, _ptr(src), 1 << src_log, _qm(alpha),
+                                              _ptr(dst), 1 << (src_log - 1),
+                                              _ptr(layers) if layers is not None else None, root, _stream(stream)))
+        return root.raw if root is not None else None
+
+    def commit_columns(self, evals, coeffs, lde, layers, log_size: int, log_blowup: int, n_cols: int,
+                       stream=None) -> bytes:
+        """Interpolate, extend and commit n_cols columns; returns the root."""
+        root = ctypes.create_string_buffer(32)
+        _check(_lib.stwo_b200_commit_columns(self._h, log_size, log_blowup, n_cols, _ptr(evals), 1 << log_size,
+                                             _ptr(coeffs), 1 << log_size, _ptr(lde), 1 << (log_size + log_blowup),
+                                             _ptr(layers), root, _stream(stream)))
+        return root.raw
+
+    def interpolate_secure_composition(self, comp, comp_log: int, log_blowup: int, lde, stream=None) -> None:
+        """comp (4 x 2^comp_log evaluations) -> coefficients; lde (8 x 2^(comp_log-1+log_blowup)) the
+        extensions of the left then right coefficient halves."""
+        _check(_lib.stwo_b200_interpolate_secure_composition(self._h, comp_log, _ptr(comp), 1 << comp_log, log_blowup,
+                                                             _ptr(lde), 1 << (comp_log - 1 + log_blowup),
+                                                             _stream(stream)))
 
     def fold_circle_into_line(self, src, dst, src_log: int, alpha, accumulate: bool = False, stream=None) -> None:
         _check(_lib.stwo_b200_fold_circle_into_line(self._h, src_log, _ptr(src), 1 << src_log, _qm(alpha), _ptr(dst),
