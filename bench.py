@@ -414,8 +414,8 @@ def main():
         "e2e_full_trace": {"value": world * n_full / (e2e_full_ms / 1e3), "unit": "proofs/s", "proofs": n_full,
                            "h2d_bytes_per_proof": 4 * n_words,
                            "input": "every trace column from pinned host memory (host-link bound)"},
-        "roofline": {"bound": "hbm", "kernel": "circle FFT pass: interpolate + blow-up extend (k_fft_low<1>, "
-                     "k_fft_high, k_fft_low<0>)", "achieved": fft_gbs, "peak": hbm_peak, "unit": "GB/s",
+        "roofline": {"bound": "hbm", "kernel": "circle FFT pass: interpolate + blow-up extend (k_fft_low12<1>, "
+                     "k_fft_high16, k_fft_low12<0>)", "achieved": fft_gbs, "peak": hbm_peak, "unit": "GB/s",
                      "frac": fft_gbs / hbm_peak, "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)",
                      "traffic": FFT_TRAFFIC_BYTES.get((args.log_n, args.width)),
                      "algorithmic_bytes": fft_bytes, "ms": fft_ms},
