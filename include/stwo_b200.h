@@ -90,6 +90,11 @@ typedef struct {
   float host_encode;
 } stwo_b200_stage_times;
 
+/* Device pointers: Merkle layer buffers must be 16-byte aligned, FRI fold sources 8-byte aligned with
+ * an even stride, OODS coefficient columns (2^log_size >= 16) 16-byte aligned with a stride that is a
+ * multiple of 4; other pointers need the alignment of their element type. Calls that break this
+ * return STWO_B200_E_INVALID without launching anything. */
+
 /* ---- Runtime --------------------------------------------------------------------------------- */
 
 /* Creates a context on `device`: point tables and twiddle towers for domains up to 2^23

@@ -21,6 +21,12 @@ uint64_t launch_count() { return g_launches.load(std::memory_order_relaxed); }
 static_assert(sizeof(sb::StageTimes) == sizeof(stwo_b200_stage_times), "stage times layout");
 
 namespace {
+// Kernels behind the ABI read Merkle layers as 16-byte vectors, FRI fold sources as 8-byte pairs
+// and OODS coefficients as 16-byte vectors: misaligned device pointers are refused up front.
+inline bool is_aligned(const void* p, uintptr_t a) { return (reinterpret_cast<uintptr_t>(p) & (a - 1)) == 0; }
+}  // namespace
+
+namespace {
 
 thread_local std::string g_last_error;
 
@@ -214,6 +220,8 @@ int32_t stwo_b200_eval_at_point(stwo_b200_context* ctx, uint32_t log_size, uint3
   CK_CTX(ctx);
   if (log_size > 28 || (n_cols && (!coeffs || !out_dev))) return set_error(STWO_B200_E_INVALID, "bad eval_at_point arguments");
   if (n_cols == 0) return STWO_B200_OK;
+  if (!sb::eval_at_point_aligned(log_size, n_cols, coeffs, stride))
+    return set_error(STWO_B200_E_INVALID, "coefficients must be 16-byte aligned with a stride of a multiple of 4");
   size_t parts = sb::eval_at_point_partial_count(log_size, n_cols);
   void* scratch = nullptr;
   cudaError_t e = cudaMallocAsync(&scratch, parts * sizeof(sb::QM31), st(stream));
@@ -229,6 +237,7 @@ int32_t stwo_b200_merkle_commit(stwo_b200_context* ctx, uint32_t log_size, uint3
                                 uint64_t stride, uint8_t* layers_dev, uint8_t* root_host, void* stream) {
   CK_CTX(ctx);
   if (log_size > 28 || !layers_dev || (n_cols && !cols)) return set_error(STWO_B200_E_INVALID, "bad merkle arguments");
+  if (!is_aligned(layers_dev, 16)) return set_error(STWO_B200_E_INVALID, "layers_dev must be 16-byte aligned");
   if (n_cols == 0) log_size = 0;
   cudaError_t e = sb::merkle_commit(log_size, n_cols, cols, stride, layers_dev, st(stream));
   if (e != cudaSuccess) return cuda_status(e, "merkle_commit");
@@ -247,6 +256,7 @@ int32_t stwo_b200_merkle_commit_lifted(stwo_b200_context* ctx, uint32_t n_cols, 
   CK_CTX(ctx);
   if (!layers_dev || (n_cols && (!cols || !log_sizes)) || n_cols > 2048)
     return set_error(STWO_B200_E_INVALID, "bad merkle_commit_lifted arguments");
+  if (!is_aligned(layers_dev, 16)) return set_error(STWO_B200_E_INVALID, "layers_dev must be 16-byte aligned");
   uint32_t max_log = 0;
   for (uint32_t c = 0; c < n_cols; ++c) {
     if (log_sizes[c] > 28 || !cols[c]) return set_error(STWO_B200_E_INVALID, "bad lifted column");
@@ -296,6 +306,8 @@ int32_t stwo_b200_fold_circle_into_line(stwo_b200_context* ctx, uint32_t src_log
                                         uint64_t dst_stride, int32_t accumulate, void* stream) {
   CK_CTX(ctx);
   if (!domain_ok(ctx, src_log) || src_log < 2 || !src || !dst) return set_error(STWO_B200_E_INVALID, "bad fold arguments");
+  if (!is_aligned(src, 8) || (src_stride & 1))
+    return set_error(STWO_B200_E_INVALID, "fold source must be 8-byte aligned with an even stride");
   return cuda_status(sb::fold_circle_into_line(ctx->ctx.tables, src_log, src, src_stride, q(alpha), dst, dst_stride,
                                                accumulate != 0, st(stream)),
                      "fold_circle_into_line");
@@ -305,6 +317,8 @@ int32_t stwo_b200_fold_line(stwo_b200_context* ctx, uint32_t src_log, const uint
                             stwo_b200_qm31 alpha, uint32_t* dst, uint64_t dst_stride, void* stream) {
   CK_CTX(ctx);
   if (src_log < 1 || !domain_ok(ctx, src_log + 1) || !src || !dst) return set_error(STWO_B200_E_INVALID, "bad fold arguments");
+  if (!is_aligned(src, 8) || (src_stride & 1))
+    return set_error(STWO_B200_E_INVALID, "fold source must be 8-byte aligned with an even stride");
   return cuda_status(sb::fold_line(ctx->ctx.tables, src_log, src, src_stride, q(alpha), dst, dst_stride, st(stream)),
                      "fold_line");
 }
@@ -326,7 +340,7 @@ int32_t stwo_b200_fold_and_commit(stwo_b200_context* ctx, int32_t circle, uint32
   CK_CTX(ctx);
   if (src_log < 2 || !domain_ok(ctx, circle ? src_log : src_log + 1) || !src || !dst ||
       (reinterpret_cast<uintptr_t>(src) & 7) || (src_stride & 1) || src_stride < (1ull << src_log) ||
-      dst_stride < (1ull << (src_log - 1)) || (root_host && !layers_dev))
+      dst_stride < (1ull << (src_log - 1)) || (root_host && !layers_dev) || (layers_dev && !is_aligned(layers_dev, 16)))
     return set_error(STWO_B200_E_INVALID, "bad fold_and_commit arguments");
   cudaStream_t s = st(stream);
   void* a_dev = nullptr;
@@ -349,7 +363,7 @@ int32_t stwo_b200_commit_columns(stwo_b200_context* ctx, uint32_t log_size, uint
                                  void* stream) {
   CK_CTX(ctx);
   if (!domain_ok(ctx, log_size + log_blowup) || log_blowup == 0 || log_blowup > 4 || n_cols == 0 || !evals ||
-      !coeffs || !lde || !layers_dev)
+      !coeffs || !lde || !layers_dev || !is_aligned(layers_dev, 16))
     return set_error(STWO_B200_E_INVALID, "bad commit_columns arguments");
   cudaStream_t s = st(stream);
   cudaError_t e = sb::interpolate_extend(ctx->ctx.tables, log_size, log_blowup, n_cols, evals, evals_stride, coeffs,

@@ -82,6 +82,12 @@ cudaError_t wide_fib_composition(uint32_t log_n, uint32_t W, const uint32_t* eva
 cudaError_t eval_at_point(const DeviceTables& t, uint32_t log_size, uint32_t n_cols, const uint32_t* coeffs,
                           uint64_t stride, PointQ p, QM31* factors_dev, QM31* partial, QM31* out,
                           cudaStream_t stream);
+// Whether eval_at_point may run on these columns: with 2^log_size >= 16 each thread reads 16
+// coefficients as 16-byte vectors, so the base must be 16-byte aligned and the stride a multiple of 4.
+inline bool eval_at_point_aligned(uint32_t log_size, uint32_t n_cols, const uint32_t* coeffs, uint64_t stride) {
+  if (log_size < 4) return true;
+  return (reinterpret_cast<uintptr_t>(coeffs) & 15) == 0 && (n_cols <= 1 || stride % 4 == 0);
+}
 size_t eval_at_point_partial_count(uint32_t log_size, uint32_t n_cols);
 
 // ---- DEEP quotients (src/core/pcs/quotients/row_evaluation.zig) -----------

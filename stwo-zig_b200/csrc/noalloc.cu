@@ -66,6 +66,9 @@ int32_t stwo_b200_eval_at_point_noalloc(stwo_b200_context* ctx, uint32_t log_siz
   if (log_size > 28 || (n_cols && (!coeffs || !out_dev)))
     return sb::set_last_error(STWO_B200_E_INVALID, "bad eval_at_point_noalloc arguments");
   if (n_cols == 0) return STWO_B200_OK;
+  if (!sb::eval_at_point_aligned(log_size, n_cols, coeffs, stride))
+    return sb::set_last_error(STWO_B200_E_INVALID,
+                              "coefficients must be 16-byte aligned with a stride of a multiple of 4");
   const size_t parts = sb::eval_at_point_partial_count(log_size, n_cols);
   if (parts > kScratch)
     return sb::set_last_error(STWO_B200_E_INVALID, "eval_at_point_noalloc: n_cols * max(1, 2^(log_size-12)) = " +

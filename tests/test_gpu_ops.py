@@ -176,3 +176,31 @@ def test_lifted_merkle_equals_uniform_commit(ctx):
     rb = ctx.merkle_commit_lifted([dev[i << 12:(i + 1) << 12] for i in range(7)], layers_b)
     assert ra == rb
     assert torch.equal(layers_a, layers_b)
+
+
+def test_misaligned_pointers_are_refused(ctx):
+    """The ABI refuses device pointers its kernels cannot read as vectors (Merkle layers: 16 bytes;
+    FRI fold sources: 8 bytes and an even stride; OODS coefficients: 16 bytes) before any launch."""
+    import stwo_b200 as sb
+    import torch
+    buf = torch.zeros(1 << 14, dtype=torch.int32, device="cuda")
+    off = buf[1:]                                   # 4 bytes past an aligned base
+    dst = torch.zeros(1 << 12, dtype=torch.int32, device="cuda")
+    layers = torch.zeros(((2 << 10) - 1) * 32 + 64, dtype=torch.uint8, device="cuda")
+    layers_off = layers[4:]
+    alpha = [3, 0, 0, 0]
+    calls = [
+        lambda: ctx.merkle_commit(buf, 8, 4, layers_off),
+        lambda: ctx.merkle_commit_lifted([buf[:256], buf[256:384]], layers_off),
+        lambda: ctx.fold_circle_into_line(off, dst, 8, alpha),
+        lambda: ctx.fold_line(off, dst, 8, alpha),
+        lambda: ctx.fold_and_commit(buf, dst, 8, alpha, layers=layers_off),
+        lambda: ctx.eval_at_point(off, 10, 2, 1 << 10, [1, 0, 0, 0], [2, 0, 0, 0], dst),
+        lambda: ctx.eval_at_point_noalloc(off, 10, 2, 1 << 10, [1, 0, 0, 0], [2, 0, 0, 0], dst),
+    ]
+    for i, call in enumerate(calls):
+        with pytest.raises(sb.StwoError) as e:
+            call()
+        assert e.value.status == sb.E_INVALID, i
+    torch.cuda.synchronize()
+    ctx.merkle_commit(buf, 8, 4, layers)  # the same call with aligned pointers still runs
