@@ -192,3 +192,17 @@ def test_protocol_variants_match_oracle(ctx, log_n, W, over):
                                    trace_seed=31 * log_n + W, channel_seed=0)
     assert got == ref
     assert sb.verify_wide_fibonacci(got, log_n, W, channel_seed=0)
+
+
+def test_widest_statement_matches_oracle(ctx):
+    """sequence_len 1000, the widest statement the prover takes (1008 quotient columns against the
+    quotient kernel's 1024 entries); one column more is refused."""
+    import stwo_b200 as sb
+    o, g = cfg_pair("functional")
+    ref = oracle.prove_wide_fib(6, 1000, o, trace_kind=1, trace_seed=1000)
+    got = ctx.prove_wide_fibonacci(sb.Statement(6, 1000), g, trace_kind=sb.TRACE_SEEDED, trace_seed=1000)
+    assert got == ref
+    assert sb.verify_wide_fibonacci(got, 6, 1000)
+    with pytest.raises(sb.StwoError) as e:
+        ctx.prove_wide_fibonacci(sb.Statement(6, 1001), g, trace_kind=sb.TRACE_SEEDED, trace_seed=1)
+    assert e.value.status == sb.E_INVALID
