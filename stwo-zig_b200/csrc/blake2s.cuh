@@ -66,6 +66,21 @@ SB_HD uint32_t b2s_fadd(uint32_t a, uint32_t b, uint32_t one) {
     SB_B2S_G(v3, v4, v9, v14, m[s14], m[s15]);                                             \
   } while (0)
 
+// Rounds 2..10 on the working state v0..v15 and message m (the proof-of-work
+// grind runs the first round itself, most of it precomputed per prefix).
+#define SB_B2S_ROUNDS_2_TO_10()                                            \
+  do {                                                                     \
+    SB_B2S_ROUND(14, 10, 4, 8, 9, 15, 13, 6, 1, 12, 0, 2, 11, 7, 5, 3);    \
+    SB_B2S_ROUND(11, 8, 12, 0, 5, 2, 15, 13, 10, 14, 3, 6, 7, 1, 9, 4);    \
+    SB_B2S_ROUND(7, 9, 3, 1, 13, 12, 11, 14, 2, 6, 5, 10, 4, 0, 15, 8);    \
+    SB_B2S_ROUND(9, 0, 5, 7, 2, 4, 10, 15, 14, 1, 11, 12, 6, 8, 3, 13);    \
+    SB_B2S_ROUND(2, 12, 6, 10, 0, 11, 8, 3, 4, 13, 7, 5, 15, 14, 1, 9);    \
+    SB_B2S_ROUND(12, 5, 1, 15, 14, 13, 4, 10, 0, 7, 6, 3, 9, 2, 8, 11);    \
+    SB_B2S_ROUND(13, 11, 7, 14, 12, 1, 3, 9, 5, 0, 15, 4, 8, 6, 2, 10);    \
+    SB_B2S_ROUND(6, 15, 14, 9, 11, 3, 0, 8, 12, 2, 13, 7, 1, 4, 10, 5);    \
+    SB_B2S_ROUND(10, 2, 8, 4, 7, 6, 1, 5, 15, 11, 9, 14, 3, 12, 13, 0);    \
+  } while (0)
+
 // h <- compress(h, m, t, last). All indices are compile-time constants so the
 // message and state stay in registers.
 SB_HD void b2s_compress(uint32_t h[8], const uint32_t m[16], uint32_t t_lo, bool last, uint32_t one = 1) {
@@ -73,15 +88,7 @@ SB_HD void b2s_compress(uint32_t h[8], const uint32_t m[16], uint32_t t_lo, bool
   uint32_t v8 = B2sIv::v0, v9 = B2sIv::v1, v10 = B2sIv::v2, v11 = B2sIv::v3;
   uint32_t v12 = B2sIv::v4 ^ t_lo, v13 = B2sIv::v5, v14 = last ? ~B2sIv::v6 : B2sIv::v6, v15 = B2sIv::v7;
   SB_B2S_ROUND(0, 1, 2, 3, 4, 5, 6, 7, 8, 9, 10, 11, 12, 13, 14, 15);
-  SB_B2S_ROUND(14, 10, 4, 8, 9, 15, 13, 6, 1, 12, 0, 2, 11, 7, 5, 3);
-  SB_B2S_ROUND(11, 8, 12, 0, 5, 2, 15, 13, 10, 14, 3, 6, 7, 1, 9, 4);
-  SB_B2S_ROUND(7, 9, 3, 1, 13, 12, 11, 14, 2, 6, 5, 10, 4, 0, 15, 8);
-  SB_B2S_ROUND(9, 0, 5, 7, 2, 4, 10, 15, 14, 1, 11, 12, 6, 8, 3, 13);
-  SB_B2S_ROUND(2, 12, 6, 10, 0, 11, 8, 3, 4, 13, 7, 5, 15, 14, 1, 9);
-  SB_B2S_ROUND(12, 5, 1, 15, 14, 13, 4, 10, 0, 7, 6, 3, 9, 2, 8, 11);
-  SB_B2S_ROUND(13, 11, 7, 14, 12, 1, 3, 9, 5, 0, 15, 4, 8, 6, 2, 10);
-  SB_B2S_ROUND(6, 15, 14, 9, 11, 3, 0, 8, 12, 2, 13, 7, 1, 4, 10, 5);
-  SB_B2S_ROUND(10, 2, 8, 4, 7, 6, 1, 5, 15, 11, 9, 14, 3, 12, 13, 0);
+  SB_B2S_ROUNDS_2_TO_10();
   h[0] ^= v0 ^ v8; h[1] ^= v1 ^ v9; h[2] ^= v2 ^ v10; h[3] ^= v3 ^ v11;
   h[4] ^= v4 ^ v12; h[5] ^= v5 ^ v13; h[6] ^= v6 ^ v14; h[7] ^= v7 ^ v15;
 }

@@ -495,33 +495,69 @@ __device__ __forceinline__ uint32_t ctz128(uint32_t a, uint32_t b, uint32_t c, u
   return 128;
 }
 
-struct PowPrefix { uint32_t w[8]; };
+// The grind hashes prefix (32 bytes) || nonce (8 bytes) as one final block. Of
+// the first round's eight G steps only G(v0, v5, v10, v15, m8, m9) reads the
+// nonce; the other seven touch other state words and constant message words,
+// so they run once per prefix on the host. `v` is the working state after those
+// seven (v0, v5, v10, v15 as the column step left them).
+struct PowPrefix { uint32_t w[8]; uint32_t v[16]; };
+
+PowPrefix pow_prefix(const uint32_t words[8]) {
+  PowPrefix p;
+  const uint32_t one = 1;  // the additions' multiplier when this body is parsed for the device
+  (void)one;
+  uint32_t h[8], m[16] = {};
+  b2s_init(h);
+  for (int i = 0; i < 8; ++i) p.w[i] = m[i] = words[i];
+  uint32_t v0 = h[0], v1 = h[1], v2 = h[2], v3 = h[3], v4 = h[4], v5 = h[5], v6 = h[6], v7 = h[7];
+  uint32_t v8 = B2sIv::v0, v9 = B2sIv::v1, v10 = B2sIv::v2, v11 = B2sIv::v3;
+  uint32_t v12 = B2sIv::v4 ^ 40u, v13 = B2sIv::v5, v14 = ~B2sIv::v6, v15 = B2sIv::v7;
+  SB_B2S_G(v0, v4, v8, v12, m[0], m[1]);
+  SB_B2S_G(v1, v5, v9, v13, m[2], m[3]);
+  SB_B2S_G(v2, v6, v10, v14, m[4], m[5]);
+  SB_B2S_G(v3, v7, v11, v15, m[6], m[7]);
+  SB_B2S_G(v1, v6, v11, v12, m[10], m[11]);
+  SB_B2S_G(v2, v7, v8, v13, m[12], m[13]);
+  SB_B2S_G(v3, v4, v9, v14, m[14], m[15]);
+  const uint32_t v[16] = {v0, v1, v2, v3, v4, v5, v6, v7, v8, v9, v10, v11, v12, v13, v14, v15};
+  for (int i = 0; i < 16; ++i) p.v[i] = v[i];
+  return p;
+}
 
 // One bounded round of the search: nonces [base, base + grid*256*per_thread).
 // Rounds are enqueued in nonce order on one stream; a round starts by leaving
 // at once when an earlier round already found a smaller nonce, and each thread
 // stops at its first valid nonce or once the best known nonce is below its own.
+// CTA b owns the contiguous nonces [base + b*256*per_thread, +256*per_thread)
+// and CTAs are dispatched in index order, so the round runs in nonce order: once
+// the lowest valid nonce is found, only the CTAs in flight around it still work
+// (spreading each CTA's nonces over the whole round left about a quarter of a
+// round of work above the hit).
 // LOW32: for n_bits <= 32 the condition is that the low n_bits of the first hash
 // word are zero, so only that word is live and the compiler drops the last
 // round's work that only feeds the other words.
 template <bool LOW32>
 __global__ void __launch_bounds__(256) k_pow_round(PowPrefix pre, uint32_t n_bits, uint64_t base,
                                                    uint32_t per_thread, unsigned long long* found, uint32_t one) {
-  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
-  uint64_t nonce = base + (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const uint32_t stride = blockDim.x;
+  uint64_t nonce = base + (uint64_t)blockIdx.x * blockDim.x * per_thread + threadIdx.x;
   const uint32_t mask = n_bits >= 32 ? 0xffffffffu : (1u << n_bits) - 1u;
   unsigned long long best = *((volatile unsigned long long*)found);
   for (uint32_t k = 0; k < per_thread && nonce < best; ++k, nonce += stride) {
-    uint32_t h[8];
-    b2s_init(h);
     uint32_t m[16];
 #pragma unroll
     for (int i = 0; i < 8; ++i) m[i] = pre.w[i];
     m[8] = (uint32_t)nonce; m[9] = (uint32_t)(nonce >> 32);
 #pragma unroll
     for (int i = 10; i < 16; ++i) m[i] = 0;
-    b2s_compress(h, m, 40, true, one);
-    const bool ok = LOW32 ? (h[0] & mask) == 0 : ctz128(h[0], h[1], h[2], h[3]) >= n_bits;
+    uint32_t v0 = pre.v[0], v1 = pre.v[1], v2 = pre.v[2], v3 = pre.v[3], v4 = pre.v[4], v5 = pre.v[5],
+             v6 = pre.v[6], v7 = pre.v[7], v8 = pre.v[8], v9 = pre.v[9], v10 = pre.v[10], v11 = pre.v[11],
+             v12 = pre.v[12], v13 = pre.v[13], v14 = pre.v[14], v15 = pre.v[15];
+    SB_B2S_G(v0, v5, v10, v15, m[8], m[9]);
+    SB_B2S_ROUNDS_2_TO_10();
+    const uint32_t h0 = (B2sIv::v0 ^ 0x01010020u) ^ v0 ^ v8;
+    const bool ok = LOW32 ? (h0 & mask) == 0
+                          : ctz128(h0, B2sIv::v1 ^ v1 ^ v9, B2sIv::v2 ^ v2 ^ v10, B2sIv::v3 ^ v3 ^ v11) >= n_bits;
     if (ok) {
       atomicMin(found, (unsigned long long)nonce);
       return;
@@ -536,8 +572,7 @@ uint64_t pow_round_nonces(int sm_count) { return (uint64_t)sm_count * 4 * 256 * 
 
 cudaError_t pow_round(const uint32_t prefix_words[8], uint32_t n_bits, uint64_t base, uint32_t* result_dev,
                       int sm_count, cudaStream_t stream) {
-  PowPrefix pre;
-  for (int i = 0; i < 8; ++i) pre.w[i] = prefix_words[i];
+  const PowPrefix pre = pow_prefix(prefix_words);
   // Eight waves of short CTAs (14 nonces per thread, ~0.1 ms each) rather than one
   // wave of long ones, so that other streams' work gets SMs between them.
   auto* res = reinterpret_cast<unsigned long long*>(result_dev);
