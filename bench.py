@@ -693,9 +693,9 @@ def run_serve(args, ctx):
 # capture of 2^20 rows x 40 columns (dram__bytes_read.sum + dram__bytes_write.sum = 1531.5 MB),
 # scaled to 100 columns; traffic is linear in the column count.
 FFT_TRAFFIC_BYTES: dict = {(20, 100): 1532.8e6 * 100 / 40}
-# Thread instructions per nonce of the grind (one ncu capture of a 26-bit round:
-# 550.2 M warp instructions x 32 / 16,973,824 nonces).
-POW_INSTR_PER_NONCE = 1037
+# Thread instructions per nonce of the grind (one ncu capture of a full 26-bit round:
+# 532.2 M warp instructions x 32 / 16,973,824 nonces).
+POW_INSTR_PER_NONCE = 1003
 # Warp instructions of one interpolate + blow-up extend of a 2^20 column (ncu smsp__inst_executed.sum
 # of k_fft_low12<1> + k_fft_high16 + k_fft_low12<0>: 557,465,600 for 40 columns).
 FFT_WARP_INSTR_PER_COL_2P20 = 557_465_600 // 40

@@ -573,8 +573,9 @@ uint64_t pow_round_nonces(int sm_count) { return (uint64_t)sm_count * 4 * 256 * 
 cudaError_t pow_round(const uint32_t prefix_words[8], uint32_t n_bits, uint64_t base, uint32_t* result_dev,
                       int sm_count, cudaStream_t stream) {
   const PowPrefix pre = pow_prefix(prefix_words);
-  // Eight waves of short CTAs (14 nonces per thread, ~0.1 ms each) rather than one
-  // wave of long ones, so that other streams' work gets SMs between them.
+  // Four waves of short CTAs (32 registers: eight 256-thread CTAs resident per SM;
+  // 14 nonces per thread, ~0.15 ms a wave) rather than one wave of long ones, so
+  // that other streams' work gets SMs between them.
   auto* res = reinterpret_cast<unsigned long long*>(result_dev);
   if (n_bits <= 32)
     k_pow_round<true><<<sm_count * 4 * 8, 256, 0, stream>>>(pre, n_bits, base, 14, res, 1u);
