@@ -132,6 +132,19 @@ def test_pow_grind(ctx, bits):
     assert ctx.pow_grind(prefix, bits) == oracle.pow_grind(digest, bits, 8)
 
 
+def test_pow_grind_lowest_nonce_across_waves_and_rounds(ctx):
+    """24-bit grinds: the lowest valid nonces fall in later CTA waves and later bounded rounds
+    (a round is 16.97 M nonces on 148 SMs); the device must still return the lowest one."""
+    found = []
+    for i in range(6):
+        digest = bytes((i * 29 + k * 11) & 0xFF for k in range(32))
+        prefix = oracle.blake2s(struct.pack("<I", 0x12345678) + b"\0" * 12 + digest + struct.pack("<I", 24))
+        got = ctx.pow_grind(prefix, 24)
+        assert got == oracle.pow_grind(digest, 24), i
+        found.append(got)
+    assert max(found) > 4_300_000  # at least one beyond the first wave of CTAs
+
+
 def test_bad_arguments_raise(ctx):
     import stwo_b200
     import torch
