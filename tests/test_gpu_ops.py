@@ -102,11 +102,12 @@ def test_fold_line(ctx, log):
     assert np.array_equal(host(dst).reshape(4, -1), oracle.fold_line(src, alpha, log))
 
 
-@pytest.mark.parametrize("log", [0, 1, 3, 12, 13, 20])
-def test_eval_at_point(ctx, log):
+@pytest.mark.parametrize("log,n_cols", [(0, 5), (1, 5), (3, 5), (12, 5), (13, 5), (20, 5), (22, 1), (16, 64)])
+def test_eval_at_point(ctx, log, n_cols):
+    """Chunk partials per column: 1 (small columns), 237 (5 columns of 2^20), 1024 (one column of
+    2^22, the most), 16 (64 columns of 2^16): the warp-per-column partial sum at every shape."""
     import torch
-    rng = np.random.default_rng(log + 9)
-    n_cols = 5
+    rng = np.random.default_rng(log + 9 + 100 * n_cols)
     cols = rand_cols(rng, n_cols, log)
     px = rng.integers(0, P, size=4, dtype=np.uint32)
     py = rng.integers(0, P, size=4, dtype=np.uint32)
