@@ -206,3 +206,15 @@ def test_widest_statement_matches_oracle(ctx):
     with pytest.raises(sb.StwoError) as e:
         ctx.prove_wide_fibonacci(sb.Statement(6, 1001), g, trace_kind=sb.TRACE_SEEDED, trace_seed=1)
     assert e.value.status == sb.E_INVALID
+
+
+def test_largest_domain_matches_oracle(ctx):
+    """log_n_rows 22, the largest the prover takes (LDE of 2^23 rows); 23 is refused."""
+    import stwo_b200 as sb
+    o, g = cfg_pair("functional")
+    ref = oracle.prove_wide_fib(22, 16, o, trace_kind=1, trace_seed=22)
+    got = ctx.prove_wide_fibonacci(sb.Statement(22, 16), g, trace_kind=sb.TRACE_SEEDED, trace_seed=22)
+    assert got == ref
+    with pytest.raises(sb.StwoError) as e:
+        ctx.prove_wide_fibonacci(sb.Statement(23, 16), g, trace_kind=sb.TRACE_SEEDED, trace_seed=1)
+    assert e.value.status == sb.E_INVALID
