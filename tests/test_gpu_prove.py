@@ -218,3 +218,16 @@ def test_largest_domain_matches_oracle(ctx):
     with pytest.raises(sb.StwoError) as e:
         ctx.prove_wide_fibonacci(sb.Statement(23, 16), g, trace_kind=sb.TRACE_SEEDED, trace_seed=1)
     assert e.value.status == sb.E_INVALID
+
+
+def test_headline_shape_secure_matches_oracle_and_verifies(ctx):
+    """The benchmark's statement, 2^20 x 100 under the secure preset (PoW 26 bits, 70 queries),
+    byte-for-byte against the oracle, then through the Python and the library verifiers."""
+    import stwo_b200 as sb
+    o, g = cfg_pair("secure")
+    ref = oracle.prove_wide_fib(20, 100, o, trace_kind=1, trace_seed=2020, channel_seed=7)
+    got = ctx.prove_wide_fibonacci(sb.Statement(20, 100), g, trace_kind=sb.TRACE_SEEDED, trace_seed=2020,
+                                   channel_seed=7)
+    assert got == ref
+    assert verifier.verify_wide_fib(got, 20, 100, channel_seed=7)
+    assert sb.verify_wide_fibonacci(got, 20, 100, channel_seed=7)
