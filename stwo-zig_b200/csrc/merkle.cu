@@ -8,8 +8,10 @@
 //
 // One thread per leaf: a warp reads 32 consecutive rows of a column as one
 // 128-byte transaction; the message schedule and state stay in registers.
-// Each CTA hashes 256 leaves and then folds them to its subtree root in shared
-// memory (8 node levels), writing every level; the upper levels are folded by
+// Each CTA hashes 256 leaves and then folds the three node levels whose parents
+// fill whole warps (128, 64, 32) in shared memory, writing every level; a tree
+// that fits one CTA is folded to its root there. The larger layers above are
+// folded by k_merkle_layer (one parent per thread), the top 2^12 children by
 // k_merkle_nodes, up to 9 levels per launch.
 #include "blake2s.cuh"
 #include "kernels.cuh"
@@ -20,6 +22,7 @@ namespace {
 
 constexpr uint32_t LEAF_THREADS = 256;  // leaves per CTA
 constexpr uint32_t LEAF_LEVELS = 8;     // node levels folded inside a leaf CTA
+constexpr uint32_t FULL_WARP_LEVELS = 3;  // levels whose parents fill whole warps (128, 64, 32)
 constexpr uint32_t NODE_THREADS = 256;  // parents per CTA at the first level
 constexpr uint32_t NODE_FOLD_LOG = 12;  // layers up to 2^12 nodes fold inside CTAs
 
@@ -427,9 +430,9 @@ cudaError_t fri_fold_commit(const DeviceTables& t, bool circle, uint32_t src_log
   const uint32_t dst_log = src_log - 1;
   const uint64_t n = 1ull << dst_log;
   const uint32_t grid = (uint32_t)((n + LEAF_THREADS - 1) / LEAF_THREADS);
-  // One compression per leaf: the CTA also folds 8 node levels (node work equals
-  // leaf work here, and it saves the launches of the large layers).
-  const uint32_t levels = layers ? (dst_log < LEAF_LEVELS ? dst_log : LEAF_LEVELS) : 0;
+  // One compression per leaf; the CTA also folds the three full-warp node levels
+  // (the whole tree when it fits one CTA).
+  const uint32_t levels = layers ? (dst_log <= LEAF_LEVELS ? dst_log : FULL_WARP_LEVELS) : 0;
   if (circle)
     k_fri_fold_commit<true><<<grid, LEAF_THREADS, 0, stream>>>(t.view(src_log, true), dst_log, src, src_stride, alpha,
                                                                dst, dst_stride, layers, seeds, levels, 1u);
@@ -450,10 +453,11 @@ cudaError_t merkle_commit(uint32_t log_size, uint32_t n_cols, const uint32_t* co
     return cudaGetLastError();
   }
   const uint64_t n_rows = 1ull << log_size;
-  // A tree that fits one CTA is folded to its root in the leaf launch. Trees of
-  // 4-word leaves (FRI-style, one compression each) also fold 8 levels per CTA;
-  // wider leaves keep the leaf CTAs short and fold layer by layer.
-  uint32_t leaf_levels = log_size <= LEAF_LEVELS ? log_size : (n_cols <= 4 ? LEAF_LEVELS : 0);
+  // A tree that fits one CTA is folded to its root in the leaf launch; larger ones
+  // fold their three full-warp node levels there. Levels 4-8 inside the CTA would
+  // run on partly empty warps (16, 8, .. 1 parents): for 2^21 leaves of 4 words,
+  // folding 8 levels took 283 us, 3 levels 245 us and none 254 us.
+  uint32_t leaf_levels = log_size <= LEAF_LEVELS ? log_size : FULL_WARP_LEVELS;
   uint32_t grid = (uint32_t)((n_rows + LEAF_THREADS - 1) / LEAF_THREADS);
   k_merkle_leaves<<<grid, LEAF_THREADS, 0, stream>>>(log_size, n_cols, cols, stride, layers, seeds, leaf_levels, 1u); note_launch();
   cudaError_t e = cudaGetLastError();
