@@ -10,9 +10,9 @@
 // 128-byte transaction; the message schedule and state stay in registers.
 // Each CTA hashes 256 leaves and then folds the three node levels whose parents
 // fill whole warps (128, 64, 32) in shared memory, writing every level; a tree
-// that fits one CTA is folded to its root there. The larger layers above are
-// folded by k_merkle_layer (one parent per thread), the top 2^12 children by
-// k_merkle_nodes, up to 9 levels per launch.
+// that fits one CTA is folded to its root there. The layers above are folded by
+// k_merkle_nodes: four levels per launch while there are more than 2^12
+// children, then up to 9 levels per launch.
 #include "blake2s.cuh"
 #include "kernels.cuh"
 
@@ -188,20 +188,6 @@ __global__ void __launch_bounds__(NODE_THREADS) k_merkle_nodes(uint8_t* layers, 
   fold_levels(sm, per_cta, levels, layers, max_log, child_log, first, seeds.node, one);
 }
 
-// One parent layer, one thread per parent (used while layers are large, so every
-// compression has a thread of its own).
-__global__ void __launch_bounds__(256) k_merkle_layer(uint8_t* layers, uint32_t max_log, uint32_t parent_log,
-                                                     Seeds seeds, uint32_t one) {
-  const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= (1ull << parent_log)) return;
-  const uint4* c = reinterpret_cast<const uint4*>(layers + (merkle_layer_offset(max_log, parent_log + 1) + 2 * i) * 32);
-  uint4 a = c[0], b = c[1], d = c[2], e = c[3];
-  uint32_t l[8] = {a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w}, r[8] = {d.x, d.y, d.z, d.w, e.x, e.y, e.z, e.w};
-  uint32_t h[8];
-  node_hash(seeds.node, l, r, h, one);
-  store_hash(layers, merkle_layer_offset(max_log, parent_log) + i, h);
-}
-
 // FRI fold fused with the next layer's commitment (src/core/fri/folding.zig:352-384,
 // 558-602; src/prover/fri.zig:377-592): thread i folds pair (2i, 2i+1) of the source
 // into line value i, stores its 4 coordinates and, when `layers` is set, hashes it
@@ -366,13 +352,15 @@ static const Seeds& seeds_once() {
 static cudaError_t merkle_finish(uint8_t* layers, uint32_t max_log, uint32_t child_log, cudaStream_t stream) {
   const Seeds& seeds = seeds_once();
   cudaError_t e = cudaSuccess;
+  // Large layers: four levels per launch, each CTA folding 512 children (every level's
+  // parents fill whole warps: 256, 128, 64, 32).
   while (child_log > NODE_FOLD_LOG) {
-    uint32_t parent_log = child_log - 1;
-    uint32_t blocks = (uint32_t)(((1ull << parent_log) + 255) / 256);
-    k_merkle_layer<<<blocks, 256, 0, stream>>>(layers, max_log, parent_log, seeds, 1u); note_launch();
+    uint32_t levels = child_log - NODE_FOLD_LOG < 4 ? child_log - NODE_FOLD_LOG : 4;
+    uint32_t blocks = (uint32_t)((1ull << child_log) / (2 * NODE_THREADS));
+    k_merkle_nodes<<<blocks, NODE_THREADS, 0, stream>>>(layers, max_log, child_log, levels, seeds, 1u); note_launch();
     e = cudaGetLastError();
     if (e != cudaSuccess) return e;
-    child_log = parent_log;
+    child_log -= levels;
   }
   while (child_log > 0) {
     uint32_t levels = child_log < 9 ? child_log : 9;
