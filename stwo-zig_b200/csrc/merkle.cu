@@ -462,7 +462,7 @@ cudaError_t merkle_commit_lifted(uint32_t max_log, uint32_t n_cols, const uint32
   }
   if (n_cols > LIFTED_MAX_COLS) return cudaErrorInvalidValue;
   const uint64_t n_rows = 1ull << max_log;
-  uint32_t leaf_levels = max_log <= LEAF_LEVELS ? max_log : (n_cols <= 4 ? LEAF_LEVELS : 0);
+  uint32_t leaf_levels = max_log <= LEAF_LEVELS ? max_log : FULL_WARP_LEVELS;
   uint32_t grid = (uint32_t)((n_rows + LEAF_THREADS - 1) / LEAF_THREADS);
   k_merkle_leaves_lifted<<<grid, LEAF_THREADS, 0, stream>>>(max_log, n_cols, col_ptrs, col_logs, layers, seeds,
                                                             leaf_levels, 1u); note_launch();
@@ -473,9 +473,9 @@ cudaError_t merkle_commit_lifted(uint32_t max_log, uint32_t n_cols, const uint32
 
 // ---------------------------------------------------------------------------
 // Proof of work: lowest nonce with ctz(Blake2s(prefix_digest || LE64 nonce)[0..16]) >= n_bits.
-// Thread k tests nonces k, k + stride, ... and stops once its next nonce is not
-// below the best found so far, so every nonce below the result is tested and
-// the result does not depend on scheduling (src/core/channel/blake2s.zig:168-240).
+// Each thread tests its nonces in increasing order and stops once its next nonce
+// is not below the best found so far, so every nonce below the result is tested
+// and the result does not depend on scheduling (src/core/channel/blake2s.zig:168-240).
 // ---------------------------------------------------------------------------
 namespace {
 
