@@ -217,6 +217,12 @@ int32_t stwo_b200_server_wait(stwo_b200_server* server, uint64_t ticket, uint8_t
 int32_t stwo_b200_server_warmup(stwo_b200_server* server, uint32_t max_log_n_rows, uint32_t max_sequence_len,
                                 uint32_t log_blowup, uint32_t max_xor_log_n);
 int32_t stwo_b200_server_snapshot_get(stwo_b200_server* server, stwo_b200_server_snapshot* out);
+/* Time limit of every request submitted from now on, counted from its submission (0: none, the
+ * default). A request still queued at its deadline ends with STWO_B200_E_TIMEOUT without running; a
+ * running proof checks it between stages and between proof-of-work rounds and ends with
+ * STWO_B200_E_TIMEOUT, its slot free for the next request. The reference has no serving loop; its
+ * provers run to completion. */
+int32_t stwo_b200_server_set_request_timeout(stwo_b200_server* server, uint32_t timeout_ms);
 /* Finishes every queued and running request, then releases the slots. */
 int32_t stwo_b200_server_destroy(stwo_b200_server* server);
 
@@ -247,7 +253,9 @@ int32_t stwo_b200_extend_columns(stwo_b200_context* ctx, uint32_t log_size, uint
 /* Value of each coefficient column at a QM31 circle point (CircleCoefficients.evalAtPoint,
  * src/prover/poly/circle/poly.zig:62-230; evaluateCoefficientPlans hook,
  * src/prover/pcs/sampled_values.zig:68; eval_at_point / batch_eval_at_points, ffi.zig:55,:89).
- * out_dev: n_cols QM31 on the device. Allocates its scratch from the stream's pool. */
+ * out_dev: n_cols QM31 on the device, n_cols <= STWO_B200_EVAL_AT_POINT_MAX_COLS. Allocates its
+ * scratch from the stream's pool (STWO_B200_E_OOM when that fails). */
+#define STWO_B200_EVAL_AT_POINT_MAX_COLS 65535
 int32_t stwo_b200_eval_at_point(stwo_b200_context* ctx, uint32_t log_size, uint32_t n_cols, const uint32_t* coeffs,
                                 uint64_t stride, stwo_b200_qm31 px, stwo_b200_qm31 py, stwo_b200_qm31* out_dev,
                                 void* stream);
@@ -258,9 +266,10 @@ int32_t stwo_b200_eval_at_point(stwo_b200_context* ctx, uint32_t log_size, uint3
  * owns all device memory, or code where CUDA allocation calls are not allowed. The per-chunk partial
  * sums live in one fixed device array of STWO_B200_NOALLOC_EVAL_SCRATCH 16-byte entries (1 MiB, kept
  * on every GPU that loads the library until exit): n_cols * max(1, 2^(log_size-12)) must not exceed
- * it, else STWO_B200_E_INVALID. All calls on a device share the array, so calls whose work overlaps
- * on the GPU race: serialize them. The first call on each device looks up the array's address; make
- * it before any stream capture. */
+ * it, and n_cols must not exceed STWO_B200_EVAL_AT_POINT_MAX_COLS, else STWO_B200_E_INVALID. All
+ * calls on a device share the array, so calls whose work overlaps on the GPU race: serialize them.
+ * The first call on each device looks up the array's address; make it before any stream capture.
+ * The address is cached for the process: do not call this again after resetting the device. */
 #define STWO_B200_NOALLOC_EVAL_SCRATCH 65536
 int32_t stwo_b200_eval_at_point_noalloc(stwo_b200_context* ctx, uint32_t log_size, uint32_t n_cols,
                                         const uint32_t* coeffs, uint64_t stride, stwo_b200_qm31 px,
@@ -421,9 +430,20 @@ int32_t stwo_b200_xor_lookup_trace(stwo_b200_context* ctx, uint32_t log_n, uint6
 /* ---- Channel proof of work ---------------------------------------------------------------------- */
 
 /* Lowest nonce whose Blake2s(prefix_digest || LE64 nonce) has >= n_bits trailing zero bits in its
- * first 16 bytes (src/core/channel/blake2s.zig:135-240). Synchronous. */
+ * first 16 bytes (src/core/channel/blake2s.zig:135-240). Synchronous. n_bits <= STWO_B200_MAX_POW_BITS,
+ * the limit every prover applies to pow_bits too (the reference accepts any u32; a search of 2^n_bits
+ * expected nonces holds the device for that long, about 40 s at 40 bits on one B200). */
+#define STWO_B200_MAX_POW_BITS 40
 int32_t stwo_b200_pow_grind(stwo_b200_context* ctx, const uint8_t prefix_digest[32], uint32_t n_bits,
                             uint64_t* nonce_out);
+
+/* ---- Testing ------------------------------------------------------------------------------------- */
+
+/* Makes the nth device or pinned-host allocation of the library from now on fail as if out of memory
+ * (0 disarms): the failure paths return STWO_B200_E_OOM, free what the call had taken and leave the
+ * context usable. Host-side injection only, as the reference's armed failures
+ * (armOwnershipTransferFailureForTesting, src/backends/metal/commit_backend.zig:69-71). */
+int32_t stwo_b200_arm_allocation_failure_for_testing(uint32_t nth);
 
 #ifdef __cplusplus
 }

@@ -7,6 +7,7 @@
 #include <vector>
 
 #include "../../include/stwo_b200.h"
+#include "alloc.hpp"
 #include "context.hpp"
 #include "prover.hpp"
 #include "server.hpp"
@@ -218,14 +219,18 @@ int32_t stwo_b200_eval_at_point(stwo_b200_context* ctx, uint32_t log_size, uint3
                                 uint64_t stride, stwo_b200_qm31 px, stwo_b200_qm31 py, stwo_b200_qm31* out_dev,
                                 void* stream) {
   CK_CTX(ctx);
-  if (log_size > 28 || (n_cols && (!coeffs || !out_dev))) return set_error(STWO_B200_E_INVALID, "bad eval_at_point arguments");
+  if (log_size > 28 || n_cols > sb::EVAL_AT_POINT_MAX_COLS || (n_cols && (!coeffs || !out_dev)))
+    return set_error(STWO_B200_E_INVALID, "bad eval_at_point arguments");
   if (n_cols == 0) return STWO_B200_OK;
   if (!sb::eval_at_point_aligned(log_size, n_cols, coeffs, stride))
     return set_error(STWO_B200_E_INVALID, "coefficients must be 16-byte aligned with a stride of a multiple of 4");
   size_t parts = sb::eval_at_point_partial_count(log_size, n_cols);
   void* scratch = nullptr;
-  cudaError_t e = cudaMallocAsync(&scratch, parts * sizeof(sb::QM31), st(stream));
-  if (e != cudaSuccess) return cuda_status(e, "eval_at_point scratch");
+  cudaError_t e = sb::dev_malloc_async(&scratch, parts * sizeof(sb::QM31), st(stream));
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    return set_error(STWO_B200_E_OOM, std::string("eval_at_point scratch: ") + cudaGetErrorString(e));
+  }
   e = sb::eval_at_point(ctx->ctx.tables, log_size, n_cols, coeffs, stride, sb::PointQ{q(px), q(py)}, nullptr,
                         static_cast<sb::QM31*>(scratch), reinterpret_cast<sb::QM31*>(out_dev), st(stream));
   cudaError_t e2 = cudaFreeAsync(scratch, st(stream));
@@ -461,7 +466,8 @@ int32_t stwo_b200_accumulate(stwo_b200_context* ctx, uint32_t dst_log, uint32_t*
 int32_t stwo_b200_pow_grind(stwo_b200_context* ctx, const uint8_t prefix_digest[32], uint32_t n_bits,
                             uint64_t* nonce_out) {
   CK_CTX(ctx);
-  if (!prefix_digest || !nonce_out || n_bits > 64) return set_error(STWO_B200_E_INVALID, "bad pow arguments");
+  if (!prefix_digest || !nonce_out || n_bits > sb::MAX_POW_BITS)
+    return set_error(STWO_B200_E_INVALID, "bad pow arguments (n_bits above STWO_B200_MAX_POW_BITS)");
   if (n_bits == 0) { *nonce_out = 0; return STWO_B200_OK; }
   std::lock_guard<std::mutex> g(ctx->ctx.small_mu);
   cudaStream_t s = ctx->ctx.stream;
@@ -608,6 +614,17 @@ int32_t stwo_b200_server_warmup(stwo_b200_server* server, uint32_t max_log_n_row
   std::string err;
   int32_t rc = server->server->warmup(max_log_n_rows, max_sequence_len, log_blowup, max_xor_log_n, &err);
   return rc == STWO_B200_OK ? rc : set_error(rc, err);
+}
+
+int32_t stwo_b200_server_set_request_timeout(stwo_b200_server* server, uint32_t timeout_ms) {
+  if (!server) return set_error(STWO_B200_E_INVALID, "null server");
+  server->server->set_request_timeout(timeout_ms);
+  return STWO_B200_OK;
+}
+
+int32_t stwo_b200_arm_allocation_failure_for_testing(uint32_t nth) {
+  sb::alloc_fail_countdown().store(nth, std::memory_order_relaxed);
+  return STWO_B200_OK;
 }
 
 int32_t stwo_b200_server_snapshot_get(stwo_b200_server* server, stwo_b200_server_snapshot* out) {

@@ -89,6 +89,8 @@ inline bool eval_at_point_aligned(uint32_t log_size, uint32_t n_cols, const uint
   return (reinterpret_cast<uintptr_t>(coeffs) & 15) == 0 && (n_cols <= 1 || stride % 4 == 0);
 }
 size_t eval_at_point_partial_count(uint32_t log_size, uint32_t n_cols);
+// Columns of one eval_at_point call: one grid row each (the grid's y extent).
+constexpr uint32_t EVAL_AT_POINT_MAX_COLS = 65535;
 
 // ---- DEEP quotients (src/core/pcs/quotients/row_evaluation.zig) -----------
 struct QuotientBatchDev {

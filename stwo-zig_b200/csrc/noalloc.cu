@@ -19,9 +19,13 @@
 //    contents. The kernels overwrite every partial they later read, so nothing
 //    needs clearing, but two calls whose work overlaps on the GPU (different
 //    streams, or different host threads) race on the array: serialize them.
+//  - At most STWO_B200_EVAL_AT_POINT_MAX_COLS (65535) columns per call, the
+//    grid's y extent, as for the allocating entry point.
 //  - The first call on each device looks up the array's device address
 //    (cudaGetSymbolAddress) and caches it; make that first call before any
-//    stream capture.
+//    stream capture. The cached address belongs to the device's primary
+//    context: an embedder that resets the device (cudaDeviceReset) must not
+//    call this entry point again in the same process.
 #include <mutex>
 #include <string>
 
@@ -63,7 +67,7 @@ int32_t stwo_b200_eval_at_point_noalloc(stwo_b200_context* ctx, uint32_t log_siz
                                         const uint32_t* coeffs, uint64_t stride, stwo_b200_qm31 px,
                                         stwo_b200_qm31 py, stwo_b200_qm31* out_dev, void* stream) {
   if (!ctx) return sb::set_last_error(STWO_B200_E_INVALID, "null context");
-  if (log_size > 28 || (n_cols && (!coeffs || !out_dev)))
+  if (log_size > 28 || n_cols > sb::EVAL_AT_POINT_MAX_COLS || (n_cols && (!coeffs || !out_dev)))
     return sb::set_last_error(STWO_B200_E_INVALID, "bad eval_at_point_noalloc arguments");
   if (n_cols == 0) return STWO_B200_OK;
   if (!sb::eval_at_point_aligned(log_size, n_cols, coeffs, stride))

@@ -14,6 +14,7 @@
 #include <cstring>
 #include <stdexcept>
 
+#include "alloc.hpp"
 #include "blake2s.cuh"
 #include "prover.hpp"
 #include "prover_common.hpp"
@@ -192,6 +193,15 @@ WideFibProver::~WideFibProver() {
   if (stream_) cudaStreamDestroy(stream_);
 }
 
+void WideFibProver::drop_workspace() {
+  if (transient_ || !arena_) return;
+  cudaSetDevice(ctx_->device);
+  cudaFree(arena_);
+  arena_ = nullptr;
+  arena_size_ = 0;
+  ws_log_n_ = ws_W_ = ws_B_ = 0;
+}
+
 void WideFibProver::release() {
   if (arena_) cudaFree(arena_);
   if (pinned_) cudaFreeHost(pinned_);
@@ -226,11 +236,11 @@ int32_t WideFibProver::reserve(uint32_t log_n, uint32_t W, uint32_t B, size_t* h
 int32_t WideFibProver::ensure_workspace(uint32_t log_n, uint32_t W, uint32_t B) {
   if (!pinned_) {
     pinned_size_ = GATHER_SCRATCH + (1 << 20);
-    if (cudaMallocHost(&pinned_, pinned_size_) != cudaSuccess) { pinned_ = nullptr; return fail(E_OOM, "pinned staging allocation failed"); }
+    if (host_malloc_pinned(reinterpret_cast<void**>(&pinned_), pinned_size_) != cudaSuccess) { pinned_ = nullptr; return fail(E_OOM, "pinned staging allocation failed"); }
   }
   size_t need = workspace_bytes(log_n, W, B);
   if (transient_) {
-    if (cudaMallocAsync(&arena_, need, stream_) != cudaSuccess) {
+    if (dev_malloc_async(reinterpret_cast<void**>(&arena_), need, stream_) != cudaSuccess) {
       arena_ = nullptr;
       cudaGetLastError();
       return fail(E_OOM, "device workspace allocation failed");
@@ -245,7 +255,7 @@ int32_t WideFibProver::ensure_workspace(uint32_t log_n, uint32_t W, uint32_t B) 
     return OK;
   }
   if (arena_) { cudaFree(arena_); arena_ = nullptr; }
-  if (cudaMalloc(&arena_, need) != cudaSuccess) { arena_ = nullptr; cudaGetLastError(); return fail(E_OOM, "device workspace allocation failed"); }
+  if (dev_malloc(reinterpret_cast<void**>(&arena_), need) != cudaSuccess) { arena_ = nullptr; cudaGetLastError(); return fail(E_OOM, "device workspace allocation failed"); }
   arena_size_ = need;
   ws_log_n_ = log_n; ws_W_ = W; ws_B_ = B;
   return OK;
@@ -256,7 +266,7 @@ int32_t WideFibProver::prove(const ProveRequest& req, std::string& out, StageTim
   const PcsConfig& cfg = req.config;
   const uint32_t B = cfg.log_blowup_factor;
   if (n < 1 || n > 22 || W < 2 || W > 1000 || B < 1 || B > 4 || n + B > ctx_->tables.tower_log + 1 ||
-      n + 1 > ctx_->tables.tower_log + 1 || cfg.n_queries == 0 || cfg.n_queries > 4096 || cfg.pow_bits > 64)
+      n + 1 > ctx_->tables.tower_log + 1 || cfg.n_queries == 0 || cfg.n_queries > 4096 || cfg.pow_bits > MAX_POW_BITS)
     return fail(E_INVALID, "unsupported proof shape or configuration");
   if (n + B < cfg.log_last_layer_degree_bound + B + 1) return fail(E_INVALID, "last layer larger than the domain");
   if (req.trace_kind < 0 || req.trace_kind > TRACE_FIRST_COLUMNS)
@@ -340,6 +350,7 @@ int32_t WideFibProver::prove(const ProveRequest& req, std::string& out, StageTim
   SB_CK(cudaEventRecord(ev_[3], s));
   SB_CK(sync());
   std::memcpy(root1, pin, 32);
+  if (deadline_.passed()) return fail(E_TIMEOUT, "proof deadline passed after the main commitment");
   ch.mix_root(root1);
   {
     uint32_t st[2] = {n, W};
@@ -377,6 +388,7 @@ int32_t WideFibProver::prove(const ProveRequest& req, std::string& out, StageTim
   SB_CK(cudaEventRecord(ev_[5], s));
   SB_CK(sync());
   std::memcpy(root2, pin, 32);
+  if (deadline_.passed()) return fail(E_TIMEOUT, "proof deadline passed after the composition commitment");
   ch.mix_root(root2);
 
   // OODS point and sampled values of every coefficient column.
@@ -425,7 +437,7 @@ int32_t WideFibProver::prove(const ProveRequest& req, std::string& out, StageTim
   {
     std::string ferr;
     int32_t frc = fri_pow_queries(T, ctx_->sm_count, ch, cfg, l.L, l.n_inner, l.last_log, fbuf, pin, s, fs, ev_[8],
-                                  ev_[9], fr, ferr);
+                                  ev_[9], deadline_, fr, ferr);
     if (frc != OK) return fail(frc, ferr);
   }
   const std::vector<uint64_t>& queries = fr.queries;
@@ -522,7 +534,7 @@ const char* status_string(int32_t code) {
     case E_INVALID: return "invalid argument";
     case E_OOM: return "out of device memory";
     case E_CUDA: return "CUDA error";
-    case E_TIMEOUT: return "device search bound reached";
+    case E_TIMEOUT: return "deadline or search bound reached";
     case E_CONSTRAINTS: return "constraints not satisfied";
     case E_BUFFER_TOO_SMALL: return "output buffer too small";
     case E_FALLBACK: return "operation not taken by the device";

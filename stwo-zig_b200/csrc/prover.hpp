@@ -2,6 +2,7 @@
 #pragma once
 #include <cuda_runtime.h>
 
+#include <chrono>
 #include <cstdint>
 #include <mutex>
 #include <string>
@@ -19,6 +20,20 @@ struct PcsConfig {
 };
 
 constexpr int TRACE_FIRST_COLUMNS = 2;
+
+// Largest accepted proof-of-work difficulty. The grind tests 2^pow_bits nonces on average
+// (about 40 s on one B200 at 40 bits) and holds its stream meanwhile; the reference accepts any
+// u32, so the cap is this backend's own.
+constexpr uint32_t MAX_POW_BITS = 40;
+
+using Clock = std::chrono::steady_clock;
+// Optional time limit of one proof, checked between stages and between proof-of-work rounds; a
+// proof past it ends with E_TIMEOUT and leaves no work in flight.
+struct Deadline {
+  Clock::time_point at = Clock::time_point::max();
+  bool set() const { return at != Clock::time_point::max(); }
+  bool passed() const { return set() && Clock::now() >= at; }
+};
 
 struct ProveRequest {
   uint32_t log_n_rows = 0, sequence_len = 0;
@@ -73,6 +88,12 @@ class WideFibProver {
   // Grows the persistent workspace to a shape ahead of use (no-op in transient mode); returns the
   // bytes the prover holds afterwards in *held.
   int32_t reserve(uint32_t log_n, uint32_t W, uint32_t B, size_t* held);
+  // Frees the persistent workspace (the serving loop gives back an idle slot's memory).
+  void drop_workspace();
+  // Device workspace held between proofs (0 in transient mode).
+  size_t held_bytes() const { return transient_ ? 0 : arena_size_; }
+  // Time limit of the next proofs (a default Deadline: none).
+  void set_deadline(Deadline d) { deadline_ = d; }
 
  private:
   int32_t ensure_workspace(uint32_t log_n, uint32_t W, uint32_t B);
@@ -94,6 +115,7 @@ class WideFibProver {
   uint8_t* pinned_ = nullptr;
   size_t pinned_size_ = 0;
   cudaEvent_t ev_[12];
+  Deadline deadline_;
 };
 
 // LogUp XOR-lookup AIR request (xor_prover.cu): 2^log_n lookups of seeded w-bit pairs
@@ -115,6 +137,7 @@ class LogupXorProver {
   const std::string& error() const { return err_; }
   // Device workspace of one proof of this shape (bytes); 0 for an impossible shape.
   static size_t workspace_bytes(uint32_t log_n, uint32_t log_table, uint32_t log_blowup, uint32_t log_last_layer);
+  void set_deadline(Deadline d) { deadline_ = d; }
 
  private:
   static constexpr size_t PINNED_BYTES = (8 << 20) + (1 << 20);
@@ -123,6 +146,7 @@ class LogupXorProver {
   cudaStream_t stream_ = nullptr, fast_ = nullptr;
   uint8_t* pinned_ = nullptr;
   std::string err_;
+  Deadline deadline_;
 };
 
 struct Context {

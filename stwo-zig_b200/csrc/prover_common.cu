@@ -16,7 +16,8 @@ namespace sb {
 
 int32_t fri_pow_queries(const DeviceTables& T, int sm_count, Channel& ch, const PcsConfig& cfg, uint32_t L,
                         uint32_t n_inner, uint32_t last_log, const FriBuffers& fb, uint8_t* pin, cudaStream_t s,
-                        cudaStream_t fs, cudaEvent_t ev_fri, cudaEvent_t ev_pow, FriResult& out, std::string& err) {
+                        cudaStream_t fs, cudaEvent_t ev_fri, cudaEvent_t ev_pow, const Deadline& deadline,
+                        FriResult& out, std::string& err) {
   const uint64_t NL = 1ull << L;
   // FRI: first layer, then inner layers each committed before its fold. The channel steps
   // between them (mix the layer's root, draw its alpha) run on the device, so the layers
@@ -130,6 +131,10 @@ int32_t fri_pow_queries(const DeviceTables& T, int sm_count, Channel& ch, const 
       SB_CKE(cudaMemcpyAsync(pin, fb.pow_result, 8, cudaMemcpyDeviceToHost, s));
       SB_CKE(cudaStreamSynchronize(s));
       std::memcpy(&nonce, pin, 8);
+      if (nonce == ~0ull && deadline.passed()) {
+        err = "proof deadline passed during the proof-of-work search";
+        return E_TIMEOUT;
+      }
     }
     if (nonce == ~0ull) { err = "proof-of-work search bound reached"; return E_TIMEOUT; }
   }

@@ -260,10 +260,12 @@ struct FriResult {
 // Runs on `fs` (FRI, latency-bound) and `s` (proof of work); `pin` is pinned host staging
 // (at least 64 KB). The FRI layers draw their alphas on the device (FriChannelDev); the
 // host replays the same channel steps from the returned roots and checks every alpha.
-// ev_fri and ev_pow (nullable) are recorded after the last layer and after the grind.
+// ev_fri and ev_pow (nullable) are recorded after the last layer and after the grind. A deadline
+// that passes during the grind ends it after the current rounds with E_TIMEOUT.
 int32_t fri_pow_queries(const DeviceTables& T, int sm_count, Channel& ch, const PcsConfig& cfg, uint32_t L,
                         uint32_t n_inner, uint32_t last_log, const FriBuffers& fb, uint8_t* pin, cudaStream_t s,
-                        cudaStream_t fs, cudaEvent_t ev_fri, cudaEvent_t ev_pow, FriResult& out, std::string& err);
+                        cudaStream_t fs, cudaEvent_t ev_fri, cudaEvent_t ev_pow, const Deadline& deadline,
+                        FriResult& out, std::string& err);
 
 // ---------------------------------------------------------------------------
 // Decommitment (src/prover/vcs_lifted/decommit.zig:56-352, src/prover/fri.zig:624-850):

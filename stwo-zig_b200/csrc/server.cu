@@ -19,7 +19,7 @@ bool profile_limits(uint32_t profile, ResourceLimits* out) {
 }
 
 Server::Server(Context* ctx, uint32_t slots, uint64_t budget, uint32_t profile, uint32_t flags)
-    : ctx_(ctx), n_slots_(slots), budget_(budget), flags_(flags), held_(slots, 0) {
+    : ctx_(ctx), n_slots_(slots), budget_(budget), flags_(flags), held_(slots, 0), idle_(slots, 0) {
   if (!profile_limits(profile, &limits_)) limits_ = {0, 0};
   snap_.budget_bytes = budget;
 }
@@ -71,12 +71,51 @@ int32_t Server::enqueue(Entry* e, uint64_t cells, size_t ws, uint64_t* ticket, s
   e->stats.accounted_bytes = accounted;
   e->stats.workspace_bytes = ws;
   e->t_submit = std::chrono::steady_clock::now();
+  if (timeout_ms_) e->deadline.at = e->t_submit + std::chrono::milliseconds(timeout_ms_);
   table_[e->ticket] = e;
   queue_.push_back(e);
   ++snap_.submitted;
   *ticket = e->ticket;
-  cv_work_.notify_one();
+  // Every idle slot looks at the new head: the one it fits on takes it.
+  cv_work_.notify_all();
   return OK;
+}
+
+void Server::set_request_timeout(uint32_t ms) {
+  std::lock_guard<std::mutex> g(mu_);
+  timeout_ms_ = ms;
+}
+
+uint64_t Server::extra_on(uint32_t slot, const Entry* e) const {
+  // Transient workspaces count while their proof runs; a persistent one counts for as long as its
+  // slot holds it (a slot grows to the largest proof it has run). XOR-lookup proofs always take
+  // their workspace from the pool for the proof's duration.
+  if (!(flags_ & SERVER_PERSISTENT_WORKSPACES) || e->is_xor) return e->workspace;
+  return e->workspace > held_[slot] ? e->workspace - held_[slot] : 0;
+}
+
+int64_t Server::best_idle_slot(const Entry* e) const {
+  int64_t best = -1;
+  uint64_t best_extra = 0;
+  for (uint32_t i = 0; i < n_slots_; ++i) {
+    if (!idle_[i]) continue;
+    uint64_t x = extra_on(i, e);
+    if (best < 0 || x < best_extra) { best = i; best_extra = x; }
+  }
+  return best;
+}
+
+void Server::finish(Entry* e, int32_t status, std::string&& proof, std::string&& error) {
+  e->status = status;
+  if (status == OK) {
+    e->proof = std::move(proof);
+    ++snap_.completed;
+  } else {
+    e->error = std::move(error);
+    ++snap_.failed;
+  }
+  e->done = true;
+  cv_done_.notify_all();
 }
 
 int32_t Server::submit(const ProveRequest& r, uint64_t* ticket, std::string* err) {
@@ -114,24 +153,56 @@ int32_t Server::submit_xor(const XorRequest& r, uint64_t* ticket, std::string* e
 void Server::worker(uint32_t slot) {
   cudaSetDevice(ctx_->device);
   WideFibProver* prover = provers_[slot];
+  const bool persistent = flags_ & SERVER_PERSISTENT_WORKSPACES;
   std::unique_lock<std::mutex> lk(mu_);
   for (;;) {
-    // First in, first admitted: the head waits until its workspace fits the budget. Transient
-    // workspaces count while their proof runs; persistent ones count for as long as a slot holds
-    // them (a slot grows its workspace to the largest proof it has run).
-    const bool persistent = flags_ & SERVER_PERSISTENT_WORKSPACES;
-    // XOR-lookup proofs always take their workspace from the pool for the proof's duration.
-    auto extra = [&](const Entry* h) -> uint64_t {
-      if (!persistent || h->is_xor) return h->workspace;
-      return h->workspace > held_[slot] ? h->workspace - held_[slot] : 0;
-    };
-    cv_work_.wait(lk, [&] {
-      return (stopping_ && queue_.empty()) || (!queue_.empty() && in_use_ + extra(queue_.front()) <= budget_);
-    });
-    if (queue_.empty()) return;
-    Entry* e = queue_.front();
+    // Admission, first in first admitted: the head runs on a free slot once its workspace fits the
+    // budget. Every idle slot re-evaluates on each change (submit, admission, completion, release):
+    // - the head fits here: take it;
+    // - it fits on another idle slot (one that holds more workspace): leave it to that slot;
+    // - it fits nowhere: an idle slot whose held workspace is not what the head would reuse gives it
+    //   back, so the head fits once the proofs in flight finish (a workspace never exceeds the
+    //   budget, which submit checks).
+    idle_[slot] = 1;
+    Entry* e = nullptr;
+    for (;;) {
+      if (queue_.empty()) {
+        if (stopping_) {
+          idle_[slot] = 0;
+          return;
+        }
+        cv_work_.wait(lk);
+        continue;
+      }
+      Entry* h = queue_.front();
+      if (h->deadline.passed()) {
+        queue_.pop_front();
+        h->t_start = std::chrono::steady_clock::now();
+        h->stats.queued_ms = std::chrono::duration<double, std::milli>(h->t_start - h->t_submit).count();
+        finish(h, E_TIMEOUT, std::string(), std::string("request deadline passed before admission"));
+        cv_work_.notify_all();
+        continue;
+      }
+      if (in_use_ + extra_on(slot, h) <= budget_) {
+        e = h;
+        break;
+      }
+      const int64_t best = best_idle_slot(h);
+      const bool fits_elsewhere = best >= 0 && best != (int64_t)slot && in_use_ + extra_on((uint32_t)best, h) <= budget_;
+      if (!fits_elsewhere && persistent && held_[slot] > 0 && (best != (int64_t)slot || h->is_xor)) {
+        // Give back this idle slot's workspace (cudaFree waits for the device; no proof of this slot
+        // is in flight, and the others do not need the lock until they finish).
+        prover->drop_workspace();
+        in_use_ -= held_[slot];
+        held_[slot] = 0;
+        cv_work_.notify_all();
+        continue;
+      }
+      cv_work_.wait(lk);
+    }
     queue_.pop_front();
-    const uint64_t added = extra(e);
+    idle_[slot] = 0;
+    const uint64_t added = extra_on(slot, e);
     in_use_ += added;
     if (persistent && !e->is_xor) held_[slot] += added;
     ++in_flight_;
@@ -141,13 +212,15 @@ void Server::worker(uint32_t slot) {
     e->stats.slot = slot;
     lk.unlock();
     // Another head may fit beside this one.
-    cv_work_.notify_one();
+    cv_work_.notify_all();
     std::string proof, xerr;
     int32_t rc;
     if (e->is_xor) {
+      xor_provers_[slot]->set_deadline(e->deadline);
       rc = xor_provers_[slot]->prove(e->xreq, proof);
       if (rc != OK) xerr = xor_provers_[slot]->error();
     } else {
+      prover->set_deadline(e->deadline);
       rc = prover->prove(e->req, proof, &e->stats.stages);
       if (rc != OK) xerr = prover->error();
     }
@@ -165,20 +238,18 @@ void Server::worker(uint32_t slot) {
     }
     auto t_end = std::chrono::steady_clock::now();
     lk.lock();
-    if (!persistent || e->is_xor) in_use_ -= e->workspace;
-    --in_flight_;
-    e->status = rc;
-    if (rc == OK) {
-      e->proof.swap(proof);
-      ++snap_.completed;
+    if (!persistent || e->is_xor) {
+      in_use_ -= e->workspace;
     } else {
-      e->error = xerr;
-      ++snap_.failed;
+      // The slot's accounting follows what its prover holds (a failed growth holds nothing).
+      const uint64_t actual = prover->held_bytes();
+      in_use_ = in_use_ - held_[slot] + actual;
+      held_[slot] = actual;
     }
+    --in_flight_;
     e->stats.queued_ms = std::chrono::duration<double, std::milli>(e->t_start - e->t_submit).count();
     e->stats.run_ms = std::chrono::duration<double, std::milli>(t_end - e->t_start).count();
-    e->done = true;
-    cv_done_.notify_all();
+    finish(e, rc, std::move(proof), std::move(xerr));
     cv_work_.notify_all();
   }
 }

@@ -58,6 +58,10 @@ class Server {
   // it while the server is idle.
   int32_t warmup(uint32_t max_log_n_rows, uint32_t max_sequence_len, uint32_t log_blowup, uint32_t max_xor_log_n,
                  std::string* err);
+  // Time limit of every request submitted from now on, from its submission (0: none). A request
+  // still queued at its deadline ends with E_TIMEOUT without running; a running proof checks the
+  // deadline between stages and proof-of-work rounds and ends with E_TIMEOUT.
+  void set_request_timeout(uint32_t ms);
   // Blocks until the request is done. E_BUFFER_TOO_SMALL keeps the result for another call.
   int32_t wait(uint64_t ticket, uint8_t* out, size_t cap, size_t* len, RequestStats* stats, std::string* err);
   ServerSnapshot snapshot();
@@ -71,12 +75,19 @@ class Server {
     size_t workspace = 0;
     RequestStats stats;
     std::chrono::steady_clock::time_point t_submit, t_start;
+    Deadline deadline;
     bool done = false;
     int32_t status = 0;
     std::string proof, error;
   };
   void worker(uint32_t slot);
   int32_t enqueue(Entry* e, uint64_t cells, size_t workspace, uint64_t* ticket, std::string* err);
+  // Workspace bytes the request would add to in_use_ on `slot` (caller holds mu_).
+  uint64_t extra_on(uint32_t slot, const Entry* e) const;
+  // The idle slot on which the request adds the least (lowest index on ties), or -1.
+  int64_t best_idle_slot(const Entry* e) const;
+  // Marks a request done with `status` and wakes its waiter (caller holds mu_).
+  void finish(Entry* e, int32_t status, std::string&& proof, std::string&& error);
 
   Context* ctx_;
   uint32_t n_slots_;
@@ -84,6 +95,8 @@ class Server {
   uint32_t flags_;
   ResourceLimits limits_;
   std::vector<uint64_t> held_;  // persistent mode: workspace bytes each slot holds
+  std::vector<uint8_t> idle_;   // slots waiting for a request
+  uint32_t timeout_ms_ = 0;
   std::mutex mu_;
   std::condition_variable cv_work_, cv_done_;
   std::deque<Entry*> queue_;

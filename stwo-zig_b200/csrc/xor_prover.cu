@@ -38,6 +38,7 @@
 #include <algorithm>
 #include <cstring>
 
+#include "alloc.hpp"
 #include "prover_common.hpp"
 
 namespace sb {
@@ -231,7 +232,6 @@ LogupXorProver::LogupXorProver(Context* ctx) : ctx_(ctx) {
   cudaDeviceGetStreamPriorityRange(&least, &greatest);
   cudaStreamCreateWithPriority(&stream_, cudaStreamNonBlocking, least);
   cudaStreamCreateWithPriority(&fast_, cudaStreamNonBlocking, greatest);
-  cudaMallocHost(&pinned_, PINNED_BYTES);
 }
 
 LogupXorProver::~LogupXorProver() {
@@ -244,14 +244,20 @@ int32_t LogupXorProver::prove(const XorRequest& req, std::string& out) {
   const PcsConfig& cfg = req.config;
   const uint32_t B = cfg.log_blowup_factor;
   if (req.log_n < 1 || req.log_n > 22 || (req.log_table != 8 && req.log_table != 16) || B < 1 || B > 4 ||
-      cfg.n_queries == 0 || cfg.n_queries > 4096 || cfg.pow_bits > 64)
+      cfg.n_queries == 0 || cfg.n_queries > 4096 || cfg.pow_bits > MAX_POW_BITS)
     return fail(E_INVALID, "unsupported XOR-lookup shape or configuration");
   const uint32_t n = req.log_n, t = req.log_table;
   const uint32_t L = std::max(n, t), LDE = L + B, CL = L + 1;
   if (LDE > ctx_->tables.tower_log + 1 || cfg.log_last_layer_degree_bound + B + 1 > LDE)
     return fail(E_INVALID, "domain too large for the context or last layer too large");
-  if (!pinned_ || !stream_ || !fast_) return fail(E_OOM, "stream or pinned staging allocation failed");
+  if (!stream_ || !fast_) return fail(E_CUDA, "stream creation failed");
   cudaSetDevice(ctx_->device);
+  // Pinned staging on first use (a failed allocation leaves the prover usable for the next call).
+  if (!pinned_ && host_malloc_pinned(reinterpret_cast<void**>(&pinned_), PINNED_BYTES) != cudaSuccess) {
+    pinned_ = nullptr;
+    cudaGetLastError();
+    return fail(E_OOM, "pinned staging allocation failed");
+  }
   const uint64_t N = 1ull << L, NL = 1ull << LDE, NC = 1ull << CL;
   const uint32_t last_log = cfg.log_last_layer_degree_bound + B;
   const uint32_t n_inner = (LDE - 1) - last_log;
@@ -263,7 +269,7 @@ int32_t LogupXorProver::prove(const XorRequest& req, std::string& out) {
   XorShape shape{L, B, n, t, n_inner};
   const size_t need = xor_workspace_bytes(shape);
   uint8_t* arena_mem = nullptr;
-  if (cudaMallocAsync(reinterpret_cast<void**>(&arena_mem), need, s) != cudaSuccess) {
+  if (dev_malloc_async(reinterpret_cast<void**>(&arena_mem), need, s) != cudaSuccess) {
     cudaGetLastError();
     return fail(E_OOM, "device workspace allocation failed");
   }
@@ -314,6 +320,7 @@ int32_t LogupXorProver::prove(const XorRequest& req, std::string& out) {
     SB_CK(cudaMemcpyAsync(pin, b.tree[tr] + (2 * leaves - 2) * 32, 32, cudaMemcpyDeviceToHost, s));
     SB_CK(cudaStreamSynchronize(s));
     std::memcpy(roots[tr], pin, 32);
+    if (deadline_.passed()) return fail(E_TIMEOUT, "proof deadline passed after a commitment");
     ch.mix_root(roots[tr]);
     return OK;
   };
@@ -539,7 +546,7 @@ int32_t LogupXorProver::prove(const XorRequest& req, std::string& out) {
   {
     std::string ferr;
     int32_t frc = fri_pow_queries(T, ctx_->sm_count, ch, cfg, LDE, n_inner, last_log, fbuf, pin, s, fs, nullptr,
-                                  nullptr, fr, ferr);
+                                  nullptr, deadline_, fr, ferr);
     if (frc != OK) return fail(frc, ferr);
   }
   DecommitPlan plan;

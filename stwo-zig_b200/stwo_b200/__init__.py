@@ -128,6 +128,8 @@ _SIGS = {
     "stwo_b200_server_warmup": [_vp, _u32, _u32, _u32, _u32],
     "stwo_b200_server_snapshot_get": [_vp, ctypes.POINTER(ServerSnapshotC)],
     "stwo_b200_server_destroy": [_vp],
+    "stwo_b200_server_set_request_timeout": [_vp, _u32],
+    "stwo_b200_arm_allocation_failure_for_testing": [_u32],
     "stwo_b200_xor_lookup_trace": [_vp, _u32, _u64, _vp, _vp, _vp, _vp],
     "stwo_b200_batch_inverse": [_vp, _u32, _u64, _vp, _u64, _vp, _u64, _vp],
     "stwo_b200_logup_interaction": [_vp, _u32, _u32, ctypes.POINTER(LogupUseC), ctypes.POINTER(QM31C), QM31C,
@@ -561,6 +563,10 @@ class Server:
         """Sizes every slot for the largest shapes before traffic (call while idle)."""
         _check(_lib.stwo_b200_server_warmup(self._h, max_log_n_rows, max_sequence_len, log_blowup, max_xor_log_n))
 
+    def set_request_timeout(self, timeout_ms: int) -> None:
+        """Time limit of every request submitted from now on (0: none); see the C header."""
+        _check(_lib.stwo_b200_server_set_request_timeout(self._h, timeout_ms))
+
     def snapshot(self) -> dict:
         s = ServerSnapshotC()
         _check(_lib.stwo_b200_server_snapshot_get(self._h, ctypes.byref(s)))
@@ -583,3 +589,9 @@ class Server:
             self.close()
         except Exception:
             pass
+
+
+def arm_allocation_failure_for_testing(nth: int) -> None:
+    """Makes the library's nth device or pinned allocation from now on fail as out of memory
+    (0 disarms); a host-side test hook, no GPU fault is involved."""
+    _check(_lib.stwo_b200_arm_allocation_failure_for_testing(nth))

@@ -1,0 +1,169 @@
+"""Failure handling on the host side: out-of-memory on an allocation, request deadlines, the
+proof-of-work cap, and serving-loop progress when slots hold workspaces of different sizes.
+
+Failures are injected on the host (the library's allocation hook, a deadline that runs out, a tight
+memory budget), as the reference arms its failures (armOwnershipTransferFailureForTesting,
+src/backends/metal/commit_backend.zig:69-71; fail-closed admission,
+src/prover/native/resource_admission.zig:73-89). Nothing faults, traps or hangs the GPU: the
+serving-loop case runs in a child process with a host-side time limit.
+"""
+import os
+import subprocess
+import sys
+import textwrap
+
+import numpy as np
+import pytest
+
+import oracle
+
+pytestmark = pytest.mark.gpu
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def _cfg(preset="functional", **over):
+    import stwo_b200 as sb
+    c = oracle.config(preset, **over)
+    return c, sb.PcsConfig(c.pow_bits, sb.FriConfig(c.log_blowup_factor, c.log_last_layer_degree_bound, c.n_queries))
+
+
+def test_failed_workspace_allocation_leaves_the_context_usable():
+    import stwo_b200 as sb
+    import torch
+    o, g = _cfg()
+    ref = oracle.prove_wide_fib(16, 32, o, trace_kind=1, trace_seed=4)
+    c = sb.Context(0)  # its own prover pool: a new prover allocates pinned staging, then its workspace
+    try:
+        for nth in (1, 2):  # the pinned staging, then the device workspace
+            torch.cuda.synchronize()
+            free_before, _ = torch.cuda.mem_get_info()
+            sb.arm_allocation_failure_for_testing(nth)
+            with pytest.raises(sb.StwoError) as e:
+                c.prove_wide_fibonacci(sb.Statement(16, 32), g, trace_kind=sb.TRACE_SEEDED, trace_seed=4)
+            assert e.value.status == sb.E_OOM
+            free_after, _ = torch.cuda.mem_get_info()
+            assert free_after >= free_before  # the failed call kept no device memory
+        assert c.prove_wide_fibonacci(sb.Statement(16, 32), g, trace_kind=sb.TRACE_SEEDED, trace_seed=4) == ref
+        # Growing the prover's workspace for a larger shape: the old one is released, the new one fails.
+        torch.cuda.synchronize()
+        free_before, _ = torch.cuda.mem_get_info()
+        sb.arm_allocation_failure_for_testing(1)
+        with pytest.raises(sb.StwoError) as e:
+            c.prove_wide_fibonacci(sb.Statement(17, 32), g, trace_kind=sb.TRACE_SEEDED, trace_seed=5)
+        assert e.value.status == sb.E_OOM
+        assert torch.cuda.mem_get_info()[0] >= free_before
+        ref = oracle.prove_wide_fib(17, 32, o, trace_kind=1, trace_seed=5)
+        assert c.prove_wide_fibonacci(sb.Statement(17, 32), g, trace_kind=sb.TRACE_SEEDED, trace_seed=5) == ref
+    finally:
+        sb.arm_allocation_failure_for_testing(0)
+        c.close()
+
+
+def test_failed_allocations_of_the_xor_prover_and_op_level_calls(ctx):
+    import stwo_b200 as sb
+    import torch
+    _, g = _cfg()
+    want = ctx.prove_logup_xor(12, g, seed=5, log_table=8)
+    try:
+        _xor_and_op_level_failures(ctx, sb, torch, g, want)
+    finally:
+        sb.arm_allocation_failure_for_testing(0)
+
+
+def _xor_and_op_level_failures(ctx, sb, torch, g, want):
+    sb.arm_allocation_failure_for_testing(1)
+    with pytest.raises(sb.StwoError) as e:
+        ctx.prove_logup_xor(12, g, seed=5, log_table=8)
+    assert e.value.status == sb.E_OOM
+    assert ctx.prove_logup_xor(12, g, seed=5, log_table=8) == want
+    # The op-level OODS evaluation takes its scratch from the stream's pool.
+    cols = torch.ones(2 << 14, dtype=torch.int32, device="cuda")
+    out = torch.zeros(8, dtype=torch.int32, device="cuda")
+    sb.arm_allocation_failure_for_testing(1)
+    with pytest.raises(sb.StwoError) as e:
+        ctx.eval_at_point(cols, 14, 2, 1 << 14, [1, 2, 3, 4], [5, 6, 7, 8], out)
+    assert e.value.status == sb.E_OOM
+    ctx.eval_at_point(cols, 14, 2, 1 << 14, [1, 2, 3, 4], [5, 6, 7, 8], out)
+    torch.cuda.synchronize()
+
+
+def test_pow_bits_above_the_cap_are_refused(ctx):
+    import stwo_b200 as sb
+    _, g = _cfg(pow_bits=41)
+    with pytest.raises(sb.StwoError) as e:
+        ctx.prove_wide_fibonacci(sb.Statement(8, 8), g, trace_kind=sb.TRACE_SEEDED, trace_seed=1)
+    assert e.value.status == sb.E_INVALID
+    with pytest.raises(sb.StwoError) as e:
+        ctx.pow_grind(bytes(32), 41)
+    assert e.value.status == sb.E_INVALID
+
+
+def test_request_deadlines(ctx):
+    import stwo_b200 as sb
+    _, hard = _cfg(pow_bits=40)  # about 2^40 nonces expected: far beyond the deadline
+    o, g = _cfg()
+    with sb.Server(ctx, slots=1, profile=1) as srv:
+        srv.set_request_timeout(200)
+        t_run = srv.submit(sb.Statement(12, 16), hard, trace_kind=sb.TRACE_SEEDED, trace_seed=11)
+        srv.set_request_timeout(20)
+        t_queued = srv.submit(sb.Statement(12, 16), g, trace_kind=sb.TRACE_SEEDED, trace_seed=12)
+        srv.set_request_timeout(0)
+        t_ok = srv.submit(sb.Statement(12, 16), g, trace_kind=sb.TRACE_SEEDED, trace_seed=13)
+        with pytest.raises(sb.StwoError) as e:
+            srv.wait(t_run)
+        assert e.value.status == sb.E_TIMEOUT and "proof-of-work" in str(e.value)
+        with pytest.raises(sb.StwoError) as e:
+            srv.wait(t_queued)
+        assert e.value.status == sb.E_TIMEOUT and "before admission" in str(e.value)
+        proof, _ = srv.wait(t_ok)
+        snap = srv.snapshot()
+    assert snap["failed"] == 2 and snap["completed"] == 1
+    assert proof == oracle.prove_wide_fib(12, 16, o, trace_kind=1, trace_seed=13)
+
+
+_LIVENESS = textwrap.dedent(r"""
+    import sys
+    sys.path[:0] = [{root!r} + "/stwo-zig_b200", {root!r} + "/oracle"]
+    import oracle
+    import stwo_b200 as sb
+    c = oracle.config("functional")
+    g = sb.PcsConfig(c.pow_bits, sb.FriConfig(c.log_blowup_factor, c.log_last_layer_degree_bound, c.n_queries))
+    ctx = sb.Context(0)
+    def ws(log_n, W):
+        with sb.Server(ctx, slots=1, profile=1) as p:
+            return p.wait(p.submit(sb.Statement(log_n, W), g, trace_kind=sb.TRACE_SEEDED, trace_seed=1))[1]["workspace_bytes"]
+    def ws_xor(log_n, log_table):
+        with sb.Server(ctx, slots=1, profile=1) as p:
+            return p.wait(p.submit_xor(log_n, g, seed=1, log_table=log_table))[1]["workspace_bytes"]
+    mid, big, xr = ws(15, 32), ws(16, 32), ws_xor(14, 8)
+    assert 3 * mid <= 2 * big, (mid, big)  # the budget below holds two mid-size slots
+    # Two slots warmed to the mid shape, then a larger proof: on either slot it needs more than the
+    # budget leaves while the other slot keeps its workspace.
+    with sb.Server(ctx, slots=2, profile=1, memory_budget=big + mid // 2, persistent_workspaces=True) as srv:
+        srv.warmup(15, 32, 1, 0)
+        assert srv.snapshot()["peak_workspace_bytes"] == 2 * mid  # both slots hold the mid shape
+        t = srv.submit(sb.Statement(16, 32), g, trace_kind=sb.TRACE_SEEDED, trace_seed=21)
+        proof, _ = srv.wait(t)
+        assert proof == ctx.prove_wide_fibonacci(sb.Statement(16, 32), g, trace_kind=sb.TRACE_SEEDED, trace_seed=21)
+        t = srv.submit(sb.Statement(15, 32), g, trace_kind=sb.TRACE_SEEDED, trace_seed=22)
+        srv.wait(t)
+        print("wide ok", srv.snapshot(), flush=True)
+    # An XOR-lookup proof (pool workspace) that fits once one of the two warmed slots lets go.
+    with sb.Server(ctx, slots=2, profile=1, memory_budget=2 * mid + xr - 1, persistent_workspaces=True) as srv:
+        srv.warmup(15, 32, 1, 0)
+        t = srv.submit_xor(14, g, seed=23, log_table=8)
+        proof, _ = srv.wait(t)
+        assert proof == ctx.prove_logup_xor(14, g, seed=23, log_table=8)
+        print("xor ok", srv.snapshot(), flush=True)
+    ctx.close()
+""")
+
+
+def test_serving_loop_progresses_when_warmed_slots_hold_the_budget():
+    """Persistent slots warmed to one shape, then a request that fits only after an idle slot gives
+    its workspace back. Runs in a child process so that a stalled admission fails the test by the
+    time limit instead of blocking the test run."""
+    r = subprocess.run([sys.executable, "-c", _LIVENESS.format(root=ROOT)], capture_output=True, text=True,
+                       timeout=300)
+    assert r.returncode == 0, r.stdout + r.stderr
+    assert "wide ok" in r.stdout and "xor ok" in r.stdout
