@@ -714,6 +714,204 @@ std::vector<size_t> fold_queries(const std::vector<size_t>& q) {
   return out;
 }
 
+// DEEP quotient batches (src/core/pcs/quotients/samples.zig:163-300): samples grouped by point in
+// order of first appearance, each sample a committed column (its LDE at its own log size, read at
+// the lifted index of the lifting domain) with its sampled value and random-coefficient power.
+struct QuotientSample { const uint32_t* col; uint32_t log_size; QM31 value; QM31 rp; };
+struct QuotientBatch { PointQ point; std::vector<QuotientSample> samples; };
+
+QuotientBatch& batch_for(std::vector<QuotientBatch>& batches, const PointQ& p) {
+  for (QuotientBatch& b : batches)
+    if (qeq(b.point.x, p.x) && qeq(b.point.y, p.y)) return b;
+  batches.push_back({p, {}});
+  return batches.back();
+}
+
+// Row values of the DEEP quotient on CanonicCoset(lifting), bit-reversed
+// (src/core/pcs/quotients/row_evaluation.zig:24-140,402-521; line coefficients
+// src/core/constraints.zig:87-97): per batch at point P, with a = conj(v) - v, c = conj(Py) - Py,
+// b = v c - a Py, the row (x, y) adds (sum_i rp_i c v_i(x, y) - sum_i rp_i (a y + b)) divided by
+// (Re Px - x) Im Py - (Re Py - y) Im Px.
+void quotient_columns(const std::vector<QuotientBatch>& batches, uint32_t lifting, std::vector<uint32_t> out[4]) {
+  const size_t NL = (size_t)1 << lifting;
+  struct Lc { const uint32_t* col; uint32_t log_size; QM31 c; };
+  struct Prepared { CM31 prx, pry, pix, piy; QM31 sum_a, sum_b; std::vector<Lc> lc; };
+  std::vector<Prepared> prep;
+  for (const QuotientBatch& b : batches) {
+    Prepared p;
+    p.prx = b.point.x.c0; p.pry = b.point.y.c0; p.pix = b.point.x.c1; p.piy = b.point.y.c1;
+    p.sum_a = qzero(); p.sum_b = qzero();
+    QM31 cy = qsub(qconj(b.point.y), b.point.y);
+    for (const QuotientSample& q : b.samples) {
+      QM31 a = qsub(qconj(q.value), q.value);
+      QM31 bb = qsub(qmul(q.value, cy), qmul(a, b.point.y));
+      p.sum_a = qadd(p.sum_a, qmul(q.rp, a));
+      p.sum_b = qadd(p.sum_b, qmul(q.rp, bb));
+      p.lc.push_back({q.col, q.log_size, qmul(q.rp, cy)});
+    }
+    prep.push_back(std::move(p));
+  }
+  for (int k = 0; k < 4; ++k) out[k].assign(NL, 0);
+  CircleDomain qdom = canonic_domain(lifting);
+#pragma omp parallel for schedule(static)
+  for (long long row = 0; row < (long long)NL; ++row) {
+    PointM dp = qdom.at(bit_reverse_index(row, lifting));
+    QM31 acc = qzero();
+    for (const Prepared& p : prep) {
+      QM31 num = qzero();
+      for (const Lc& l : p.lc) num = qadd(num, qmulm(l.c, l.col[lifted_index(row, lifting, l.log_size)]));
+      num = qsub(num, qadd(qmulm(p.sum_a, dp.y), p.sum_b));
+      CM31 den = csub(cmul(csub(p.prx, CM31{dp.x, 0}), p.piy), cmul(csub(p.pry, CM31{dp.y, 0}), p.pix));
+      acc = qadd(acc, qmulc(num, cinv(den)));
+    }
+    uint32_t w[4]; qstore(acc, w);
+    for (int k = 0; k < 4; ++k) out[k][row] = w[k];
+  }
+}
+
+// FRI commitment over the quotient column, the last layer, the proof of work and the queries
+// (src/prover/fri.zig:163-620, verifier order src/core/fri.zig:54-145; src/prover/pcs/scheme.zig:
+// 731-745; src/core/queries.zig:8-60).
+struct FriInner { MerkleTree tree; std::vector<uint32_t> coords[4]; };
+struct FriRun {
+  MerkleTree first_tree;
+  std::vector<FriInner> inner;
+  std::vector<QM31> last_coeffs;
+  uint64_t nonce = 0;
+  std::vector<size_t> queries;
+  bool ok = true;  // false: the last layer exceeds its degree bound
+};
+
+FriRun fri_pow_queries(Channel& ch, std::vector<uint32_t> qcol[4], uint32_t lifting, const oracle_pcs_config& cfg,
+                       int n_threads) {
+  FriRun fr;
+  const uint32_t B = cfg.log_blowup_factor;
+  CircleDomain qdom = canonic_domain(lifting);
+  std::vector<ColRef> fcols;
+  for (int k = 0; k < 4; ++k) fcols.push_back({qcol[k].data(), lifting});
+  fr.first_tree = merkle_commit(fcols);
+  ch.mix_root(fr.first_tree.root());
+  QM31 alpha = ch.draw_secure_felt();
+  // fold_circle_into_line (src/core/fri/folding.zig:558-602).
+  uint32_t line_log = lifting - 1;
+  Coset line_coset = qdom.half;  // LineDomain(halfOdds(lifting-1))
+  std::vector<uint32_t> cur[4];
+  for (int k = 0; k < 4; ++k) cur[k].assign((size_t)1 << line_log, 0);
+  {
+    size_t m = (size_t)1 << line_log;
+    std::vector<PointM> pts = qdom.half.points(m);
+    std::vector<uint32_t> py(m);
+    for (size_t i = 0; i < m; ++i) py[bit_reverse_index(i, line_log)] = pts[i].y;
+    QM31 a2 = qsq(alpha);
+    for (size_t i = 0; i < m; ++i) {
+      QM31 f0 = qfrom(qcol[0][2 * i], qcol[1][2 * i], qcol[2][2 * i], qcol[3][2 * i]);
+      QM31 f1 = qfrom(qcol[0][2 * i + 1], qcol[1][2 * i + 1], qcol[2][2 * i + 1], qcol[3][2 * i + 1]);
+      qibutterfly(f0, f1, minv(py[i]));
+      QM31 r = qadd(qmul(qzero(), a2), qadd(qmul(alpha, f1), f0));
+      uint32_t w[4]; qstore(r, w);
+      for (int k = 0; k < 4; ++k) cur[k][i] = w[k];
+    }
+  }
+  const uint32_t last_log = cfg.log_last_layer_degree_bound + B;
+  while (line_log > last_log) {
+    FriInner L;
+    for (int k = 0; k < 4; ++k) L.coords[k] = cur[k];
+    std::vector<ColRef> lcols;
+    for (int k = 0; k < 4; ++k) lcols.push_back({L.coords[k].data(), line_log});
+    L.tree = merkle_commit(lcols);
+    ch.mix_root(L.tree.root());
+    QM31 a = ch.draw_secure_felt();
+    // fold_line (src/core/fri/folding.zig:352-384).
+    size_t m = (size_t)1 << (line_log - 1);
+    std::vector<PointM> pts = line_coset.points(m);
+    std::vector<uint32_t> xs(m);
+    for (size_t i = 0; i < m; ++i) xs[bit_reverse_index(i, line_log - 1)] = pts[i].x;
+    std::vector<uint32_t> nxt[4];
+    for (int k = 0; k < 4; ++k) nxt[k].resize(m);
+    for (size_t i = 0; i < m; ++i) {
+      QM31 f0 = qfrom(cur[0][2 * i], cur[1][2 * i], cur[2][2 * i], cur[3][2 * i]);
+      QM31 f1 = qfrom(cur[0][2 * i + 1], cur[1][2 * i + 1], cur[2][2 * i + 1], cur[3][2 * i + 1]);
+      qibutterfly(f0, f1, minv(xs[i]));
+      QM31 r = qadd(f0, qmul(a, f1));
+      uint32_t w[4]; qstore(r, w);
+      for (int k = 0; k < 4; ++k) nxt[k][i] = w[k];
+    }
+    for (int k = 0; k < 4; ++k) cur[k].swap(nxt[k]);
+    fr.inner.push_back(std::move(L));
+    line_coset = line_coset.dbl();
+    line_log -= 1;
+  }
+  // Last layer: line IFFT (src/backend/line_evaluation.zig:97-145), degree check, truncate, mix.
+  {
+    size_t m = (size_t)1 << line_log;
+    std::vector<QM31> v(m);
+    for (size_t i = 0; i < m; ++i) v[i] = qfrom(cur[0][i], cur[1][i], cur[2][i], cur[3][i]);
+    bit_reverse(v);
+    Coset d = line_coset;
+    while (d.size() > 1) {
+      size_t chunk = d.size(), half = chunk / 2;
+      std::vector<PointM> pts = d.points(half);
+      for (size_t st = 0; st < m; st += chunk)
+        for (size_t i = 0; i < half; ++i) qibutterfly(v[st + i], v[st + half + i], minv(pts[i].x));
+      d = d.dbl();
+    }
+    uint32_t li = minv((uint32_t)(m % P));
+    for (QM31& x : v) x = qmulm(x, li);
+    bit_reverse(v);  // ordered coefficients
+    size_t bound = (size_t)1 << cfg.log_last_layer_degree_bound;
+    for (size_t i = bound; i < m; ++i)
+      if (!qiszero(v[i])) { fr.ok = false; return fr; }  // InvalidLastLayerDegree
+    fr.last_coeffs.assign(v.begin(), v.begin() + bound);
+    bit_reverse(fr.last_coeffs);
+    ch.mix_felts(fr.last_coeffs);
+  }
+  fr.nonce = pow_grind(ch.digest, cfg.pow_bits, n_threads);
+  ch.mix_u64(fr.nonce);
+  uint32_t mask = (1u << lifting) - 1;
+  while (fr.queries.size() < cfg.n_queries) {
+    auto w = ch.draw_u32s();
+    for (uint32_t x : w) { fr.queries.push_back(x & mask); if (fr.queries.size() == cfg.n_queries) break; }
+  }
+  std::sort(fr.queries.begin(), fr.queries.end());
+  fr.queries.erase(std::unique(fr.queries.begin(), fr.queries.end()), fr.queries.end());
+  return fr;
+}
+
+// Trace-tree decommitments and the FRI proof in wire order: "decommitments", "queried_values",
+// "proof_of_work", "fri_proof" (src/interop/proof_wire.zig:19-77, src/prover/fri.zig:624-850).
+void json_decommit_and_fri(Json& j, const std::vector<const Decommitment*>& ds, FriRun& fr,
+                           std::vector<uint32_t> qcol[4]) {
+  j.s += "\"decommitments\":[";
+  for (size_t t = 0; t < ds.size(); ++t) { if (t) j.s += ','; j.s += "{\"hash_witness\":"; j.hashes(ds[t]->witness); j.s += '}'; }
+  j.s += "],\"queried_values\":[";
+  for (size_t t = 0; t < ds.size(); ++t) {
+    if (t) j.s += ',';
+    j.s += '[';
+    for (size_t c = 0; c < ds[t]->queried.size(); ++c) {
+      if (c) j.s += ',';
+      j.s += '[';
+      for (size_t q = 0; q < ds[t]->queried[c].size(); ++q) { if (q) j.s += ','; j.u(ds[t]->queried[c][q]); }
+      j.s += ']';
+    }
+    j.s += ']';
+  }
+  j.s += "],\"proof_of_work\":"; j.u(fr.nonce);
+  FriLayerProof first_proof = fri_decommit_layer(fr.first_tree, qcol, fr.queries);
+  std::vector<FriLayerProof> inner_proofs;
+  std::vector<size_t> lq = fold_queries(fr.queries);
+  for (FriInner& L : fr.inner) { inner_proofs.push_back(fri_decommit_layer(L.tree, L.coords, lq)); lq = fold_queries(lq); }
+  auto layer = [&](const FriLayerProof& L) {
+    j.s += "{\"fri_witness\":"; j.qms(L.witness);
+    j.s += ",\"decommitment\":{\"hash_witness\":"; j.hashes(L.hash_witness);
+    j.s += "},\"commitment\":"; j.hash(L.commitment); j.s += '}';
+  };
+  j.s += ",\"fri_proof\":{\"first_layer\":"; layer(first_proof);
+  j.s += ",\"inner_layers\":[";
+  for (size_t i = 0; i < inner_proofs.size(); ++i) { if (i) j.s += ','; layer(inner_proofs[i]); }
+  j.s += "],\"last_layer_poly\":"; j.qms(fr.last_coeffs);
+  j.s += "}";
+}
+
 struct ProveParams {
   uint32_t log_n, W;
   oracle_pcs_config cfg;
@@ -822,150 +1020,25 @@ std::string prove_wide_fib(const ProveParams& pp, const uint32_t* trace) {
   }
   QM31 quot_coeff = ch.draw_secure_felt();
 
-  // DEEP quotients on the lifting domain (src/core/pcs/quotients/row_evaluation.zig,
-  // samples.zig): one batch at the OODS point with all W+8 columns, powers 1, a, a^2, ...
-  const uint32_t n_q = W + 8;
-  std::vector<QM31> lc_a(n_q), lc_b(n_q), lc_c(n_q);
+  // DEEP quotients on the lifting domain: one batch at the OODS point with all W+8 columns,
+  // powers 1, a, a^2, ... in column order.
+  std::vector<QuotientBatch> batches;
   {
     QM31 rp = qone();
-    PointQ pc = {qconj(oods.x), qconj(oods.y)};
-    for (uint32_t i = 0; i < n_q; ++i) {
-      QM31 v = i < W ? sampled_main[i] : sampled_comp[i - W];
-      QM31 a = qsub(qconj(v), v);
-      QM31 c = qsub(pc.y, oods.y);
-      QM31 b = qsub(qmul(v, c), qmul(a, oods.y));
-      lc_a[i] = qmul(rp, a); lc_b[i] = qmul(rp, b); lc_c[i] = qmul(rp, c);
-      rp = qmul(rp, quot_coeff);
-    }
+    QuotientBatch& b = batch_for(batches, oods);
+    for (uint32_t c = 0; c < W; ++c) { b.samples.push_back({lde[c].data(), LDE, sampled_main[c], rp}); rp = qmul(rp, quot_coeff); }
+    for (int k = 0; k < 8; ++k) { b.samples.push_back({comp_lde[k].data(), LDE, sampled_comp[k], rp}); rp = qmul(rp, quot_coeff); }
   }
-  QM31 sum_a = qzero(), sum_b = qzero();
-  for (uint32_t i = 0; i < n_q; ++i) { sum_a = qadd(sum_a, lc_a[i]); sum_b = qadd(sum_b, lc_b[i]); }
-  CircleDomain qdom = canonic_domain(lifting);
   std::vector<uint32_t> qcol[4];
-  for (int k = 0; k < 4; ++k) qcol[k].resize(NL);
-  CM31 prx = oods.x.c0, pry = oods.y.c0, pix = oods.x.c1, piy = oods.y.c1;
-#pragma omp parallel for schedule(static)
-  for (long long row = 0; row < (long long)NL; ++row) {
-    PointM dp = qdom.at(bit_reverse_index(row, lifting));
-    QM31 num = qzero();
-    for (uint32_t i = 0; i < n_q; ++i) {
-      uint32_t v = i < W ? lde[i][row] : comp_lde[i - W][row];
-      num = qadd(num, qmulm(lc_c[i], v));
-    }
-    num = qsub(num, qadd(qmulm(sum_a, dp.y), sum_b));
-    CM31 den = csub(cmul(csub(prx, CM31{dp.x, 0}), piy), cmul(csub(pry, CM31{dp.y, 0}), pix));
-    QM31 r = qmulc(num, cinv(den));
-    uint32_t w[4]; qstore(r, w);
-    for (int k = 0; k < 4; ++k) qcol[k][row] = w[k];
-  }
+  quotient_columns(batches, lifting, qcol);
 
-  // FRI commit (src/prover/fri.zig:163-620; verifier order src/core/fri.zig:54-145).
-  std::vector<ColRef> fcols;
-  for (int k = 0; k < 4; ++k) fcols.push_back({qcol[k].data(), lifting});
-  MerkleTree first_tree = merkle_commit(fcols);
-  ch.mix_root(first_tree.root());
-  QM31 alpha = ch.draw_secure_felt();
-  // fold_circle_into_line (src/core/fri/folding.zig:558-602).
-  uint32_t line_log = lifting - 1;
-  Coset line_coset = qdom.half;  // LineDomain(halfOdds(lifting-1))
-  std::vector<uint32_t> cur[4];
-  for (int k = 0; k < 4; ++k) cur[k].assign((size_t)1 << line_log, 0);
-  {
-    size_t m = (size_t)1 << line_log;
-    std::vector<PointM> pts = qdom.half.points(m);
-    std::vector<uint32_t> py(m);
-    for (size_t i = 0; i < m; ++i) py[bit_reverse_index(i, line_log)] = pts[i].y;
-    QM31 a2 = qsq(alpha);
-    for (size_t i = 0; i < m; ++i) {
-      QM31 f0 = qfrom(qcol[0][2 * i], qcol[1][2 * i], qcol[2][2 * i], qcol[3][2 * i]);
-      QM31 f1 = qfrom(qcol[0][2 * i + 1], qcol[1][2 * i + 1], qcol[2][2 * i + 1], qcol[3][2 * i + 1]);
-      qibutterfly(f0, f1, minv(py[i]));
-      QM31 r = qadd(qmul(qzero(), a2), qadd(qmul(alpha, f1), f0));
-      uint32_t w[4]; qstore(r, w);
-      for (int k = 0; k < 4; ++k) cur[k][i] = w[k];
-    }
-  }
-  const uint32_t last_log = pp.cfg.log_last_layer_degree_bound + B;
-  struct Inner { MerkleTree tree; std::vector<uint32_t> coords[4]; };
-  std::vector<Inner> inner;
-  while (line_log > last_log) {
-    Inner L;
-    for (int k = 0; k < 4; ++k) L.coords[k] = cur[k];
-    std::vector<ColRef> lcols;
-    for (int k = 0; k < 4; ++k) lcols.push_back({L.coords[k].data(), line_log});
-    L.tree = merkle_commit(lcols);
-    ch.mix_root(L.tree.root());
-    QM31 a = ch.draw_secure_felt();
-    // fold_line (src/core/fri/folding.zig:352-384).
-    size_t m = (size_t)1 << (line_log - 1);
-    std::vector<PointM> pts = line_coset.points(m);
-    std::vector<uint32_t> xs(m);
-    for (size_t i = 0; i < m; ++i) xs[bit_reverse_index(i, line_log - 1)] = pts[i].x;
-    std::vector<uint32_t> nxt[4];
-    for (int k = 0; k < 4; ++k) nxt[k].resize(m);
-    for (size_t i = 0; i < m; ++i) {
-      QM31 f0 = qfrom(cur[0][2 * i], cur[1][2 * i], cur[2][2 * i], cur[3][2 * i]);
-      QM31 f1 = qfrom(cur[0][2 * i + 1], cur[1][2 * i + 1], cur[2][2 * i + 1], cur[3][2 * i + 1]);
-      qibutterfly(f0, f1, minv(xs[i]));
-      QM31 r = qadd(f0, qmul(a, f1));
-      uint32_t w[4]; qstore(r, w);
-      for (int k = 0; k < 4; ++k) nxt[k][i] = w[k];
-    }
-    for (int k = 0; k < 4; ++k) cur[k].swap(nxt[k]);
-    inner.push_back(std::move(L));
-    line_coset = line_coset.dbl();
-    line_log -= 1;
-  }
-  // Last layer: line IFFT (src/backend/line_evaluation.zig:97-145), degree check, truncate, mix.
-  std::vector<QM31> last_coeffs;
-  {
-    size_t m = (size_t)1 << line_log;
-    std::vector<QM31> v(m);
-    for (size_t i = 0; i < m; ++i) v[i] = qfrom(cur[0][i], cur[1][i], cur[2][i], cur[3][i]);
-    bit_reverse(v);
-    Coset d = line_coset;
-    while (d.size() > 1) {
-      size_t chunk = d.size(), half = chunk / 2;
-      std::vector<PointM> pts = d.points(half);
-      for (size_t st = 0; st < m; st += chunk)
-        for (size_t i = 0; i < half; ++i) qibutterfly(v[st + i], v[st + half + i], minv(pts[i].x));
-      d = d.dbl();
-    }
-    uint32_t li = minv((uint32_t)(m % P));
-    for (QM31& x : v) x = qmulm(x, li);
-    bit_reverse(v);  // ordered coefficients
-    size_t bound = (size_t)1 << pp.cfg.log_last_layer_degree_bound;
-    for (size_t i = bound; i < m; ++i)
-      if (!qiszero(v[i])) return std::string();  // InvalidLastLayerDegree
-    last_coeffs.assign(v.begin(), v.begin() + bound);
-    bit_reverse(last_coeffs);
-    ch.mix_felts(last_coeffs);
-  }
-
-  // PoW, then queries (src/prover/pcs/scheme.zig:731-745, src/core/queries.zig:8-60).
-  uint64_t nonce = pow_grind(ch.digest, pp.cfg.pow_bits, pp.n_threads);
-  ch.mix_u64(nonce);
-  std::vector<size_t> queries;
-  {
-    uint32_t mask = (1u << lifting) - 1;
-    while (queries.size() < pp.cfg.n_queries) {
-      auto w = ch.draw_u32s();
-      for (uint32_t x : w) { queries.push_back(x & mask); if (queries.size() == pp.cfg.n_queries) break; }
-    }
-    std::sort(queries.begin(), queries.end());
-    queries.erase(std::unique(queries.begin(), queries.end()), queries.end());
-  }
-
-  // FRI decommit.
-  FriLayerProof first_proof = fri_decommit_layer(first_tree, qcol, queries);
-  std::vector<FriLayerProof> inner_proofs;
-  std::vector<size_t> lq = fold_queries(queries);
-  for (Inner& L : inner) { inner_proofs.push_back(fri_decommit_layer(L.tree, L.coords, lq)); lq = fold_queries(lq); }
+  FriRun fr = fri_pow_queries(ch, qcol, lifting, pp.cfg, pp.n_threads);
+  if (!fr.ok) return std::string();
 
   // Trace decommit (tree 0 has no columns and no positions).
   Decommitment d0 = merkle_decommit(t0, {}, {});
-  Decommitment d1 = merkle_decommit(t1, main_cols, queries);
-  Decommitment d2 = merkle_decommit(t2, comp_cols, queries);
+  Decommitment d1 = merkle_decommit(t1, main_cols, fr.queries);
+  Decommitment d2 = merkle_decommit(t2, comp_cols, fr.queries);
 
   // Wire encoding.
   Json j;
@@ -979,32 +1052,9 @@ std::string prove_wide_fib(const ProveParams& pp, const uint32_t* trace) {
   for (uint32_t c = 0; c < W; ++c) { if (c) j.s += ','; j.s += '['; j.qm(sampled_main[c]); j.s += ']'; }
   j.s += "],[";
   for (int c = 0; c < 8; ++c) { if (c) j.s += ','; j.s += '['; j.qm(sampled_comp[c]); j.s += ']'; }
-  j.s += "]],\"decommitments\":[";
-  const Decommitment* ds[3] = {&d0, &d1, &d2};
-  for (int t = 0; t < 3; ++t) { if (t) j.s += ','; j.s += "{\"hash_witness\":"; j.hashes(ds[t]->witness); j.s += '}'; }
-  j.s += "],\"queried_values\":[";
-  for (int t = 0; t < 3; ++t) {
-    if (t) j.s += ',';
-    j.s += '[';
-    for (size_t c = 0; c < ds[t]->queried.size(); ++c) {
-      if (c) j.s += ',';
-      j.s += '[';
-      for (size_t q = 0; q < ds[t]->queried[c].size(); ++q) { if (q) j.s += ','; j.u(ds[t]->queried[c][q]); }
-      j.s += ']';
-    }
-    j.s += ']';
-  }
-  j.s += "],\"proof_of_work\":"; j.u(nonce);
-  auto layer = [&](const FriLayerProof& L) {
-    j.s += "{\"fri_witness\":"; j.qms(L.witness);
-    j.s += ",\"decommitment\":{\"hash_witness\":"; j.hashes(L.hash_witness);
-    j.s += "},\"commitment\":"; j.hash(L.commitment); j.s += '}';
-  };
-  j.s += ",\"fri_proof\":{\"first_layer\":"; layer(first_proof);
-  j.s += ",\"inner_layers\":[";
-  for (size_t i = 0; i < inner_proofs.size(); ++i) { if (i) j.s += ','; layer(inner_proofs[i]); }
-  j.s += "],\"last_layer_poly\":"; j.qms(last_coeffs);
-  j.s += "}}";
+  j.s += "]],";
+  json_decommit_and_fri(j, {&d0, &d1, &d2}, fr, qcol);
+  j.s += "}";
 
   // Prover self-check of the composition OODS value (src/prover/prove.zig:366-386).
   {

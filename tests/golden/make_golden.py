@@ -8,7 +8,7 @@ and the known-answer values in the reference's tests, and writes:
                        SHA-256 of the JSON wire bytes (plus the full bytes for the 2^10 x 8 proof)
   kats.json            Blake2s / Merkle / proof known answers quoted in the reference's tests
 
-Usage: python tests/golden/make_golden.py [/path/to/stwo-zig]
+Usage: python tests/golden/make_golden.py /path/to/stwo-zig
 """
 from __future__ import annotations
 
@@ -81,4 +81,6 @@ def main(ref_root: str) -> None:
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    if len(sys.argv) != 2:
+        sys.exit(__doc__)
+    main(sys.argv[1])

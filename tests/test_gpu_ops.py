@@ -1,4 +1,6 @@
 """Op-level parity of the CUDA kernels (through the C ABI) against the CPU oracle."""
+import json
+import os
 import struct
 
 import numpy as np
@@ -144,6 +146,18 @@ def test_pow_grind_lowest_nonce_across_waves_and_rounds(ctx):
         assert got == oracle.pow_grind(digest, 24), i
         found.append(got)
     assert max(found) > 4_300_000  # at least one beyond the first wave of CTAs
+
+
+POW_VECTORS = json.load(open(os.path.join(os.path.dirname(__file__), "golden", "pow_vectors.json")))
+
+
+@pytest.mark.parametrize("vec", POW_VECTORS, ids=lambda v: f"{v['n_bits']}bits-{v['digest'][:8]}")
+def test_pow_grind_above_32_bits(ctx, vec):
+    """More than 32 bits: a hit must also zero the second hash word (the 128-bit trailing-zero
+    path). The fixture's nonces are the oracle's (tests/test_oracle.py pins them on the CPU)."""
+    digest = bytes.fromhex(vec["digest"])
+    prefix = oracle.blake2s(struct.pack("<I", 0x12345678) + b"\0" * 12 + digest + struct.pack("<I", vec["n_bits"]))
+    assert ctx.pow_grind(prefix, vec["n_bits"]) == vec["nonce"]
 
 
 def test_bad_arguments_raise(ctx):

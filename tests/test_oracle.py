@@ -74,6 +74,16 @@ def test_extension_agrees_with_evaluation():
     assert np.array_equal(back[: c.size], c) and not back[c.size:].any()
 
 
+POW_VECTORS = json.load(open(os.path.join(GOLDEN, "pow_vectors.json")))
+
+
+@pytest.mark.parametrize("vec", POW_VECTORS, ids=lambda v: f"{v['n_bits']}bits-{v['digest'][:8]}")
+def test_pow_vectors_above_32_bits(vec):
+    """The fixture's lowest nonces at 33 and 34 bits (made on the GPU by
+    tests/golden/make_pow_vectors.py), confirmed by the oracle scanning every smaller nonce."""
+    assert oracle.pow_grind(bytes.fromhex(vec["digest"]), vec["n_bits"]) == vec["nonce"]
+
+
 def test_pow_grind_is_lowest_valid_nonce():
     digest = bytes(range(32))
     nonce = oracle.pow_grind(digest, 8, 4)
