@@ -131,13 +131,34 @@ class ClockSampler:
         return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
 
 
-def cpu_oracle_prove(log_n, width, preset, seed, n_threads=0):
+def cpu_oracle_prove(log_n, width, preset, seed, n_threads=0, trace_kind=1):
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle
     t = time.perf_counter()
-    proof = oracle.prove_wide_fib(log_n, width, oracle.config(preset), trace_kind=1, trace_seed=seed,
+    proof = oracle.prove_wide_fib(log_n, width, oracle.config(preset), trace_kind=trace_kind, trace_seed=seed,
                                   n_threads=n_threads)
     return time.perf_counter() - t, proof
+
+
+def cpu_oracle_pow_seconds():
+    import oracle
+    return oracle.last_pow_seconds()
+
+
+# The reference's published CPU times of its own benchmark shape (functional preset, 2^20 x 100, the
+# (1, row) trace), Apple M5 Max, 18 threads: vectors/reports/benchmark_history/runs/
+# 2026-07-21-192442-matrix-v6-483bca66/report.json and autoresearch/ledger/promotions.tsv:112.
+REFERENCE_PUBLISHED_FUNCTIONAL_MS = {"apple_m5_max_cpu_simd_18_threads": [870.1, 332.8]}
+
+
+def cpu_calibration(log_n, width):
+    """The port on the shape and preset the reference publishes: two functional proofs of the
+    reference's own (1, row) trace (the second is timed), beside the published numbers."""
+    cpu_oracle_prove(log_n, width, "functional", 0, trace_kind=0)
+    dt, _ = cpu_oracle_prove(log_n, width, "functional", 0, trace_kind=0)
+    return {"functional_ms": 1e3 * dt, "functional_pow_ms": 1e3 * cpu_oracle_pow_seconds(),
+            "functional_shape": f"2^{log_n}x{width}, functional preset, (1, row) trace",
+            "reference_published_functional_ms": REFERENCE_PUBLISHED_FUNCTIONAL_MS}
 
 
 def run_reference(args, rank, world):
@@ -148,10 +169,11 @@ def run_reference(args, rank, world):
     cores = os.cpu_count() or 1
     for i in range(args.warmup):
         cpu_oracle_prove(args.log_n, args.width, args.preset, 10_000 + i)
-    times = []
+    times, pow_s = [], []
     for i in range(args.steps):
         dt, _ = cpu_oracle_prove(args.log_n, args.width, args.preset, 20_000 + i)
         times.append(dt)
+        pow_s.append(cpu_oracle_pow_seconds())
     total = sum(times)
     value = args.steps / total
     out = {
@@ -163,9 +185,11 @@ def run_reference(args, rank, world):
         "p50_ms": 1e3 * pct(times, 50), "p99_ms": 1e3 * pct(times, 99),
         "cpu_baseline": {"value": value, "unit": "proofs/s", "cores": cores, "kind": "port",
                          "sample": f"{args.steps} full {args.preset} proofs of 2^{args.log_n}x{args.width}, "
-                                   "C++ restatement of the reference CPU prover, all host threads"},
+                                   "C++ restatement of the reference CPU prover, all host threads",
+                         "pow_ms": 1e3 * statistics.mean(pow_s)},
         "e2e": {"value": value, "unit": "proofs/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
+    out["cpu_baseline"].update(cpu_calibration(args.log_n, args.width))
     print(json.dumps(out), flush=True)
 
 
@@ -443,10 +467,11 @@ def main():
         out["roofline_issue"]["frac"] = out["roofline_issue"]["achieved"] / out["roofline_issue"]["peak"]
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         n_cpu = min(3, n_traces)
-        total, same = 0.0, True
+        total, same, pow_s = 0.0, True, []
         for i in range(n_cpu):
             dt, ref = cpu_oracle_prove(args.log_n, args.width, args.preset, seeds[i])
             total += dt
+            pow_s.append(cpu_oracle_pow_seconds())
             same &= ref == proofs_b[i]
         out["cpu_baseline"] = {"value": n_cpu / total, "unit": "proofs/s", "cores": os.cpu_count() or 1,
                                "kind": "port",
@@ -454,6 +479,8 @@ def main():
                                          f"steps 0..{n_cpu - 1}, {total:.1f} s), C++ restatement of the reference CPU "
                                          "prover, all host threads"}
         out["cpu_baseline"]["proof_identical"] = bool(same)
+        out["cpu_baseline"]["pow_ms"] = 1e3 * statistics.mean(pow_s)
+        out["cpu_baseline"].update(cpu_calibration(args.log_n, args.width))
     if rank == 0:
         print(json.dumps(out), flush=True)
     if world > 1:

@@ -17,6 +17,7 @@
 
 #include <algorithm>
 #include <array>
+#include <chrono>
 #include <atomic>
 #include <cstdint>
 #include <cstring>
@@ -558,9 +559,16 @@ Decommitment merkle_decommit(const MerkleTree& t, const std::vector<ColRef>& col
     for (size_t j = 0; j < positions.size(); ++j) q[j] = c.data[lifted_index(positions[j], t.max_log, c.log_size)];
     d.queried.push_back(std::move(q));
   }
-  std::vector<size_t> prev;
-  for (size_t i = 0; i < positions.size(); ++i)
-    if (i == 0 || positions[i - 1] != positions[i]) prev.push_back(positions[i]);
+  // The witness covers the sorted unique positions, the order in which the reference verifier
+  // walks them (src/core/vcs_lifted/verifier.zig:109-138). The reference prover walks the positions
+  // as given, dropping only adjacent repeats (src/prover/vcs_lifted/decommit.zig:166-176): the same
+  // witness for sorted positions (every trace tree and FRI layer), but not for the preprocessed
+  // positions of a tree smaller than the lifting domain, which preparePreprocessedQueryPositions can
+  // leave out of order (src/core/pcs/utils.zig:292-314) and which only a proof the verifier accepts
+  // may carry.
+  std::vector<size_t> prev(positions);
+  std::sort(prev.begin(), prev.end());
+  prev.erase(std::unique(prev.begin(), prev.end()), prev.end());
   for (int layer = (int)t.max_log - 1; layer >= 0; --layer) {
     const std::vector<Hash>& child = t.layers[layer + 1];
     std::vector<size_t> cur;
@@ -772,6 +780,9 @@ void quotient_columns(const std::vector<QuotientBatch>& batches, uint32_t liftin
 // FRI commitment over the quotient column, the last layer, the proof of work and the queries
 // (src/prover/fri.zig:163-620, verifier order src/core/fri.zig:54-145; src/prover/pcs/scheme.zig:
 // 731-745; src/core/queries.zig:8-60).
+// Wall time of the last proof's proof-of-work grind (reported beside the CPU baseline).
+double& last_pow_seconds() { static thread_local double s = 0; return s; }
+
 struct FriInner { MerkleTree tree; std::vector<uint32_t> coords[4]; };
 struct FriRun {
   MerkleTree first_tree;
@@ -865,7 +876,9 @@ FriRun fri_pow_queries(Channel& ch, std::vector<uint32_t> qcol[4], uint32_t lift
     bit_reverse(fr.last_coeffs);
     ch.mix_felts(fr.last_coeffs);
   }
+  const auto t_pow = std::chrono::steady_clock::now();
   fr.nonce = pow_grind(ch.digest, cfg.pow_bits, n_threads);
+  last_pow_seconds() = std::chrono::duration<double>(std::chrono::steady_clock::now() - t_pow).count();
   ch.mix_u64(fr.nonce);
   uint32_t mask = (1u << lifting) - 1;
   while (fr.queries.size() < cfg.n_queries) {
@@ -1077,6 +1090,291 @@ std::string prove_wide_fib(const ProveParams& pp, const uint32_t* trace) {
   return j.s;
 }
 
+// ---------------------------------------------------------------------------
+// LogUp XOR-lookup AIR (no reference AIR exists; it is built from the reference's pieces): a main
+// component of 2^n lookups (a, b, c = a ^ b of w = t/2-bit operands) and a table component of 2^t
+// rows (ta, tb, ta ^ tb with multiplicities m), each at its own size under the lifted PCS
+// (columns of several sizes in one tree, src/prover/vcs_lifted/leaves.zig:104-115). The LogUp
+// columns are the coset-order cumulative sums with the total/N shift of
+// src/tests/metal/backend/commitment_test.zig:73-154 (oracle_logup_interaction below); the PCS
+// samples, quotient batches and periodicity samples follow src/core/pcs/quotients/samples.zig:
+// 163-300; the preprocessed tree is queried at src/core/pcs/utils.zig:292-314's positions; the FRI,
+// proof-of-work, query and decommitment tail is the wide-Fibonacci one. Transcript:
+//   config; tree 0 (ta, tb, tc); tree 1 (a, b, c, m); statement (n, t); [channel seed];
+//   z, alpha; tree 2 (S_M, S_T: 4 coordinate columns each); claimed sums;
+//   random_coeff; tree 3 (composition halves); OODS point; sampled values; quotient coefficient;
+//   FRI; last layer; PoW; queries.
+// Constraints (cyclic thanks to the shift), with d = a + alpha b + alpha^2 c - z at a row and
+// S(x g^-1) the previous row at the component's size:
+//   C_M = (S_M(x) - S_M(x g^-1) + claimed_M / 2^n) d_M(x) - 1
+//   C_T = (S_T(x) - S_T(x g^-1) + claimed_T / 2^t) d_T(x) + m(x)
+// composed as random_coeff C_M / Z_M + C_T / Z_T on CanonicCoset(L + 1), L = max(n, t), each
+// component entering through the lifting map.
+// ---------------------------------------------------------------------------
+struct XorParams {
+  uint32_t log_n, log_table;
+  oracle_pcs_config cfg;
+  uint64_t seed;
+  bool has_channel_seed;
+  uint64_t channel_seed;
+  int n_threads;
+};
+
+// Storage position (bit-reversed circle order) of logical coset row k at size 2^log.
+inline size_t storage_of_row(size_t k, uint32_t log) {
+  size_t n = (size_t)1 << log;
+  size_t ci = (k & 1) == 0 ? k / 2 : n - 1 - k / 2;
+  return bit_reverse_index(ci, log);
+}
+
+std::string prove_logup_xor(const XorParams& xp) {
+  const uint32_t n = xp.log_n, t = xp.log_table, B = xp.cfg.log_blowup_factor;
+  const uint32_t L = std::max(n, t), LDE = L + B, CL = L + 1;
+  const size_t NC = (size_t)1 << CL;
+  const uint32_t w = t / 2, wmask = (1u << w) - 1;
+  // Columns: tree 0 (0-2: ta, tb, tc), tree 1 (3-5: a, b, c; 6: m), tree 2 (7-10: S_M; 11-14: S_T).
+  enum { TA = 0, A = 3, M = 6, SM = 7, ST = 11, NCOLS = 15 };
+  struct Col { uint32_t log; std::vector<uint32_t> vals, coeffs, lde, evc; };
+  std::vector<Col> col(NCOLS);
+  for (int c = 0; c < NCOLS; ++c) col[c].log = (c < A || c == M || c >= ST) ? t : n;
+  for (Col& c : col) c.vals.assign((size_t)1 << c.log, 0);
+
+  // Trace: main rows are seeded by their logical (coset-order) row k: SplitMix64 of
+  // seed ^ (0xD6E8FEB86659FD93 (k + 1)), a = low w bits, b = w bits from bit 8; table row k holds
+  // ta = k >> w, tb = k & (2^w - 1) (the bitwise table layout of
+  // src/frontends/riscv/air/preprocessed/bitwise.zig:17-35) and the count of main rows (ta, tb).
+  std::vector<uint32_t> hist((size_t)1 << t, 0);
+  for (size_t s = 0; s < ((size_t)1 << n); ++s) {
+    uint64_t state = xp.seed ^ (0xD6E8FEB86659FD93ull * ((uint64_t)logical_row(n, s) + 1));
+    uint64_t x = splitmix64(state);
+    uint32_t a = (uint32_t)x & wmask, b = (uint32_t)(x >> 8) & wmask;
+    col[A].vals[s] = a; col[A + 1].vals[s] = b; col[A + 2].vals[s] = a ^ b;
+    ++hist[(a << w) | b];
+  }
+  for (size_t s = 0; s < ((size_t)1 << t); ++s) {
+    size_t k = logical_row(t, s);
+    uint32_t ta = (uint32_t)(k >> w), tb = (uint32_t)k & wmask;
+    col[TA].vals[s] = ta; col[TA + 1].vals[s] = tb; col[TA + 2].vals[s] = ta ^ tb;
+    col[M].vals[s] = hist[k];
+  }
+
+  std::vector<Twiddles> tw(LDE + 2);
+  std::vector<bool> have(LDE + 2, false);
+  auto twiddles = [&](uint32_t log) -> const Twiddles& {
+    if (!have[log]) { tw[log] = make_twiddles(canonic_domain(log).half); have[log] = true; }
+    return tw[log];
+  };
+  // Coefficients, own-size LDE (blowup B) and own-size evaluation on CanonicCoset(log + 1).
+  auto prepare = [&](int first, int count) {
+    for (int c = first; c < first + count; ++c) {
+      Col& k = col[c];
+      k.coeffs = k.vals;
+      circle_interpolate(k.coeffs.data(), canonic_domain(k.log), twiddles(k.log));
+      k.lde.resize((size_t)1 << (k.log + B));
+      circle_extend(k.coeffs.data(), k.log, B, k.lde.data(), twiddles(k.log + B));
+      if (B == 1) { k.evc = k.lde; continue; }
+      k.evc.resize((size_t)2 << k.log);
+      circle_extend(k.coeffs.data(), k.log, 1, k.evc.data(), twiddles(k.log + 1));
+    }
+  };
+  auto refs = [&](int first, int count) {
+    std::vector<ColRef> r;
+    for (int c = first; c < first + count; ++c) r.push_back({col[c].lde.data(), col[c].log + B});
+    return r;
+  };
+
+  Channel ch;
+  ch.mix_felts({qfrom(xp.cfg.pow_bits, B, xp.cfg.n_queries, xp.cfg.log_last_layer_degree_bound)});
+  prepare(TA, 3);
+  MerkleTree t0 = merkle_commit(refs(TA, 3));
+  ch.mix_root(t0.root());
+  prepare(A, 4);
+  MerkleTree t1 = merkle_commit(refs(A, 4));
+  ch.mix_root(t1.root());
+  ch.mix_u32s({n, t});
+  if (xp.has_channel_seed) ch.mix_u64(xp.channel_seed);
+
+  // Interaction: each component's LogUp column at its own size.
+  const QM31 z = ch.draw_secure_felt();
+  const QM31 alpha = ch.draw_secure_felt();
+  const QM31 alpha2 = qsq(alpha);
+  QM31 claimed[2];
+  {
+    uint32_t alphas[12];
+    qstore(qone(), alphas); qstore(alpha, alphas + 4); qstore(alpha2, alphas + 8);
+    uint32_t zw[4]; qstore(z, zw);
+    for (int comp = 0; comp < 2; ++comp) {
+      const int words0 = comp == 0 ? A : TA, out0 = comp == 0 ? SM : ST;
+      const uint32_t log = col[words0].log;
+      oracle_logup_use u{};
+      u.n_words = 3;
+      for (int j = 0; j < 3; ++j) u.words[j] = col[words0 + j].vals.data();
+      u.multiplicity = comp == 0 ? nullptr : col[M].vals.data();
+      u.negate = comp == 0 ? 0 : 1;
+      std::vector<uint32_t> out((size_t)4 << log);
+      uint32_t cw[4];
+      int rc = oracle_logup_interaction(log, 1, &u, alphas, zw, 1, 1, out.data(), cw);
+      if (rc != 0) return std::string("DIVISION_BY_ZERO");
+      claimed[comp] = qload(cw);
+      for (int k = 0; k < 4; ++k)
+        col[out0 + k].vals.assign(out.begin() + ((size_t)k << log), out.begin() + ((size_t)(k + 1) << log));
+    }
+  }
+  prepare(SM, 8);
+  MerkleTree t2 = merkle_commit(refs(SM, 8));
+  ch.mix_root(t2.root());
+  ch.mix_felts({claimed[0], claimed[1]});
+
+  // Composition on CanonicCoset(L + 1).
+  const QM31 random_coeff = ch.draw_secure_felt();
+  std::vector<uint32_t> comp[4];
+  for (int k = 0; k < 4; ++k) comp[k].resize(NC);
+  {
+    const QM31 shift[2] = {qmulm(claimed[0], minv((uint32_t)(((size_t)1 << n) % P))),
+                           qmulm(claimed[1], minv((uint32_t)(((size_t)1 << t) % P)))};
+    uint32_t den[2][2];
+    for (int c = 0; c < 2; ++c) {
+      const uint32_t k = c == 0 ? n : t;
+      CircleDomain cd = canonic_domain(k + 1);
+      Coset trace = coset_odds(k);
+      den[c][0] = minv(coset_vanishing_m(trace, cd.at(0)));
+      den[c][1] = minv(coset_vanishing_m(trace, cd.at(1)));
+    }
+    auto at = [&](int c, size_t r) { return col[c].evc[lifted_index(r, CL, col[c].log + 1)]; };
+    auto sec = [&](int c0, size_t r) { return qfrom(at(c0, r), at(c0 + 1, r), at(c0 + 2, r), at(c0 + 3, r)); };
+#pragma omp parallel for schedule(static)
+    for (long long rr = 0; rr < (long long)NC; ++rr) {
+      const size_t r = (size_t)rr;
+      const size_t rp = storage_of_row((logical_row(CL, r) + NC - 2) % NC, CL);  // x g_L^-1
+      const QM31 d_main = qsub(qadd(qadd(qbase(at(A, r)), qmulm(alpha, at(A + 1, r))), qmulm(alpha2, at(A + 2, r))), z);
+      const QM31 d_table =
+          qsub(qadd(qadd(qbase(at(TA, r)), qmulm(alpha, at(TA + 1, r))), qmulm(alpha2, at(TA + 2, r))), z);
+      const QM31 c_main = qsub(qmul(qadd(qsub(sec(SM, r), sec(SM, rp)), shift[0]), d_main), qone());
+      const QM31 c_table = qadd(qmul(qadd(qsub(sec(ST, r), sec(ST, rp)), shift[1]), d_table), qbase(at(M, r)));
+      const size_t h = r >> L;
+      const QM31 q = qadd(qmulm(qmul(random_coeff, c_main), den[0][h]), qmulm(c_table, den[1][h]));
+      uint32_t wq[4]; qstore(q, wq);
+      for (int k = 0; k < 4; ++k) comp[k][r] = wq[k];
+    }
+  }
+  // Interpolate, split at mid (left = first 2^L coefficients), extend, commit as tree 3.
+  std::vector<std::vector<uint32_t>> comp_coeffs(8, std::vector<uint32_t>((size_t)1 << L)),
+      comp_lde(8, std::vector<uint32_t>((size_t)1 << LDE));
+  for (int k = 0; k < 4; ++k) {
+    std::vector<uint32_t> tmp = comp[k];
+    circle_interpolate(tmp.data(), canonic_domain(CL), twiddles(CL));
+    std::memcpy(comp_coeffs[k].data(), tmp.data(), ((size_t)4) << L);
+    std::memcpy(comp_coeffs[4 + k].data(), tmp.data() + ((size_t)1 << L), ((size_t)4) << L);
+  }
+  for (int k = 0; k < 8; ++k) circle_extend(comp_coeffs[k].data(), L, B, comp_lde[k].data(), twiddles(LDE));
+  std::vector<ColRef> comp_cols;
+  for (int k = 0; k < 8; ++k) comp_cols.push_back({comp_lde[k].data(), LDE});
+  MerkleTree t3 = merkle_commit(comp_cols);
+  ch.mix_root(t3.root());
+
+  // Samples: every column at the OODS point P, tree 2 also at P - g_L (the previous row,
+  // src/frontends/riscv/air/logup.zig:45-48); a column of 2^k rows at those points doubled L - k
+  // times (its lifted polynomial).
+  const PointQ oods = random_secure_point(ch);
+  const PointQ prev = qpadd(oods, qpneg(qpfromm(index_to_point(subgroup_gen(L)))));
+  auto doubled = [&](PointQ p, uint32_t k) { for (uint32_t i = k; i < L; ++i) p = qpdbl(p); return p; };
+  std::vector<QM31> cur(NCOLS), before(NCOLS), sampled_comp(8);
+  for (int c = 0; c < NCOLS; ++c) {
+    cur[c] = eval_at_point(col[c].coeffs.data(), col[c].log, doubled(oods, col[c].log));
+    if (c >= SM) before[c] = eval_at_point(col[c].coeffs.data(), col[c].log, doubled(prev, col[c].log));
+  }
+  for (int k = 0; k < 8; ++k) sampled_comp[k] = eval_at_point(comp_coeffs[k].data(), L, oods);
+  {
+    std::vector<QM31> flat;
+    for (int c = 0; c < SM; ++c) flat.push_back(cur[c]);
+    for (int c = SM; c < NCOLS; ++c) { flat.push_back(before[c]); flat.push_back(cur[c]); }
+    flat.insert(flat.end(), sampled_comp.begin(), sampled_comp.end());
+    ch.mix_felts(flat);
+  }
+  const QM31 quot_coeff = ch.draw_secure_felt();
+
+  // Quotient batches: random powers over (tree, column, sample); a two-sample column first takes
+  // its periodicity sample at its second point plus the lifting domain's generator doubled to the
+  // column's committed log size; batches by point in order of first appearance.
+  std::vector<QuotientBatch> batches;
+  {
+    QM31 rp = qone();
+    auto next = [&]() { QM31 r = rp; rp = qmul(rp, quot_coeff); return r; };
+    const PointM lifting_gen = index_to_point(subgroup_gen(LDE));  // CanonicCoset(LDE).step()
+    for (int c = 0; c < SM; ++c) batch_for(batches, oods).samples.push_back({col[c].lde.data(), col[c].log + B, cur[c], next()});
+    for (int c = SM; c < NCOLS; ++c) {
+      PointM g = lifting_gen;
+      for (uint32_t i = 0; i < col[c].log + B; ++i) g = pdbl(g);
+      const uint32_t lg = col[c].log + B;
+      batch_for(batches, qpadd(oods, qpfromm(g))).samples.push_back({col[c].lde.data(), lg, cur[c], next()});
+      batch_for(batches, prev).samples.push_back({col[c].lde.data(), lg, before[c], next()});
+      batch_for(batches, oods).samples.push_back({col[c].lde.data(), lg, cur[c], next()});
+    }
+    for (int k = 0; k < 8; ++k) batch_for(batches, oods).samples.push_back({comp_lde[k].data(), LDE, sampled_comp[k], next()});
+  }
+  std::vector<uint32_t> qcol[4];
+  quotient_columns(batches, LDE, qcol);
+
+  FriRun fr = fri_pow_queries(ch, qcol, LDE, xp.cfg, xp.n_threads);
+  if (!fr.ok) return std::string();
+
+  // Decommitments: tree 0 at the lifting domain's positions mapped to its own size.
+  std::vector<size_t> pre_q;
+  for (size_t q : fr.queries) pre_q.push_back(((q >> (LDE - (t + B) + 1)) << 1) + (q & 1));
+  Decommitment d0 = merkle_decommit(t0, refs(TA, 3), pre_q);
+  Decommitment d1 = merkle_decommit(t1, refs(A, 4), fr.queries);
+  Decommitment d2 = merkle_decommit(t2, refs(SM, 8), fr.queries);
+  Decommitment d3 = merkle_decommit(t3, comp_cols, fr.queries);
+
+  // Self-checks: the lookup balances and the composition matches the constraints at P.
+  if (!qiszero(qadd(claimed[0], claimed[1]))) return std::string("CONSTRAINTS_NOT_SATISFIED");
+  {
+    const QM31 basis[4] = {qone(), qfrom(0, 1, 0, 0), qfrom(0, 0, 1, 0), qfrom(0, 0, 0, 1)};
+    auto secure = [&](const std::vector<QM31>& v, int c0) {
+      QM31 r = qzero();
+      for (int k = 0; k < 4; ++k) r = qadd(r, qmul(v[c0 + k], basis[k]));
+      return r;
+    };
+    QM31 left = qzero(), right = qzero();
+    for (int k = 0; k < 4; ++k) { left = qadd(left, qmul(sampled_comp[k], basis[k])); right = qadd(right, qmul(sampled_comp[4 + k], basis[k])); }
+    PointQ pp = oods;
+    for (uint32_t i = 0; i + 2 < CL; ++i) pp = qpdbl(pp);
+    const QM31 comp_oods = qadd(left, qmul(pp.x, right));
+    const QM31 d_main = qsub(qadd(qadd(cur[A], qmul(alpha, cur[A + 1])), qmul(alpha2, cur[A + 2])), z);
+    const QM31 d_table = qsub(qadd(qadd(cur[TA], qmul(alpha, cur[TA + 1])), qmul(alpha2, cur[TA + 2])), z);
+    const QM31 c_main = qsub(qmul(qadd(qsub(secure(cur, SM), secure(before, SM)),
+                                       qmulm(claimed[0], minv((uint32_t)(((size_t)1 << n) % P)))), d_main), qone());
+    const QM31 c_table = qadd(qmul(qadd(qsub(secure(cur, ST), secure(before, ST)),
+                                        qmulm(claimed[1], minv((uint32_t)(((size_t)1 << t) % P)))), d_table), cur[M]);
+    const QM31 expect = qadd(qmul(qmul(random_coeff, c_main), qinv(coset_vanishing_q(coset_odds(n), doubled(oods, n)))),
+                             qmul(c_table, qinv(coset_vanishing_q(coset_odds(t), doubled(oods, t)))));
+    if (!qeq(expect, comp_oods)) return std::string("CONSTRAINTS_NOT_SATISFIED");
+  }
+
+  Json j;
+  j.s += "{\"config\":{\"pow_bits\":"; j.u(xp.cfg.pow_bits);
+  j.s += ",\"fri_config\":{\"log_blowup_factor\":"; j.u(B);
+  j.s += ",\"log_last_layer_degree_bound\":"; j.u(xp.cfg.log_last_layer_degree_bound);
+  j.s += ",\"n_queries\":"; j.u(xp.cfg.n_queries);
+  j.s += ",\"fold_step\":1},\"lifting_log_size\":null},\"statement\":{\"log_n\":"; j.u(n);
+  j.s += ",\"log_table\":"; j.u(t);
+  j.s += "},\"commitments\":[";
+  j.hash(t0.root()); j.s += ','; j.hash(t1.root()); j.s += ','; j.hash(t2.root()); j.s += ','; j.hash(t3.root());
+  j.s += "],\"claimed_sums\":["; j.qm(claimed[0]); j.s += ','; j.qm(claimed[1]);
+  j.s += "],\"sampled_values\":[[";
+  for (int c = TA; c < A; ++c) { if (c != TA) j.s += ','; j.s += '['; j.qm(cur[c]); j.s += ']'; }
+  j.s += "],[";
+  for (int c = A; c < SM; ++c) { if (c != A) j.s += ','; j.s += '['; j.qm(cur[c]); j.s += ']'; }
+  j.s += "],[";
+  for (int c = SM; c < NCOLS; ++c) { if (c != SM) j.s += ','; j.s += '['; j.qm(before[c]); j.s += ','; j.qm(cur[c]); j.s += ']'; }
+  j.s += "],[";
+  for (int k = 0; k < 8; ++k) { if (k) j.s += ','; j.s += '['; j.qm(sampled_comp[k]); j.s += ']'; }
+  j.s += "]],";
+  json_decommit_and_fri(j, {&d0, &d1, &d2, &d3}, fr, qcol);
+  j.s += "}";
+  return j.s;
+}
+
 }  // namespace
 
 // ---------------------------------------------------------------------------
@@ -1137,6 +1435,30 @@ int oracle_prove_wide_fib(uint32_t log_n_rows, uint32_t sequence_len, const orac
   std::memcpy(out, s.data(), s.size());
   return 0;
 }
+
+int oracle_prove_logup_xor(uint32_t log_n, uint32_t log_table, const oracle_pcs_config* cfg, uint64_t seed,
+                           int has_channel_seed, uint64_t channel_seed, int n_threads, uint8_t* out, size_t out_cap,
+                           size_t* out_len) {
+  if (!cfg || log_n < 1 || log_n > 24 || (log_table != 8 && log_table != 16) || cfg->log_blowup_factor < 1 ||
+      cfg->log_blowup_factor > 4 || cfg->n_queries == 0)
+    return -1;
+  if (cfg->log_last_layer_degree_bound + cfg->log_blowup_factor + 1 > std::max(log_n, log_table) + cfg->log_blowup_factor)
+    return -1;
+#ifdef _OPENMP
+  if (n_threads > 0) omp_set_num_threads(n_threads);
+#endif
+  XorParams xp{log_n, log_table, *cfg, seed, has_channel_seed != 0, channel_seed, n_threads};
+  std::string s = prove_logup_xor(xp);
+  if (s.empty()) return -3;
+  if (s == "CONSTRAINTS_NOT_SATISFIED") return -4;
+  if (s == "DIVISION_BY_ZERO") return -5;
+  if (out_len) *out_len = s.size();
+  if (!out || out_cap < s.size()) return -2;
+  std::memcpy(out, s.data(), s.size());
+  return 0;
+}
+
+double oracle_last_pow_seconds(void) { return last_pow_seconds(); }
 
 int oracle_interpolate(uint32_t log_size, uint32_t* values) {
   if (log_size < 1 || log_size > 28 || !values) return -1;

@@ -49,6 +49,9 @@ def lib():
             ctypes.c_uint32, ctypes.c_uint32, ctypes.POINTER(PcsConfig), u32p, ctypes.c_int,
             ctypes.c_uint64, ctypes.c_int, ctypes.c_uint64, ctypes.c_int, ctypes.c_void_p,
             ctypes.c_size_t, ctypes.POINTER(ctypes.c_size_t)]
+        _lib.oracle_prove_logup_xor.argtypes = [
+            ctypes.c_uint32, ctypes.c_uint32, ctypes.POINTER(PcsConfig), ctypes.c_uint64, ctypes.c_int,
+            ctypes.c_uint64, ctypes.c_int, ctypes.c_void_p, ctypes.c_size_t, ctypes.POINTER(ctypes.c_size_t)]
         _lib.oracle_gen_trace.argtypes = [ctypes.c_uint32, ctypes.c_uint32, ctypes.c_int,
                                           ctypes.c_uint64, u32p]
         _lib.oracle_pow_grind.argtypes = [ctypes.c_char_p, ctypes.c_uint32, ctypes.c_int,
@@ -90,6 +93,26 @@ def prove_wide_fib(log_n_rows: int, sequence_len: int, cfg: PcsConfig, trace: np
     if rc != 0:
         raise RuntimeError(f"oracle prove failed: {rc}")
     return buf.raw[: n.value]
+
+
+def prove_logup_xor(log_n: int, cfg: PcsConfig, seed: int = 0, log_table: int = 16,
+                    channel_seed: int | None = None, n_threads: int = 0) -> bytes:
+    """The LogUp XOR-lookup AIR proof of the oracle (oracle.cpp prove_logup_xor)."""
+    cap = 1 << 26
+    buf = ctypes.create_string_buffer(cap)
+    n = ctypes.c_size_t(0)
+    rc = lib().oracle_prove_logup_xor(log_n, log_table, ctypes.byref(cfg), seed, int(channel_seed is not None),
+                                      channel_seed or 0, n_threads, buf, cap, ctypes.byref(n))
+    if rc != 0:
+        raise RuntimeError(f"oracle XOR-lookup prove failed: {rc}")
+    return buf.raw[: n.value]
+
+
+def last_pow_seconds() -> float:
+    """Wall time of the proof-of-work grind of this thread's last oracle proof."""
+    f = lib().oracle_last_pow_seconds
+    f.restype = ctypes.c_double
+    return f()
 
 
 def interpolate(values: np.ndarray) -> np.ndarray:

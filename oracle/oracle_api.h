@@ -40,6 +40,17 @@ int oracle_prove_wide_fib(uint32_t log_n_rows, uint32_t sequence_len, const orac
                           int has_channel_seed, uint64_t channel_seed, int n_threads,
                           uint8_t* out, size_t out_cap, size_t* out_len);
 
+/* LogUp XOR-lookup AIR proof (2^log_n lookups of seeded (log_table/2)-bit pairs into the
+ * 2^log_table-row XOR table, both components at their own sizes under the lifted PCS); the JSON
+ * layout of the wide-Fibonacci proof plus "statement" and "claimed_sums". Returns -5 on a zero LogUp
+ * denominator, -4 when a self-check fails, -2 when out_cap is too small (out_len set). */
+int oracle_prove_logup_xor(uint32_t log_n, uint32_t log_table, const oracle_pcs_config* cfg, uint64_t seed,
+                           int has_channel_seed, uint64_t channel_seed, int n_threads, uint8_t* out,
+                           size_t out_cap, size_t* out_len);
+
+/* Seconds the calling thread's last oracle proof spent in its proof-of-work grind. */
+double oracle_last_pow_seconds(void);
+
 /* Op-level checkers (all host buffers). */
 int oracle_interpolate(uint32_t log_size, uint32_t* values /* in: evals, out: coeffs */);
 int oracle_evaluate(uint32_t log_size, uint32_t* values /* in: coeffs, out: evals */);

@@ -2,7 +2,8 @@
 reference counterpart, so the verifier's transcript replay, LogUp cancellation, OODS constraint
 check and PCS/FRI decommitment checks are the parity gate). The main and table components keep
 their own sizes (2^log_n and 2^log_table rows) under the lifted PCS: cases cover the lookups
-smaller than, equal to and larger than the table."""
+smaller than, equal to and larger than the table. Every proof is also compared byte for byte with
+the oracle's own XOR-lookup prover, which shares no code with the GPU prover."""
 import json
 
 import pytest
@@ -31,6 +32,24 @@ def test_xor_air_proof_verifies(ctx, log_n, log_table, preset, over):
     assert verifier.verify_logup_xor(p, log_n, log_table, channel_seed=3)
     with pytest.raises(verifier.VerificationError):
         verifier.verify_logup_xor(p, log_n, log_table, channel_seed=4)
+
+
+_PRESETS = {"functional": ("functional", {}), "secure": ("secure", {}),
+            "blowup2": ("functional", dict(log_blowup_factor=2, n_queries=5, log_last_layer_degree_bound=1))}
+
+
+@pytest.mark.parametrize("preset", sorted(_PRESETS))
+@pytest.mark.parametrize("log_table", [8, 16])
+@pytest.mark.parametrize("log_n", [6, 12, 16, 20])
+def test_xor_air_proof_equals_the_oracle(ctx, log_n, log_table, preset):
+    """Byte for byte against the oracle's independent prover (oracle/oracle.cpp prove_logup_xor):
+    lookups smaller than, equal to and larger than the table, three protocol variants."""
+    name, over = _PRESETS[preset]
+    o = oracle.config(name, **over)
+    g = _cfg(name, **over)
+    seed, chan = 1000 + log_n + log_table, 11 * log_n
+    assert ctx.prove_logup_xor(log_n, g, seed=seed, log_table=log_table, channel_seed=chan) == \
+        oracle.prove_logup_xor(log_n, o, seed=seed, log_table=log_table, channel_seed=chan)
 
 
 def test_xor_air_full_size_and_determinism(ctx):
