@@ -84,10 +84,12 @@ typedef struct {
 } stwo_b200_wide_fib_request;
 
 /* Device time per proving stage, in milliseconds; host_encode is the host time after the last device
- * stage (JSON wire encoding and the OODS self-check). */
+ * stage (JSON wire encoding and the OODS self-check); host_gaps the host time between the transcript's
+ * stream synchronizations and the next device work (for a proof that runs alone, the device idles
+ * then: total - host_gaps bounds the proof's device work). */
 typedef struct {
   float upload, trace, main_commit, composition, composition_commit, oods, quotients, fri, pow, decommit, total;
-  float host_encode;
+  float host_encode, host_gaps;
 } stwo_b200_stage_times;
 
 /* Device pointers: Merkle layer buffers must be 16-byte aligned, FRI fold sources 8-byte aligned with

@@ -446,6 +446,112 @@ __global__ void __launch_bounds__(MAXT, MINB) k_fft_high16(High16Params p) {
   }
 }
 
+// Windows of the high pass over R row bits: an optional short window [0, R % 4) first, then
+// full 4-bit windows. Window i covers row bits [win_w0(i), win_w0(i) + 4) of which it applies
+// win_nl(i) layers.
+template <int R>
+__host__ __device__ constexpr int win_count() { return R / 4 + (R % 4 ? 1 : 0); }
+template <int R>
+__host__ __device__ constexpr uint32_t win_w0(int i) { return R % 4 ? (i == 0 ? 0u : (uint32_t)(R % 4 + 4 * (i - 1))) : 4u * i; }
+template <int R>
+__host__ __device__ constexpr uint32_t win_nl(int i) { return (R % 4 && i == 0) ? (uint32_t)(R % 4) : 4u; }
+
+// Interpolation's high layers fused with the blow-up-2 extension, for columns of 2^(12 + R)
+// words (R = 5..10): one CTA of 2^R threads per tile of 2^R rows x 16 adjacent low indices
+// (row m, low index t is transform index (m << 12) + g * 16 + t), each thread 16 rows of one low
+// index per window. The inverse windows run bottom-up; the last one, which covers the top row
+// bits [R - 4, R), also scales by 1/n, stores the coefficients, and applies the extension's
+// forward window over the same row bits to two copies of its 16 coefficients: the extension's
+// top layer pairs every coefficient with a zero row, so it only copies row m to m + 2^R (the
+// reference skips it the same way, src/prover/poly/circle/transforms.zig:132-147), and the two
+// copies then differ only in their twiddles. The remaining forward windows run top-down on both
+// halves. One shared-memory exchange and barrier per window boundary; the generic kernel pays a
+// zero fill, a 9th layer of butterflies on zeros and three more exchanges on 2^20 -> 2^21.
+template <int R>
+__global__ void __launch_bounds__(1 << R, R <= 8 ? (1024 >> R) : 1) k_fft_high16_lde1(High16Params p) {
+  static_assert(R >= 5 && R <= 10, "tile rows");
+  constexpr int NW = win_count<R>();
+  extern __shared__ uint32_t sm[];  // 16 << (R + 1) words: both halves of the extended tile
+  const uint32_t th = threadIdx.x, t = th & 15, q = th >> 4;
+  const uint32_t g = blockIdx.x, col = blockIdx.y;
+  // Row m of low index t is word (m << 12) + t past these (the tile's 16 low indices are adjacent).
+  const uint32_t* src = p.src + col * p.ss + g * 16 + t;
+  uint32_t* coef = p.coef + col * p.cs + g * 16 + t;
+  uint32_t* out = p.out + col * p.os + g * 16 + t;
+  const uint32_t hoff = swz((1u << R) << 4);  // shared position of row m + 2^R relative to row m
+  uint32_t x[16], y[16];
+#pragma unroll
+  for (int i = 0; i < NW; ++i) {
+    const uint32_t w0 = win_w0<R>(i), nl = win_nl<R>(i);
+    const uint32_t mb = spread(q, w0);
+    const uint32_t a = swz((mb << 4) | t);
+    if (i == 0) {
+#pragma unroll
+      for (int k = 0; k < 16; ++k) x[k] = __ldg(src + ((uint64_t)(mb + ((uint32_t)k << w0)) << B12));
+    } else {
+#pragma unroll
+      for (int k = 0; k < 16; ++k) x[k] = sm[a ^ swz((uint32_t)k << (w0 + 4))];
+    }
+    radix16_dyn<true>(x, p.itv, B12, w0, mb, nl);
+    if (i + 1 < NW) {
+#pragma unroll
+      for (int k = 0; k < 16; ++k) sm[a ^ swz((uint32_t)k << (w0 + 4))] = x[k];
+      __syncthreads();
+    }
+  }
+  {
+    constexpr uint32_t w0 = R - 4;
+    const uint32_t mb = spread(q, w0);
+#pragma unroll
+    for (int k = 0; k < 16; ++k) {
+      const uint32_t v = mmul(x[k], p.scale);
+      coef[(uint64_t)(mb + ((uint32_t)k << w0)) << B12] = v;
+      x[k] = v;
+      y[k] = v;
+    }
+    radix16<false, 0, 4>(x, p.ftv, B12, w0, mb);
+    radix16<false, 0, 4>(y, p.ftv, B12, w0, mb | (1u << R));
+    const uint32_t a = swz((mb << 4) | t);
+#pragma unroll
+    for (int k = 0; k < 16; ++k) {
+      const uint32_t pos = a ^ swz((uint32_t)k << (w0 + 4));
+      sm[pos] = x[k];
+      sm[pos ^ hoff] = y[k];
+    }
+    __syncthreads();
+  }
+#pragma unroll
+  for (int i = NW - 2; i >= 0; --i) {
+    const uint32_t w0 = win_w0<R>(i), nl = win_nl<R>(i);
+    const uint32_t mb = spread(q, w0);
+    const uint32_t a = swz((mb << 4) | t);
+#pragma unroll
+    for (int k = 0; k < 16; ++k) {
+      const uint32_t pos = a ^ swz((uint32_t)k << (w0 + 4));
+      x[k] = sm[pos];
+      y[k] = sm[pos ^ hoff];
+    }
+    radix16_dyn<false>(x, p.ftv, B12, w0, mb, nl);
+    radix16_dyn<false>(y, p.ftv, B12, w0, mb | (1u << R), nl);
+    if (i > 0) {
+#pragma unroll
+      for (int k = 0; k < 16; ++k) {
+        const uint32_t pos = a ^ swz((uint32_t)k << (w0 + 4));
+        sm[pos] = x[k];
+        sm[pos ^ hoff] = y[k];
+      }
+      __syncthreads();
+    } else {
+#pragma unroll
+      for (int k = 0; k < 16; ++k) {
+        const uint64_t m = mb + ((uint32_t)k << w0);
+        out[m << B12] = x[k];
+        out[(m + (1u << R)) << B12] = y[k];
+      }
+    }
+  }
+}
+
 inline uint32_t inv_pow2(uint32_t log) { return minv(1u << log); }
 
 }  // namespace
@@ -534,6 +640,31 @@ static cudaError_t launch_high16(const High16Params& p, uint32_t n_cols, cudaStr
   else k_fft_high16<1024, 1><<<grid, 1u << rows, smem, stream>>>(p);
   note_launch();
   return cudaGetLastError();
+}
+
+template <int R>
+static cudaError_t launch_lde1_rows(const High16Params& p, uint32_t n_cols, cudaStream_t stream) {
+  const size_t smem = (size_t)64 << (R + 1);
+  static const bool attr_set = [] {  // once per process (thread-safe static initialisation)
+    cudaFuncSetAttribute(k_fft_high16_lde1<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)((size_t)64 << (R + 1)));
+    return true;
+  }();
+  (void)attr_set;
+  k_fft_high16_lde1<R><<<dim3(1u << (B12 - 4), n_cols), 1u << R, smem, stream>>>(p);
+  note_launch();
+  return cudaGetLastError();
+}
+
+// The fused interpolate + blow-up-2 extension high pass (rows_in in [5, 10]).
+static cudaError_t launch_high16_lde1(const High16Params& p, uint32_t n_cols, cudaStream_t stream) {
+  switch (p.rows_in) {
+    case 5: return launch_lde1_rows<5>(p, n_cols, stream);
+    case 6: return launch_lde1_rows<6>(p, n_cols, stream);
+    case 7: return launch_lde1_rows<7>(p, n_cols, stream);
+    case 8: return launch_lde1_rows<8>(p, n_cols, stream);
+    case 9: return launch_lde1_rows<9>(p, n_cols, stream);
+    default: return launch_lde1_rows<10>(p, n_cols, stream);
+  }
 }
 
 cudaError_t fft_columns(const DeviceTables& t, bool inverse, uint32_t log_size, uint32_t n_cols, uint32_t* cols,
@@ -631,7 +762,7 @@ cudaError_t interpolate_extend(const DeviceTables& t, uint32_t log_size, uint32_
     p.do_forward = 1; p.ftv = t.view(out_log, false); p.rows_out = out_log - B12;
     p.dup = log_blowup == 1; p.fwd_layers = p.dup ? p.rows_in : p.rows_out;
     p.out = lde; p.os = lde_stride;
-    e = launch_high16(p, n_cols, stream);
+    e = log_blowup == 1 && p.rows_in >= 5 ? launch_high16_lde1(p, n_cols, stream) : launch_high16(p, n_cols, stream);
     if (e != cudaSuccess) return e;
     return launch_low12(t, false, out_log, n_cols, lde, lde_stride, lde, lde_stride, 0, stream);
   }

@@ -25,6 +25,7 @@ struct DeviceTables {
   uint32_t* tw = nullptr;      // forward twiddle tower
   uint32_t* itw = nullptr;     // inverse twiddle tower
   uint32_t tower_log = 0;      // R: root half coset halfOdds(R)
+  uint32_t sm_count = 148;     // multiprocessors of the device (persistent grid sizes)
   TwiddleView view(uint32_t domain_log, bool inverse) const;
 };
 

@@ -116,6 +116,7 @@ int32_t Context::init(int dev, uint32_t tower_log) {
   if (cudaGetDeviceCount(&n) != cudaSuccess || n <= dev) return E_NO_DEVICE;
   if (cudaSetDevice(dev) != cudaSuccess) return E_CUDA;
   cudaDeviceGetAttribute(&sm_count, cudaDevAttrMultiProcessorCount, dev);
+  tables.sm_count = (uint32_t)std::max(sm_count, 1);
   if (cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking) != cudaSuccess) return E_CUDA;
   // Keep freed stream-ordered allocations cached in this process's default pool
   // instead of returning them to the driver at every synchronization.
@@ -349,6 +350,9 @@ int32_t WideFibProver::prove(const ProveRequest& req, std::string& out, StageTim
   SB_CK(cudaMemcpyAsync(pin, b.tree1 + (2 * l.NL - 2) * 32, 32, cudaMemcpyDeviceToHost, s));
   SB_CK(cudaEventRecord(ev_[3], s));
   SB_CK(sync());
+  Clock::time_point gap = Clock::now();
+  float host_gaps = 0;
+  auto gap_end = [&]() { host_gaps += std::chrono::duration<float, std::milli>(Clock::now() - gap).count(); };
   std::memcpy(root1, pin, 32);
   if (deadline_.passed()) return fail(E_TIMEOUT, "proof deadline passed after the main commitment");
   ch.mix_root(root1);
@@ -367,6 +371,7 @@ int32_t WideFibProver::prove(const ProveRequest& req, std::string& out, StageTim
     for (uint32_t i = 0; i < n_cons; ++i) { pw[i] = cur; cur = qmul(cur, random_coeff); }
     QM31* hc = reinterpret_cast<QM31*>(pin);
     for (uint32_t k = 0; k < n_cons; ++k) hc[k] = pw[n_cons - 1 - k];
+    gap_end();
     SB_CK(cudaMemcpyAsync(b.comp_coeffs, hc, n_cons * sizeof(QM31), cudaMemcpyHostToDevice, s));
   }
   if (B != 1) SB_CK(extend(T, n, 1, W, b.coeffs, l.N, b.eval_c, l.NC, s));
@@ -387,12 +392,14 @@ int32_t WideFibProver::prove(const ProveRequest& req, std::string& out, StageTim
   SB_CK(cudaMemcpyAsync(pin, b.tree2 + (2 * l.NL - 2) * 32, 32, cudaMemcpyDeviceToHost, s));
   SB_CK(cudaEventRecord(ev_[5], s));
   SB_CK(sync());
+  gap = Clock::now();
   std::memcpy(root2, pin, 32);
   if (deadline_.passed()) return fail(E_TIMEOUT, "proof deadline passed after the composition commitment");
   ch.mix_root(root2);
 
   // OODS point and sampled values of every coefficient column.
   PointQ oods = random_secure_point(ch);
+  gap_end();
   SB_CK(eval_at_point(T, n, W, b.coeffs, l.N, oods, nullptr, b.oods_partial, b.oods_out, fs));
   SB_CK(eval_at_point(T, n, 4, b.comp, l.NC, oods, nullptr, b.oods_partial, b.oods_out + W, fs));
   SB_CK(eval_at_point(T, n, 4, b.comp + l.N, l.NC, oods, nullptr, b.oods_partial, b.oods_out + W + 4, fs));
@@ -400,6 +407,7 @@ int32_t WideFibProver::prove(const ProveRequest& req, std::string& out, StageTim
   SB_CK(cudaMemcpyAsync(pin, b.oods_out, (W + 8) * sizeof(QM31), cudaMemcpyDeviceToHost, fs));
   SB_CK(cudaEventRecord(ev_[6], fs));
   SB_CK(fsync());
+  gap = Clock::now();
   std::memcpy(sampled.data(), pin, (W + 8) * sizeof(QM31));
   ch.mix_felts(sampled.data(), sampled.size());
   QM31 quot_coeff = ch.draw_secure_felt();
@@ -424,6 +432,7 @@ int32_t WideFibProver::prove(const ProveRequest& req, std::string& out, StageTim
     for (uint32_t i = 0; i < 8; ++i) hp[W + i] = b.comp_lde + (size_t)i * l.NL;
     QuotientBatchDev* hb = reinterpret_cast<QuotientBatchDev*>(pin + 128 * 1024);
     hb->point = oods; hb->sum_a = sum_a; hb->sum_b = sum_b; hb->first = 0; hb->count = nq;
+    gap_end();
     SB_CK(cudaMemcpyAsync(b.quot_c, hc, nq * sizeof(QM31), cudaMemcpyHostToDevice, fs));
     SB_CK(cudaMemcpyAsync(b.col_ptrs, hp, nq * sizeof(void*), cudaMemcpyHostToDevice, fs));
     SB_CK(cudaMemcpyAsync(b.batch, hb, sizeof(QuotientBatchDev), cudaMemcpyHostToDevice, fs));
@@ -452,6 +461,7 @@ int32_t WideFibProver::prove(const ProveRequest& req, std::string& out, StageTim
     plan.add_tree(b.tree1, l.L, c1, queries);
     plan.add_tree(b.tree2, l.L, c2, queries);
     plan.add_fri(fbuf, l.L, l.n_inner, queries);
+    host_gaps += fr.host_gap_ms + std::chrono::duration<float, std::milli>(Clock::now() - fr.gap_start).count();
     std::string gerr;
     int32_t grc = plan.gather(b.scratch, b.scratch_bytes, pin, pinned_size_, fs, ev_[10], gerr);
     if (grc != OK) return fail(grc, gerr);
@@ -523,6 +533,7 @@ int32_t WideFibProver::prove(const ProveRequest& req, std::string& out, StageTim
     times->total = el(0, 10);
     times->host_encode =
         std::chrono::duration<float, std::milli>(std::chrono::steady_clock::now() - t_encode).count();
+    times->host_gaps = host_gaps;
   }
   out = j.str();
   return OK;

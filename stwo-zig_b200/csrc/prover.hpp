@@ -48,11 +48,13 @@ struct ProveRequest {
   uint64_t channel_seed = 0;
 };
 
-// Stage timings of one proof (milliseconds of device time between events), and the host time
-// spent after the last device stage (proof encoding and the OODS self-check).
+// Stage timings of one proof (milliseconds of device time between events), the host time spent
+// after the last device stage (proof encoding and the OODS self-check), and the host time between
+// a stream synchronization of the transcript and the next device work (the device may idle then
+// when the proof runs alone: total - host_gaps bounds its device work).
 struct StageTimes {
   float upload = 0, trace = 0, main_commit = 0, composition = 0, composition_commit = 0, oods = 0,
-        quotients = 0, fri = 0, pow = 0, decommit = 0, total = 0, host_encode = 0;
+        quotients = 0, fri = 0, pow = 0, decommit = 0, total = 0, host_encode = 0, host_gaps = 0;
 };
 
 // Status codes shared with the C ABI.

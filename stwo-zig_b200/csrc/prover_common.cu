@@ -52,6 +52,7 @@ int32_t fri_pow_queries(const DeviceTables& T, int sm_count, Channel& ch, const 
     SB_CKE(cudaMemcpyAsync(pin, fb.chan, sizeof(FriChannelDev), cudaMemcpyDeviceToHost, fs));
     SB_CKE(cudaMemcpyAsync(pin + LAST_OFF, fb.line[n_inner], 4 * m_last * 4, cudaMemcpyDeviceToHost, fs));
     SB_CKE(cudaStreamSynchronize(fs));
+    out.gap_start = Clock::now();
     FriChannelDev dc;
     std::memcpy(&dc, pin, sizeof(dc));
     for (uint32_t k = 0; k <= n_inner; ++k) {
@@ -126,10 +127,12 @@ int32_t fri_pow_queries(const DeviceTables& T, int sm_count, Channel& ch, const 
     SB_CKE(cudaMemsetAsync(fb.pow_result, 0xff, 8, s));
     nonce = ~0ull;
     for (uint64_t base = 0; base < max_nonce && nonce == ~0ull;) {
+      out.host_gap_ms += std::chrono::duration<float, std::milli>(Clock::now() - out.gap_start).count();
       for (int r = 0; r < 4 && base < max_nonce; ++r, base += per_round)
         SB_CKE(pow_round(pw, cfg.pow_bits, base, fb.pow_result, sm_count, s));
       SB_CKE(cudaMemcpyAsync(pin, fb.pow_result, 8, cudaMemcpyDeviceToHost, s));
       SB_CKE(cudaStreamSynchronize(s));
+      out.gap_start = Clock::now();
       std::memcpy(&nonce, pin, 8);
       if (nonce == ~0ull && deadline.passed()) {
         err = "proof deadline passed during the proof-of-work search";

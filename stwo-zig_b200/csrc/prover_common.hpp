@@ -256,6 +256,10 @@ struct FriResult {
   std::vector<QM31> last_coeffs;
   uint64_t nonce = 0;
   std::vector<uint64_t> queries;  // sorted, unique
+  // Host time between the stream synchronizations of the tail and the next device work (the
+  // FRI channel replay and last layer, the proof-of-work checks, the query draw), milliseconds.
+  float host_gap_ms = 0;
+  Clock::time_point gap_start;    // when the last synchronization of the tail returned
 };
 // Runs on `fs` (FRI, latency-bound) and `s` (proof of work); `pin` is pinned host staging
 // (at least 64 KB). The FRI layers draw their alphas on the device (FriChannelDev); the

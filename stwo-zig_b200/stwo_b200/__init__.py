@@ -79,7 +79,7 @@ class ServerSnapshotC(ctypes.Structure):
 class StageTimesC(ctypes.Structure):
     _fields_ = [(n, ctypes.c_float) for n in ("upload", "trace", "main_commit", "composition", "composition_commit",
                                               "oods", "quotients", "fri", "pow", "decommit", "total",
-                                              "host_encode")]
+                                              "host_encode", "host_gaps")]
 
 
 class RequestStatsC(ctypes.Structure):

@@ -42,7 +42,8 @@ def test_interpolate_evaluate(ctx, log):
 
 
 @pytest.mark.parametrize("log,blowup", [(1, 1), (3, 1), (10, 1), (11, 1), (12, 1), (15, 1), (16, 1), (17, 1),
-                                        (19, 1), (20, 1), (21, 1), (12, 2), (16, 2), (18, 3), (5, 3)])
+                                        (18, 1), (19, 1), (20, 1), (21, 1), (22, 1), (12, 2), (16, 2), (18, 3),
+                                        (5, 3)])
 def test_interpolate_and_extend(ctx, log, blowup):
     import torch
     rng = np.random.default_rng(100 + log)

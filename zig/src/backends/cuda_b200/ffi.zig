@@ -117,6 +117,7 @@ pub const StageTimes = extern struct {
     decommit: f32,
     total: f32,
     host_encode: f32,
+    host_gaps: f32,
 };
 
 /// stwo_b200_telemetry
