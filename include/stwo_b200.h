@@ -439,6 +439,32 @@ int32_t stwo_b200_xor_lookup_trace(stwo_b200_context* ctx, uint32_t log_n, uint6
 int32_t stwo_b200_pow_grind(stwo_b200_context* ctx, const uint8_t prefix_digest[32], uint32_t n_bits,
                             uint64_t* nonce_out);
 
+/* ---- Autotuner ----------------------------------------------------------------------------------- */
+
+/* Launch-shape autotuner of the kernels that come in variants writing the same bits (op 0: the
+ * interpolate + blow-up-2 high pass, fused or generic; op 1: the Merkle leaf kernel at 5, 6 or 4 CTAs
+ * per SM; op 2: the DEEP quotient kernel at 6, 3 or 9 loads in flight), keyed by (op, log_size,
+ * n_cols) for the process. A key's first call times every variant on its own inputs with CUDA events
+ * and keeps the fastest; later calls run it. The north star's autotuner cached per
+ * (log_size, n_columns); the reference has none (its Metal backend fixes its launch shapes).
+ * mode -1 (the default) tunes; mode v >= 0 runs variant v of every op (the last one where an op has
+ * fewer) and tunes nothing. */
+typedef struct {
+  uint32_t op, log_size, n_cols;
+  int32_t variant;
+  float ms[4]; /* measured milliseconds of each variant on the key's first call (0: none) */
+} stwo_b200_tune_entry;
+int32_t stwo_b200_autotune_mode(int32_t mode);
+/* Tunes every key of one wide-Fibonacci proof shape: waits for the device, then proves one throwaway
+ * proof of that shape (no proof of work) on the calling thread, whose first calls of each op tune it.
+ * Call it while nothing else runs on the device (timings taken beside other work pick worse
+ * variants); keys met later for the first time tune inside whatever call meets them. */
+int32_t stwo_b200_autotune_wide_fibonacci(stwo_b200_context* ctx, uint32_t log_n_rows, uint32_t sequence_len,
+                                          uint32_t log_blowup);
+/* Copies the tuned keys into out[0..cap); *n receives their count (STWO_B200_E_BUFFER_TOO_SMALL when
+ * cap is smaller). */
+int32_t stwo_b200_autotune_table(stwo_b200_tune_entry* out, size_t cap, size_t* n);
+
 /* ---- Testing ------------------------------------------------------------------------------------- */
 
 /* Makes the nth device or pinned-host allocation of the library from now on fail as if out of memory

@@ -11,6 +11,7 @@
 #include "context.hpp"
 #include "prover.hpp"
 #include "server.hpp"
+#include "tuner.hpp"
 #include "verifier.hpp"
 
 namespace sb {
@@ -413,7 +414,7 @@ int32_t stwo_b200_accumulate_quotients(stwo_b200_context* ctx, uint32_t log_size
   if (e != cudaSuccess) return cuda_status(e, "quotient batch");
   e = cudaMemcpyAsync(dbatch, &hb, sizeof(hb), cudaMemcpyHostToDevice, st(stream));
   if (e == cudaSuccess)
-    e = sb::accumulate_quotients(ctx->ctx.tables, log_size, 1, static_cast<sb::QuotientBatchDev*>(dbatch), col_ptrs_dev,
+    e = sb::accumulate_quotients(ctx->ctx.tables, log_size, 1, n_cols, static_cast<sb::QuotientBatchDev*>(dbatch), col_ptrs_dev,
                                  reinterpret_cast<const sb::QM31*>(c_dev), out, out_stride, st(stream));
   cudaError_t e2 = cudaStreamSynchronize(st(stream));  // the batch descriptor lives on this host frame
   cudaFreeAsync(dbatch, st(stream));
@@ -619,6 +620,45 @@ int32_t stwo_b200_server_warmup(stwo_b200_server* server, uint32_t max_log_n_row
 int32_t stwo_b200_server_set_request_timeout(stwo_b200_server* server, uint32_t timeout_ms) {
   if (!server) return set_error(STWO_B200_E_INVALID, "null server");
   server->server->set_request_timeout(timeout_ms);
+  return STWO_B200_OK;
+}
+
+int32_t stwo_b200_autotune_mode(int32_t mode) {
+  if (mode < -1) return set_error(STWO_B200_E_INVALID, "autotune mode is -1 (tune) or a variant index");
+  sb::tune_force(mode);
+  return STWO_B200_OK;
+}
+
+int32_t stwo_b200_autotune_wide_fibonacci(stwo_b200_context* ctx, uint32_t log_n_rows, uint32_t sequence_len,
+                                          uint32_t log_blowup) {
+  CK_CTX(ctx);
+  cudaError_t e = cudaDeviceSynchronize();
+  if (e != cudaSuccess) return cuda_status(e, "autotune: device synchronization");
+  sb::ProveRequest r;
+  r.log_n_rows = log_n_rows;
+  r.sequence_len = sequence_len;
+  r.config.pow_bits = 0;  // the grind has no variants
+  r.config.log_blowup_factor = log_blowup;
+  r.config.log_last_layer_degree_bound = 0;
+  r.config.n_queries = 3;
+  r.trace_kind = 1;
+  r.trace_seed = 1;
+  sb::WideFibProver* p = ctx->ctx.acquire();
+  if (!p) return set_error(STWO_B200_E_CUDA, "stream creation failed");
+  std::string proof;
+  int32_t rc = p->prove(r, proof, nullptr);
+  std::string err = p->error();
+  ctx->ctx.release(p);
+  return rc == STWO_B200_OK ? rc : set_error(rc, err);
+}
+
+int32_t stwo_b200_autotune_table(stwo_b200_tune_entry* out, size_t cap, size_t* n) {
+  if (!n) return set_error(STWO_B200_E_INVALID, "null count");
+  std::vector<sb::TuneEntry> t = sb::tune_table();
+  *n = t.size();
+  if (t.size() > cap || (t.size() && !out)) return set_error(STWO_B200_E_BUFFER_TOO_SMALL, "autotune table buffer too small");
+  static_assert(sizeof(sb::TuneEntry) == sizeof(stwo_b200_tune_entry), "tune entry layout");
+  if (!t.empty()) std::memcpy(out, t.data(), t.size() * sizeof(sb::TuneEntry));
   return STWO_B200_OK;
 }
 

@@ -18,6 +18,7 @@
 
 #include "fft16.cuh"
 #include "kernels.cuh"
+#include "tuner.hpp"
 
 namespace sb {
 
@@ -754,17 +755,25 @@ cudaError_t interpolate_extend(const DeviceTables& t, uint32_t log_size, uint32_
   if (n_cols == 0) return cudaSuccess;
   const uint32_t out_log = log_size + log_blowup;
   if (use16(log_size, out_log, evals, ev_stride, lde, lde_stride) && aligned16(coeffs, co_stride)) {
-    cudaError_t e = launch_low12(t, true, log_size, n_cols, evals, ev_stride, coeffs, co_stride, 0, stream);
-    if (e != cudaSuccess) return e;
-    High16Params p{};
-    p.src = coeffs; p.ss = co_stride; p.rows_in = log_size - B12;
-    p.do_inverse = 1; p.itv = t.view(log_size, true); p.scale = inv_pow2(log_size); p.coef = coeffs; p.cs = co_stride;
-    p.do_forward = 1; p.ftv = t.view(out_log, false); p.rows_out = out_log - B12;
-    p.dup = log_blowup == 1; p.fwd_layers = p.dup ? p.rows_in : p.rows_out;
-    p.out = lde; p.os = lde_stride;
-    e = log_blowup == 1 && p.rows_in >= 5 ? launch_high16_lde1(p, n_cols, stream) : launch_high16(p, n_cols, stream);
-    if (e != cudaSuccess) return e;
-    return launch_low12(t, false, out_log, n_cols, lde, lde_stride, lde, lde_stride, 0, stream);
+    // Variant 0: the fused high pass (blow-up 2, 2^17 .. 2^22); variant 1: the generic one.
+    auto chain = [&](int variant) -> cudaError_t {
+      cudaError_t e = launch_low12(t, true, log_size, n_cols, evals, ev_stride, coeffs, co_stride, 0, stream);
+      if (e != cudaSuccess) return e;
+      High16Params p{};
+      p.src = coeffs; p.ss = co_stride; p.rows_in = log_size - B12;
+      p.do_inverse = 1; p.itv = t.view(log_size, true); p.scale = inv_pow2(log_size); p.coef = coeffs; p.cs = co_stride;
+      p.do_forward = 1; p.ftv = t.view(out_log, false); p.rows_out = out_log - B12;
+      p.dup = log_blowup == 1; p.fwd_layers = p.dup ? p.rows_in : p.rows_out;
+      p.out = lde; p.os = lde_stride;
+      e = log_blowup == 1 && p.rows_in >= 5 && variant == 0 ? launch_high16_lde1(p, n_cols, stream)
+                                                             : launch_high16(p, n_cols, stream);
+      if (e != cudaSuccess) return e;
+      return launch_low12(t, false, out_log, n_cols, lde, lde_stride, lde, lde_stride, 0, stream);
+    };
+    const bool fusable = log_blowup == 1 && log_size - B12 >= 5;
+    // The chain reads evals only, so it can run again for timing unless evals is also an output.
+    const bool rerunnable = evals != coeffs && evals != lde;
+    return tuned_run(TUNE_LDE1, log_size, n_cols, fusable ? 2 : 1, rerunnable, stream, chain);
   }
   const uint32_t b = std::min(log_size, LOW_BITS);
   if (log_size <= b || out_log > LOW_BITS + 12) {

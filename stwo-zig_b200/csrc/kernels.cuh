@@ -101,7 +101,7 @@ struct QuotientBatchDev {
 };
 // Single-size quotient: all columns have log size `log_size` (the lifting size).
 // col_ptrs/coeff_c are device arrays of length n_entries; batches device array.
-cudaError_t accumulate_quotients(const DeviceTables& t, uint32_t log_size, uint32_t n_batches,
+cudaError_t accumulate_quotients(const DeviceTables& t, uint32_t log_size, uint32_t n_batches, uint32_t n_entries,
                                  const QuotientBatchDev* batches, const uint32_t* const* col_ptrs,
                                  const QM31* coeff_c, uint32_t* out, uint64_t out_stride,
                                  cudaStream_t stream);

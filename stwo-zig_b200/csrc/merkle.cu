@@ -15,6 +15,7 @@
 // children, then up to 9 levels per launch.
 #include "blake2s.cuh"
 #include "kernels.cuh"
+#include "tuner.hpp"
 
 namespace sb {
 
@@ -75,7 +76,8 @@ __device__ void fold_levels(uint32_t* sm, uint32_t count, uint32_t levels, uint8
 // Five CTAs per SM (48 registers, 16 bytes spilled): a 2^21 x 100 commit took 0.765 ms,
 // against 0.789 ms at six CTAs per SM (40 registers, 80 bytes spilled), 0.887 ms at four
 // (64 registers, no spills) and 0.953 ms for the unconstrained 62-register build.
-__global__ void __launch_bounds__(LEAF_THREADS, 5) k_merkle_leaves(uint32_t log_size, uint32_t n_cols,
+template <int MINB>
+__global__ void __launch_bounds__(LEAF_THREADS, MINB) k_merkle_leaves(uint32_t log_size, uint32_t n_cols,
                                                                  const uint32_t* __restrict__ cols, uint64_t stride,
                                                                  uint8_t* layers, Seeds seeds, uint32_t levels,
                                                                  uint32_t one) {
@@ -447,10 +449,21 @@ cudaError_t merkle_commit(uint32_t log_size, uint32_t n_cols, const uint32_t* co
   // folding 8 levels took 283 us, 3 levels 245 us and none 254 us.
   uint32_t leaf_levels = log_size <= LEAF_LEVELS ? log_size : FULL_WARP_LEVELS;
   uint32_t grid = (uint32_t)((n_rows + LEAF_THREADS - 1) / LEAF_THREADS);
-  k_merkle_leaves<<<grid, LEAF_THREADS, 0, stream>>>(log_size, n_cols, cols, stride, layers, seeds, leaf_levels, 1u); note_launch();
-  cudaError_t e = cudaGetLastError();
-  if (e != cudaSuccess) return e;
-  return merkle_finish(layers, log_size, log_size - leaf_levels, stream);
+  // Variants: leaf kernels built for 5, 6 and 4 resident CTAs per SM (48, 40 and 64 registers).
+  auto commit = [&](int variant) -> cudaError_t {
+    if (variant == 1)
+      k_merkle_leaves<6><<<grid, LEAF_THREADS, 0, stream>>>(log_size, n_cols, cols, stride, layers, seeds, leaf_levels, 1u);
+    else if (variant == 2)
+      k_merkle_leaves<4><<<grid, LEAF_THREADS, 0, stream>>>(log_size, n_cols, cols, stride, layers, seeds, leaf_levels, 1u);
+    else
+      k_merkle_leaves<5><<<grid, LEAF_THREADS, 0, stream>>>(log_size, n_cols, cols, stride, layers, seeds, leaf_levels, 1u);
+    note_launch();
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    return merkle_finish(layers, log_size, log_size - leaf_levels, stream);
+  };
+  // Trees big enough for the occupancy to matter; the commit only reads the columns.
+  return tuned_run(TUNE_LEAVES, log_size, n_cols, log_size >= 16 ? 3 : 1, true, stream, commit);
 }
 
 cudaError_t merkle_commit_lifted(uint32_t max_log, uint32_t n_cols, const uint32_t* const* col_ptrs,
@@ -516,6 +529,62 @@ PowPrefix pow_prefix(const uint32_t words[8]) {
   return p;
 }
 
+// The grind's message is the 32-byte prefix digest (words 0-7), the nonce (words 8 and 9) and six
+// zero words. These rounds name the message words by token, so an addition of a word that is zero
+// (10-15 always, 9 when every nonce of the round is below 2^32) is not issued at all: 63 additions
+// of the 9 rounds that follow the first, which the generic compression issues because its message
+// words are only known at run time.
+#define SB_PADD_M0(t) SB_ADD(t, w0)
+#define SB_PADD_M1(t) SB_ADD(t, w1)
+#define SB_PADD_M2(t) SB_ADD(t, w2)
+#define SB_PADD_M3(t) SB_ADD(t, w3)
+#define SB_PADD_M4(t) SB_ADD(t, w4)
+#define SB_PADD_M5(t) SB_ADD(t, w5)
+#define SB_PADD_M6(t) SB_ADD(t, w6)
+#define SB_PADD_M7(t) SB_ADD(t, w7)
+#define SB_PADD_M8(t) SB_ADD(t, n_lo)
+#define SB_PADD_M9(t) (HI0 ? (t) : SB_ADD(t, n_hi))
+#define SB_PADD_M10(t) (t)
+#define SB_PADD_M11(t) (t)
+#define SB_PADD_M12(t) (t)
+#define SB_PADD_M13(t) (t)
+#define SB_PADD_M14(t) (t)
+#define SB_PADD_M15(t) (t)
+
+#define SB_POW_G(a, b, c, d, X, Y)                           \
+  do {                                                       \
+    a = SB_PADD_##X(SB_ADD(a, b)); d = rotr32(d ^ a, 16);    \
+    c = SB_ADD(c, d);              b = rotr32(b ^ c, 12);    \
+    a = SB_PADD_##Y(SB_ADD(a, b)); d = rotr32(d ^ a, 8);     \
+    c = SB_ADD(c, d);              b = rotr32(b ^ c, 7);     \
+  } while (0)
+
+#define SB_POW_ROUND(s0, s1, s2, s3, s4, s5, s6, s7, s8, s9, s10, s11, s12, s13, s14, s15) \
+  do {                                                                                    \
+    SB_POW_G(v0, v4, v8, v12, s0, s1);                                                    \
+    SB_POW_G(v1, v5, v9, v13, s2, s3);                                                    \
+    SB_POW_G(v2, v6, v10, v14, s4, s5);                                                   \
+    SB_POW_G(v3, v7, v11, v15, s6, s7);                                                   \
+    SB_POW_G(v0, v5, v10, v15, s8, s9);                                                   \
+    SB_POW_G(v1, v6, v11, v12, s10, s11);                                                 \
+    SB_POW_G(v2, v7, v8, v13, s12, s13);                                                  \
+    SB_POW_G(v3, v4, v9, v14, s14, s15);                                                  \
+  } while (0)
+
+// Rounds 2..10 (sigma rows 1..9 of RFC 7693 section 2.7).
+#define SB_POW_ROUNDS_2_TO_10()                                                           \
+  do {                                                                                    \
+    SB_POW_ROUND(M14, M10, M4, M8, M9, M15, M13, M6, M1, M12, M0, M2, M11, M7, M5, M3);    \
+    SB_POW_ROUND(M11, M8, M12, M0, M5, M2, M15, M13, M10, M14, M3, M6, M7, M1, M9, M4);    \
+    SB_POW_ROUND(M7, M9, M3, M1, M13, M12, M11, M14, M2, M6, M5, M10, M4, M0, M15, M8);    \
+    SB_POW_ROUND(M9, M0, M5, M7, M2, M4, M10, M15, M14, M1, M11, M12, M6, M8, M3, M13);    \
+    SB_POW_ROUND(M2, M12, M6, M10, M0, M11, M8, M3, M4, M13, M7, M5, M15, M14, M1, M9);    \
+    SB_POW_ROUND(M12, M5, M1, M15, M14, M13, M4, M10, M0, M7, M6, M3, M9, M2, M8, M11);    \
+    SB_POW_ROUND(M13, M11, M7, M14, M12, M1, M3, M9, M5, M0, M15, M4, M8, M6, M2, M10);    \
+    SB_POW_ROUND(M6, M15, M14, M9, M11, M3, M0, M8, M12, M2, M13, M7, M1, M4, M10, M5);    \
+    SB_POW_ROUND(M10, M2, M8, M4, M7, M6, M1, M5, M15, M11, M9, M14, M3, M12, M13, M0);    \
+  } while (0)
+
 // One bounded round of the search: nonces [base, base + grid*256*per_thread).
 // Rounds are enqueued in nonce order on one stream; a round starts by leaving
 // at once when an earlier round already found a smaller nonce, and each thread
@@ -528,25 +597,24 @@ PowPrefix pow_prefix(const uint32_t words[8]) {
 // LOW32: for n_bits <= 32 the condition is that the low n_bits of the first hash
 // word are zero, so only that word is live and the compiler drops the last
 // round's work that only feeds the other words.
-template <bool LOW32>
+// HI0: every nonce of the round is below 2^32, so message word 9 is zero.
+template <bool LOW32, bool HI0>
 __global__ void __launch_bounds__(256) k_pow_round(PowPrefix pre, uint32_t n_bits, uint64_t base,
                                                    uint32_t per_thread, unsigned long long* found, uint32_t one) {
   const uint32_t stride = blockDim.x;
   uint64_t nonce = base + (uint64_t)blockIdx.x * blockDim.x * per_thread + threadIdx.x;
   const uint32_t mask = n_bits >= 32 ? 0xffffffffu : (1u << n_bits) - 1u;
+  const uint32_t w0 = pre.w[0], w1 = pre.w[1], w2 = pre.w[2], w3 = pre.w[3], w4 = pre.w[4], w5 = pre.w[5],
+                 w6 = pre.w[6], w7 = pre.w[7];
   unsigned long long best = *((volatile unsigned long long*)found);
   for (uint32_t k = 0; k < per_thread && nonce < best; ++k, nonce += stride) {
-    uint32_t m[16];
-#pragma unroll
-    for (int i = 0; i < 8; ++i) m[i] = pre.w[i];
-    m[8] = (uint32_t)nonce; m[9] = (uint32_t)(nonce >> 32);
-#pragma unroll
-    for (int i = 10; i < 16; ++i) m[i] = 0;
+    const uint32_t n_lo = (uint32_t)nonce, n_hi = (uint32_t)(nonce >> 32);
+    (void)n_hi;
     uint32_t v0 = pre.v[0], v1 = pre.v[1], v2 = pre.v[2], v3 = pre.v[3], v4 = pre.v[4], v5 = pre.v[5],
              v6 = pre.v[6], v7 = pre.v[7], v8 = pre.v[8], v9 = pre.v[9], v10 = pre.v[10], v11 = pre.v[11],
              v12 = pre.v[12], v13 = pre.v[13], v14 = pre.v[14], v15 = pre.v[15];
-    SB_B2S_G(v0, v5, v10, v15, m[8], m[9]);
-    SB_B2S_ROUNDS_2_TO_10();
+    SB_POW_G(v0, v5, v10, v15, M8, M9);
+    SB_POW_ROUNDS_2_TO_10();
     const uint32_t h0 = (B2sIv::v0 ^ 0x01010020u) ^ v0 ^ v8;
     const bool ok = LOW32 ? (h0 & mask) == 0
                           : ctz128(h0, B2sIv::v1 ^ v1 ^ v9, B2sIv::v2 ^ v2 ^ v10, B2sIv::v3 ^ v3 ^ v11) >= n_bits;
@@ -569,10 +637,15 @@ cudaError_t pow_round(const uint32_t prefix_words[8], uint32_t n_bits, uint64_t 
   // 14 nonces per thread, ~0.15 ms a wave) rather than one wave of long ones, so
   // that other streams' work gets SMs between them.
   auto* res = reinterpret_cast<unsigned long long*>(result_dev);
-  if (n_bits <= 32)
-    k_pow_round<true><<<sm_count * 4 * 8, 256, 0, stream>>>(pre, n_bits, base, 14, res, 1u);
-  else
-    k_pow_round<false><<<sm_count * 4 * 8, 256, 0, stream>>>(pre, n_bits, base, 14, res, 1u);
+  const bool hi0 = base + pow_round_nonces(sm_count) <= (1ull << 32);
+  const uint32_t grid = sm_count * 4 * 8;
+  if (n_bits <= 32) {
+    if (hi0) k_pow_round<true, true><<<grid, 256, 0, stream>>>(pre, n_bits, base, 14, res, 1u);
+    else k_pow_round<true, false><<<grid, 256, 0, stream>>>(pre, n_bits, base, 14, res, 1u);
+  } else {
+    if (hi0) k_pow_round<false, true><<<grid, 256, 0, stream>>>(pre, n_bits, base, 14, res, 1u);
+    else k_pow_round<false, false><<<grid, 256, 0, stream>>>(pre, n_bits, base, 14, res, 1u);
+  }
   note_launch();
   return cudaGetLastError();
 }

@@ -437,7 +437,7 @@ int32_t WideFibProver::prove(const ProveRequest& req, std::string& out, StageTim
     SB_CK(cudaMemcpyAsync(b.col_ptrs, hp, nq * sizeof(void*), cudaMemcpyHostToDevice, fs));
     SB_CK(cudaMemcpyAsync(b.batch, hb, sizeof(QuotientBatchDev), cudaMemcpyHostToDevice, fs));
   }
-  SB_CK(accumulate_quotients(T, l.L, 1, b.batch, b.col_ptrs, b.quot_c, b.quot, l.NL, fs));
+  SB_CK(accumulate_quotients(T, l.L, 1, W + 8, b.batch, b.col_ptrs, b.quot_c, b.quot, l.NL, fs));
   SB_CK(cudaEventRecord(ev_[7], fs));
 
   // FRI, last layer, proof of work and queries.

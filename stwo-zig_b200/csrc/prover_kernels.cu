@@ -7,6 +7,7 @@
 // which gives the same canonical result as the reference's term-by-term adds.
 #include "blake2s.cuh"
 #include "kernels.cuh"
+#include "tuner.hpp"
 
 namespace sb {
 
@@ -381,8 +382,8 @@ __global__ void __launch_bounds__(256) k_quotients(PointTable pts, uint32_t log_
 // falls back to per-row inversion so a zero denominator gives the same zero as
 // the one-row kernel). Needs an output aligned to R words and 2^log_size >= R; a
 // CTA that finds a column pointer off the vector alignment loads word by word.
-template <int R, int U>
-__global__ void __launch_bounds__(256, 3) k_quotients_v(PointTable pts, uint32_t log_size, uint32_t n_batches,
+template <int R, int U, int MINB>
+__global__ void __launch_bounds__(256, MINB) k_quotients_v(PointTable pts, uint32_t log_size, uint32_t n_batches,
                                                         const QuotientBatchDev* __restrict__ batches,
                                                         const uint32_t* const* __restrict__ col_ptrs,
                                                         const QM31* __restrict__ coeff_c, uint32_t* out,
@@ -653,27 +654,50 @@ cudaError_t eval_at_point(const DeviceTables&, uint32_t log_size, uint32_t n_col
   return cudaGetLastError();
 }
 
-cudaError_t accumulate_quotients(const DeviceTables& t, uint32_t log_size, uint32_t n_batches,
+template <int R, int U, int MINB>
+static void quotients_smem_attr(size_t smem_v) {
+  cudaFuncSetAttribute(k_quotients_v<R, U, MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_v);
+}
+
+cudaError_t accumulate_quotients(const DeviceTables& t, uint32_t log_size, uint32_t n_batches, uint32_t n_entries,
                                  const QuotientBatchDev* batches, const uint32_t* const* col_ptrs, const QM31* coeff_c,
                                  uint32_t* out, uint64_t out_stride, cudaStream_t stream) {
   size_t smem = QUOT_MAX_ENTRIES * 16;
   size_t smem_v = QUOT_MAX_ENTRIES * (16 + sizeof(void*));
   static const bool attr = [&] {  // once per process (thread-safe static initialisation)
     cudaFuncSetAttribute(k_quotients, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    cudaFuncSetAttribute(k_quotients_v<QUOT_R, QUOT_U>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_v);
+    quotients_smem_attr<QUOT_R, QUOT_U, 3>(smem_v);
+    quotients_smem_attr<QUOT_R, 3, 4>(smem_v);
+    quotients_smem_attr<QUOT_R, 9, 2>(smem_v);
     return true;
   }();
   (void)attr;
   const bool vec = (reinterpret_cast<uintptr_t>(out) & (4 * QUOT_R - 1)) == 0 && out_stride % QUOT_R == 0 &&
                    (1ull << log_size) >= QUOT_R;
-  if (vec)
-    k_quotients_v<QUOT_R, QUOT_U><<<grid_for(1ull << log_size, 256 * QUOT_R), 256, smem_v, stream>>>(
-        PointTable{t.points}, log_size, n_batches, batches, col_ptrs, coeff_c, out, out_stride);
-  else
+  if (!vec) {
     k_quotients<<<grid_for(1ull << log_size, 256), 256, smem, stream>>>(PointTable{t.points}, log_size, n_batches,
                                                                         batches, col_ptrs, coeff_c, out, out_stride);
-  note_launch();
-  return cudaGetLastError();
+    note_launch();
+    return cudaGetLastError();
+  }
+  // Variants: 6 loads in flight per thread at 3 CTAs per SM, 3 at 4, 9 at 2.
+  auto run = [&](int variant) -> cudaError_t {
+    const dim3 grid(grid_for(1ull << log_size, 256 * QUOT_R));
+    const PointTable pts{t.points};
+    if (variant == 1)
+      k_quotients_v<QUOT_R, 3, 4><<<grid, 256, smem_v, stream>>>(pts, log_size, n_batches, batches, col_ptrs, coeff_c,
+                                                                   out, out_stride);
+    else if (variant == 2)
+      k_quotients_v<QUOT_R, 9, 2><<<grid, 256, smem_v, stream>>>(pts, log_size, n_batches, batches, col_ptrs, coeff_c,
+                                                                   out, out_stride);
+    else
+      k_quotients_v<QUOT_R, QUOT_U, 3><<<grid, 256, smem_v, stream>>>(pts, log_size, n_batches, batches, col_ptrs,
+                                                                      coeff_c, out, out_stride);
+    note_launch();
+    return cudaGetLastError();
+  };
+  // Reads the columns, writes `out`: re-runnable. Keyed by the committed columns read per row.
+  return tuned_run(TUNE_QUOTIENTS, log_size, n_entries, log_size >= 16 ? 3 : 1, true, stream, run);
 }
 
 cudaError_t fold_circle_into_line(const DeviceTables& t, uint32_t src_log, const uint32_t* src, uint64_t src_stride,

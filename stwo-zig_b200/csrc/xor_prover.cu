@@ -537,7 +537,7 @@ int32_t LogupXorProver::prove(const XorRequest& req, std::string& out) {
     SB_CK(cudaMemcpyAsync(b.quot_c, hc, at * sizeof(QM31), cudaMemcpyHostToDevice, fs));
     SB_CK(cudaMemcpyAsync(b.col_ptrs, hp, at * sizeof(void*), cudaMemcpyHostToDevice, fs));
     SB_CK(cudaMemcpyAsync(b.batch, hb, batches.size() * sizeof(QuotientBatchDev), cudaMemcpyHostToDevice, fs));
-    SB_CK(accumulate_quotients(T, LDE, (uint32_t)batches.size(), b.batch, b.col_ptrs, b.quot_c, b.quot, NL, fs));
+    SB_CK(accumulate_quotients(T, LDE, (uint32_t)batches.size(), at, b.batch, b.col_ptrs, b.quot_c, b.quot, NL, fs));
   }
 
   // Tail: FRI, proof of work, queries, decommitment.

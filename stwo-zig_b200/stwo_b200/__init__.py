@@ -82,6 +82,10 @@ class StageTimesC(ctypes.Structure):
                                               "host_encode", "host_gaps")]
 
 
+class TuneEntryC(ctypes.Structure):
+    _fields_ = [("op", _u32), ("log_size", _u32), ("n_cols", _u32), ("variant", _i32), ("ms", ctypes.c_float * 4)]
+
+
 class RequestStatsC(ctypes.Structure):
     _fields_ = [("accounted_bytes", _u64), ("workspace_bytes", _u64), ("queued_ms", ctypes.c_double),
                 ("run_ms", ctypes.c_double), ("slot", _u32), ("stages", StageTimesC)]
@@ -130,6 +134,9 @@ _SIGS = {
     "stwo_b200_server_destroy": [_vp],
     "stwo_b200_server_set_request_timeout": [_vp, _u32],
     "stwo_b200_arm_allocation_failure_for_testing": [_u32],
+    "stwo_b200_autotune_mode": [_i32],
+    "stwo_b200_autotune_wide_fibonacci": [_vp, _u32, _u32, _u32],
+    "stwo_b200_autotune_table": [_vp, ctypes.c_size_t, ctypes.POINTER(ctypes.c_size_t)],
     "stwo_b200_xor_lookup_trace": [_vp, _u32, _u64, _vp, _vp, _vp, _vp],
     "stwo_b200_batch_inverse": [_vp, _u32, _u64, _vp, _u64, _vp, _u64, _vp],
     "stwo_b200_logup_interaction": [_vp, _u32, _u32, ctypes.POINTER(LogupUseC), ctypes.POINTER(QM31C), QM31C,
@@ -512,6 +519,11 @@ class Context:
                                                 _ptr(out), 1 << log_rows, ctypes.byref(claimed), _stream(stream)))
         return (claimed.a, claimed.b, claimed.c, claimed.d)
 
+    def autotune_wide_fibonacci(self, log_n_rows: int, sequence_len: int, log_blowup: int = 1) -> None:
+        """Tunes the launch variants of one proof shape with the device otherwise idle (one throwaway
+        proof without proof of work)."""
+        _check(_lib.stwo_b200_autotune_wide_fibonacci(self._h, log_n_rows, sequence_len, log_blowup))
+
     def pow_grind(self, prefix_digest: bytes, n_bits: int) -> int:
         nonce = _u64(0)
         _check(_lib.stwo_b200_pow_grind(self._h, prefix_digest, n_bits, ctypes.byref(nonce)))
@@ -595,3 +607,22 @@ def arm_allocation_failure_for_testing(nth: int) -> None:
     """Makes the library's nth device or pinned allocation from now on fail as out of memory
     (0 disarms); a host-side test hook, no GPU fault is involved."""
     _check(_lib.stwo_b200_arm_allocation_failure_for_testing(nth))
+
+
+AUTOTUNE_OPS = {0: "interpolate+extend high pass (fused, generic)", 1: "Merkle leaves (5, 6, 4 CTAs/SM)",
+                2: "DEEP quotients (6, 3, 9 loads in flight)"}
+
+
+def autotune_mode(mode: int) -> None:
+    """-1: tune each (op, log_size, n_cols) on its first call (the default); v >= 0: force variant v."""
+    _check(_lib.stwo_b200_autotune_mode(mode))
+
+
+def autotune_table() -> list[dict]:
+    """The tuned keys: op, log_size, n_cols, the chosen variant and each variant's measured ms."""
+    n = ctypes.c_size_t(0)
+    _lib.stwo_b200_autotune_table(None, 0, ctypes.byref(n))
+    buf = (TuneEntryC * max(1, n.value))()
+    _check(_lib.stwo_b200_autotune_table(buf, n.value, ctypes.byref(n)))
+    return [{"op": AUTOTUNE_OPS.get(e.op, e.op), "log_size": e.log_size, "n_cols": e.n_cols, "variant": e.variant,
+             "ms": [round(x, 4) for x in e.ms]} for e in buf[:n.value]]

@@ -1,10 +1,11 @@
-"""Fused backend hooks against the sequences of entry points they replace (exact integers):
-stwo_b200_fold_and_commit (foldLineAndCommitNext, the first FRI layer's fold and commit),
-stwo_b200_commit_columns (prepareAndCommitPolys) and stwo_b200_interpolate_secure_composition
-(interpolateSecureComposition). The parts themselves are pinned against the oracle in
-test_gpu_ops.py."""
+"""Fused backend hooks against the sequences of entry points they replace and against the oracle
+directly (exact integers): stwo_b200_fold_and_commit (foldLineAndCommitNext, the first FRI layer's
+fold and commit), stwo_b200_commit_columns (prepareAndCommitPolys) and
+stwo_b200_interpolate_secure_composition (interpolateSecureComposition)."""
 import numpy as np
 import pytest
+
+import oracle
 
 pytestmark = pytest.mark.gpu
 P = 2**31 - 1
@@ -36,6 +37,11 @@ def test_fold_and_commit_equals_fold_then_commit(ctx, circle, src_log):
     assert torch.equal(dst_a, dst_b)
     assert torch.equal(lay_a, lay_b)
     assert root_a == root_b
+    # the oracle: the fold, then the lifted tree of its 4 coordinate columns
+    src_h = src.cpu().numpy().view(np.uint32).reshape(4, -1)
+    want = oracle.fold_circle_into_line(src_h, alpha) if circle else oracle.fold_line(src_h, alpha, src_log)
+    assert np.array_equal(dst_a.cpu().numpy().view(np.uint32).reshape(4, -1), want)
+    assert root_a == oracle.merkle_root(list(want))
     dst_c = torch.empty_like(dst_a)
     assert ctx.fold_and_commit(src, dst_c, src_log, alpha, circle=circle) is None  # fold only
     torch.cuda.synchronize()
@@ -58,6 +64,14 @@ def test_commit_columns_equals_extend_then_commit(ctx, log_size, log_blowup, n_c
     torch.cuda.synchronize()
     assert torch.equal(co_a, co_b) and torch.equal(lde_a, lde_b) and torch.equal(lay_a, lay_b)
     assert root_a == root_b
+    ev_h = ev.cpu().numpy().view(np.uint32).reshape(n_cols, -1)
+    co_h = co_a.cpu().numpy().view(np.uint32).reshape(n_cols, -1)
+    lde_h = lde_a.cpu().numpy().view(np.uint32).reshape(n_cols, -1)
+    want_co = [oracle.interpolate(ev_h[c]) for c in range(n_cols)]
+    want_lde = [oracle.extend(w, log_blowup) for w in want_co]
+    for c in range(n_cols):
+        assert np.array_equal(co_h[c], want_co[c]) and np.array_equal(lde_h[c], want_lde[c]), c
+    assert root_a == oracle.merkle_root(want_lde)
 
 
 @pytest.mark.parametrize("comp_log,log_blowup", [(21, 1), (13, 2), (17, 1)])
@@ -80,6 +94,14 @@ def test_interpolate_secure_composition_equals_its_steps(ctx, comp_log, log_blow
     torch.cuda.synchronize()
     assert torch.equal(comp_a, comp_b)
     assert torch.equal(lde_a, lde_b)
+    ev_h = evals.cpu().numpy().view(np.uint32).reshape(4, -1)
+    co_h = comp_a.cpu().numpy().view(np.uint32).reshape(4, -1)
+    lde_h = lde_a.cpu().numpy().view(np.uint32).reshape(8, -1)
+    for c in range(4):
+        want = oracle.interpolate(ev_h[c])
+        assert np.array_equal(co_h[c], want), c
+        assert np.array_equal(lde_h[c], oracle.extend(want[:half], log_blowup)), c
+        assert np.array_equal(lde_h[4 + c], oracle.extend(want[half:], log_blowup)), c
 
 
 def test_bad_arguments(ctx):

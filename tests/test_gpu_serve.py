@@ -55,6 +55,23 @@ def test_served_proofs_equal_their_single_runs(ctx):
         assert stats["accounted_bytes"] == 16 * r["W"] << r["log_n"]
 
 
+def test_served_proofs_equal_the_oracle(ctx):
+    """Served proofs of mixed shapes and presets, in flight together, against the oracle's bytes."""
+    import stwo_b200 as sb
+    rng = np.random.default_rng(31)
+    reqs = [dict(log_n=int(rng.integers(12, 17)), W=int(rng.choice([16, 32, 100])), preset=p,
+                 trace_seed=int(rng.integers(1, 2**62)), channel_seed=int(rng.integers(0, 2**62)))
+            for p in ("secure", "functional", "secure", "functional", "secure", "functional")]
+    with sb.Server(ctx, slots=4, profile=2) as srv:
+        tickets = [srv.submit(sb.Statement(r["log_n"], r["W"]), _cfg(r["preset"]), trace_kind=sb.TRACE_SEEDED,
+                              trace_seed=r["trace_seed"], channel_seed=r["channel_seed"]) for r in reqs]
+        served = [srv.wait(t)[0] for t in tickets]
+        assert srv.snapshot()["peak_in_flight"] > 1
+    for r, proof in zip(reqs, served):
+        assert proof == oracle.prove_wide_fib(r["log_n"], r["W"], oracle.config(r["preset"]), trace_kind=1,
+                                              trace_seed=r["trace_seed"], channel_seed=r["channel_seed"]), r
+
+
 def test_resource_profile_admission(ctx):
     import stwo_b200 as sb
     g = _cfg("functional")

@@ -301,6 +301,24 @@ pub extern fn stwo_b200_xor_lookup_trace(ctx: *Context, log_n: u32, seed: u64, m
 pub extern fn stwo_b200_pow_grind(ctx: *Context, prefix_digest: *const [32]u8, n_bits: u32, nonce_out: *u64) i32;
 
 // ---------------------------------------------------------------
+// Autotuner
+// ---------------------------------------------------------------
+
+/// stwo_b200_tune_entry
+pub const TuneEntry = extern struct {
+    op: u32,
+    log_size: u32,
+    n_cols: u32,
+    variant: i32,
+    ms: [4]f32,
+};
+
+pub extern fn stwo_b200_autotune_mode(mode: i32) i32;
+pub extern fn stwo_b200_autotune_wide_fibonacci(ctx: *Context, log_n_rows: u32, sequence_len: u32,
+    log_blowup: u32) i32;
+pub extern fn stwo_b200_autotune_table(out: ?[*]TuneEntry, cap: usize, n: *usize) i32;
+
+// ---------------------------------------------------------------
 // Testing
 // ---------------------------------------------------------------
 
