@@ -459,13 +459,19 @@ def main():
                            "nonces": nonce + 1, "ms": pow_ms, "unit": "thread instructions/s",
                            "achieved": hashes_per_s * POW_INSTR_PER_NONCE,
                            "peak": 148 * 128 * 1e6 * (clocks.summary().get("sm_mhz") or 1965.0),
-                           "peak_source": "148 SMs x 128 lanes issue x sampled SM clock (nominal)"},
+                           "peak_source": "148 SMs x 128 lanes issue x sampled SM clock (nominal)",
+                           "alu_pipe": {"alu_instr_per_nonce": POW_ALU_INSTR_PER_NONCE,
+                                        "bound_hashes_per_s": 148 * 4 * 16 * 1e6 * (clocks.summary().get("sm_mhz")
+                                                                                    or 1965.0) / POW_ALU_INSTR_PER_NONCE,
+                                        "source": "XOR and rotate run on the ALU pipe, 16 lanes per scheduler per "
+                                                  "cycle; ncu smsp__inst_executed_pipe_alu.sum of a full round"}},
         "gpu_launches": launches,
         "autotune": sb.autotune_table(),
         "clocks": clocks.summary(),
     }
     ri = out["roofline_int32"]
     ri["frac"] = ri["achieved"] / ri["peak"]
+    ri["alu_pipe"]["frac"] = hashes_per_s / ri["alu_pipe"]["bound_hashes_per_s"]
     if out["roofline_issue"]:
         out["roofline_issue"]["frac"] = out["roofline_issue"]["achieved"] / out["roofline_issue"]["peak"]
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -769,11 +775,14 @@ def ceiling_block(measured, serial, pow_bound, note=None):
 # scaled to 100 columns; traffic is linear in the column count.
 FFT_TRAFFIC_BYTES: dict = {(20, 100): 1532.3e6 * 100 / 40}
 # Thread instructions per nonce of the grind (one ncu capture of a full 26-bit round:
-# 532.2 M warp instructions x 32 / 16,973,824 nonces).
-POW_INSTR_PER_NONCE = 1003
+# 499.9 M warp instructions x 32 / 16,973,824 nonces).
+POW_INSTR_PER_NONCE = 943
+# Of those, ALU-pipe instructions (smsp__inst_executed_pipe_alu.sum, 300.9 M warp instructions): the
+# XORs and rotations; the additions run on the FMA pipe.
+POW_ALU_INSTR_PER_NONCE = 567
 # Warp instructions of one interpolate + blow-up extend of a 2^20 column (ncu smsp__inst_executed.sum
-# of k_fft_low12<1> + k_fft_high16_lde1<8> + k_fft_low12<0>: 242.5 M + 470.0 M + 486.2 M for 100 columns).
-FFT_WARP_INSTR_PER_COL_2P20 = 1_198_700_000 // 100
+# of k_fft_low12<1> + k_fft_high16_lde1<8> + k_fft_low12<0>: 203.2 M + 391.0 M + 408.4 M for 100 columns).
+FFT_WARP_INSTR_PER_COL_2P20 = 1_002_496_000 // 100
 
 if __name__ == "__main__":
     main()

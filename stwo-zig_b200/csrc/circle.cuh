@@ -85,6 +85,7 @@ SB_HD uint32_t bitrev(uint32_t i, uint32_t log_size) {
 // reads tower layers R-L .. R-1.
 struct TwiddleView {
   const uint32_t* tower;  // forward or inverse
+  const uint32_t* tower2; // the same tower's entries doubled (2t < 2^32, not reduced mod p)
   uint32_t root_log;      // R
   uint32_t line_log;      // L
   uint32_t y0;            // y (or 1/y) of halfOdds(L)'s first point, for L <= 1

@@ -209,11 +209,12 @@ __global__ void k_fft_high(HighParams p) {
   }
 }
 
+// Entries 2^R .. 2^(R+1) of tw and itw are the doubled copies (tw2, itw2).
 __global__ void k_build_tower(PointTable pts, uint32_t R, uint32_t* tw, uint32_t* itw) {
   // Entry e < 2^R - 1 belongs to layer k with offset 2^R - 2^(R-k).
   uint64_t total = 1ull << R;
   for (uint64_t e = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; e < total; e += (uint64_t)gridDim.x * blockDim.x) {
-    if (e == total - 1) { tw[e] = 1; itw[e] = 1; continue; }
+    if (e == total - 1) { tw[e] = 1; itw[e] = 1; tw[total + e] = 2; itw[total + e] = 2; continue; }
     // k = number of leading ones of e in R bits
     uint32_t k = 0;
     while ((e >> (R - 1 - k)) & 1) ++k;
@@ -223,8 +224,11 @@ __global__ void k_build_tower(PointTable pts, uint32_t R, uint32_t* tw, uint32_t
     Coset c = coset_half_odds(R - k);
     uint32_t nat = bitrev(i, len_log);
     uint32_t x = pts.at(c.index_at(nat)).x;
+    const uint32_t ix = minv(x);
     tw[e] = x;
-    itw[e] = minv(x);
+    itw[e] = ix;
+    tw[total + e] = 2 * x;
+    itw[total + e] = 2 * ix;
   }
 }
 
@@ -560,6 +564,7 @@ inline uint32_t inv_pow2(uint32_t log) { return minv(1u << log); }
 TwiddleView DeviceTables::view(uint32_t domain_log, bool inverse) const {
   TwiddleView v;
   v.tower = inverse ? itw : tw;
+  v.tower2 = inverse ? itw2 : tw2;
   v.root_log = tower_log;
   v.line_log = domain_log - 1;
   v.y0 = 0;

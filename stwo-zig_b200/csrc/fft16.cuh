@@ -5,7 +5,11 @@
 // the transform index, applies up to 4 butterfly layers of that window in
 // registers, and exchanges elements with other threads through shared memory
 // between windows. Twiddles of one window come from one to two vector loads
-// per layer (the elements of a window share consecutive twiddle blocks).
+// per layer (the elements of a window share consecutive twiddle blocks), read
+// from the doubled tower (TwiddleView::tower2): with t2 = 2t the 64-bit
+// product a * t2 = 2at holds at >> 31 in its high word and (at mod 2^31) << 1
+// in its low word, so the product's reduction needs no mask and no 64-bit
+// shift.
 //
 // Shared-memory positions are swizzled by swz(i) = i ^ (16*parity(i>>5) ^ ((i>>5)&15)).
 // swz is linear over GF(2), so the position of element k of a thread is
@@ -28,11 +32,34 @@ __host__ __device__ __forceinline__ uint32_t swz(uint32_t i) {
   return i ^ ((par << 4) ^ (v & 15));
 }
 
-// `n` consecutive twiddles of line layer s (s >= 1) starting at block h0
+// a * t mod p for a < p and t2 = 2t, t < p. With 2at = hi * 2^32 + lo (lo even),
+// at = hi * 2^31 + lo / 2 = hi + lo / 2 (mod p); hi <= 2^31 - 4 and lo / 2 < 2^31,
+// so the sum is below 2p and one conditional subtraction makes it canonical.
+__device__ __forceinline__ uint32_t mmul2(uint32_t a, uint32_t t2) {
+  const uint64_t x = (uint64_t)a * t2;
+  const uint32_t s = (uint32_t)(x >> 32) + ((uint32_t)x >> 1);
+  return umin32(s, s - P);
+}
+// Negation of a doubled twiddle: 2(p - t) = 2p - 2t, and 0 for t = 0.
+__device__ __forceinline__ uint32_t mneg2(uint32_t t2) { return t2 == 0 ? 0 : 2 * P - t2; }
+
+// The butterflies of field.cuh with the twiddle given doubled.
+__device__ __forceinline__ void butterfly2(uint32_t& v0, uint32_t& v1, uint32_t t2) {
+  const uint32_t m = mmul2(v1, t2);
+  v1 = msub(v0, m);
+  v0 = madd(v0, m);
+}
+__device__ __forceinline__ void ibutterfly2(uint32_t& v0, uint32_t& v1, uint32_t it2) {
+  const uint32_t a = v0;
+  v0 = madd(a, v1);
+  v1 = mmul2(msub(a, v1), it2);
+}
+
+// `n` consecutive doubled twiddles of line layer s (s >= 1) starting at block h0
 // (h0 is a multiple of n, the layer offset a multiple of 16 bytes).
 template <int N>
 __device__ __forceinline__ void load_line(const TwiddleView& tv, uint32_t s, uint64_t h0, uint32_t (&tw)[8]) {
-  const uint32_t* p = tv.tower + ((1u << tv.root_log) - (1u << (tv.line_log - s + 1))) + h0;
+  const uint32_t* p = tv.tower2 + ((1u << tv.root_log) - (1u << (tv.line_log - s + 1))) + h0;
   if (N == 8) {
     uint4 a = __ldg(reinterpret_cast<const uint4*>(p)), b = __ldg(reinterpret_cast<const uint4*>(p) + 1);
     tw[0] = a.x; tw[1] = a.y; tw[2] = a.z; tw[3] = a.w; tw[4] = b.x; tw[5] = b.y; tw[6] = b.z; tw[7] = b.w;
@@ -47,13 +74,13 @@ __device__ __forceinline__ void load_line(const TwiddleView& tv, uint32_t s, uin
   }
 }
 
-// Circle-layer twiddles of 8 consecutive pairs h0 .. h0+7 (h0 a multiple of 8):
+// Doubled circle-layer twiddles of 8 consecutive pairs h0 .. h0+7 (h0 a multiple of 8):
 // pattern [y, -y, -x, x] over the (x, y) pairs of line layer 0.
 __device__ __forceinline__ void load_circle8(const TwiddleView& tv, uint64_t h0, uint32_t (&tw)[8]) {
-  const uint32_t* l0 = tv.tower + ((1u << tv.root_log) - (1u << tv.line_log));
+  const uint32_t* l0 = tv.tower2 + ((1u << tv.root_log) - (1u << tv.line_log));
   uint4 q = __ldg(reinterpret_cast<const uint4*>(l0 + (h0 >> 1)));
-  tw[0] = q.y; tw[1] = mneg(q.y); tw[2] = mneg(q.x); tw[3] = q.x;
-  tw[4] = q.w; tw[5] = mneg(q.w); tw[6] = mneg(q.z); tw[7] = q.z;
+  tw[0] = q.y; tw[1] = mneg2(q.y); tw[2] = mneg2(q.x); tw[3] = q.x;
+  tw[4] = q.w; tw[5] = mneg2(q.w); tw[6] = mneg2(q.z); tw[7] = q.z;
 }
 
 // Applies window layers j in [JLO, JHI) to x (element k at transform index
@@ -76,8 +103,8 @@ __device__ __forceinline__ void layer16(uint32_t (&x)[16], const TwiddleView& tv
   for (int k = 0; k < 16; ++k) {
     if (k & (1 << J)) continue;
     const uint32_t t = tw[k >> (J + 1)];
-    if (INV) ibutterfly(x[k], x[k | (1 << J)], t);
-    else butterfly(x[k], x[k | (1 << J)], t);
+    if (INV) ibutterfly2(x[k], x[k | (1 << J)], t);
+    else butterfly2(x[k], x[k | (1 << J)], t);
   }
 }
 

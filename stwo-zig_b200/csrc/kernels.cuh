@@ -24,6 +24,10 @@ struct DeviceTables {
   PointM* points = nullptr;    // point table (circle.cuh)
   uint32_t* tw = nullptr;      // forward twiddle tower
   uint32_t* itw = nullptr;     // inverse twiddle tower
+  // Both towers doubled (2t as an integer below 2^32), for the radix-16 butterflies (fft16.cuh);
+  // they live in the second halves of the tw / itw allocations.
+  uint32_t* tw2 = nullptr;
+  uint32_t* itw2 = nullptr;
   uint32_t tower_log = 0;      // R: root half coset halfOdds(R)
   uint32_t sm_count = 148;     // multiprocessors of the device (persistent grid sizes)
   TwiddleView view(uint32_t domain_log, bool inverse) const;

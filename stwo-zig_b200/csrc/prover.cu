@@ -131,8 +131,10 @@ int32_t Context::init(int dev, uint32_t tower_log) {
   if (cudaMemcpy(tables.points, pts.data(), pts.size() * sizeof(PointM), cudaMemcpyHostToDevice) != cudaSuccess)
     return E_CUDA;
   size_t tw_words = (size_t)1 << tower_log;
-  if (cudaMalloc(&tables.tw, tw_words * 4) != cudaSuccess) return E_OOM;
-  if (cudaMalloc(&tables.itw, tw_words * 4) != cudaSuccess) return E_OOM;
+  if (cudaMalloc(&tables.tw, tw_words * 8) != cudaSuccess) return E_OOM;
+  if (cudaMalloc(&tables.itw, tw_words * 8) != cudaSuccess) return E_OOM;
+  tables.tw2 = tables.tw + tw_words;
+  tables.itw2 = tables.itw + tw_words;
   if (build_twiddle_tower(tables, tower_log, stream) != cudaSuccess) return E_CUDA;
   if (cudaStreamSynchronize(stream) != cudaSuccess) return E_CUDA;
   return OK;
