@@ -60,6 +60,9 @@ def parse():
     ap.add_argument("--rates", default="25,50,100,200,400")
     ap.add_argument("--requests", type=int, default=64)
     ap.add_argument("--slots", type=int, default=8)
+    ap.add_argument("--autotune", type=int, default=-1,
+                    help="-1: tune launch variants per shape (default); v >= 0: run variant v everywhere, "
+                         "untuned (for profiler captures, under which the tuner's timings mean nothing)")
     return ap.parse_args()
 
 
@@ -239,7 +242,10 @@ def main():
     n_words = args.width << args.log_n
     K, W = args.steps, args.warmup
     # Launch variants tuned for this shape with the device otherwise idle (part of the warm-up).
-    ctx.autotune_wide_fibonacci(args.log_n, args.width, cfg.fri_config.log_blowup_factor)
+    if args.autotune >= 0:
+        sb.autotune_mode(args.autotune)
+    else:
+        ctx.autotune_wide_fibonacci(args.log_n, args.width, cfg.fri_config.log_blowup_factor)
 
     def barrier():
         if world > 1:
@@ -466,7 +472,7 @@ def main():
                                         "source": "XOR and rotate run on the ALU pipe, 16 lanes per scheduler per "
                                                   "cycle; ncu smsp__inst_executed_pipe_alu.sum of a full round"}},
         "gpu_launches": launches,
-        "autotune": sb.autotune_table(),
+        "autotune": sb.autotune_table() if args.autotune < 0 else {"forced_variant": args.autotune},
         "clocks": clocks.summary(),
     }
     ri = out["roofline_int32"]
