@@ -777,9 +777,9 @@ def ceiling_block(measured, serial, pow_bound, note=None):
 
 
 # DRAM bytes (read + write) of one FFT pass (the 3-kernel interpolate+extend chain) from one ncu
-# capture of 2^20 rows x 40 columns (dram__bytes_read.sum + dram__bytes_write.sum = 1532.3 MB, k_fft_low12<1> + k_fft_high16_lde1<8> + k_fft_low12<0>),
+# capture of 2^20 rows x 40 columns (dram__bytes_read.sum + dram__bytes_write.sum = 1533.6 MB, k_fft_low12<1> + k_fft_high16_lde1<8> + k_fft_low12<0>),
 # scaled to 100 columns; traffic is linear in the column count.
-FFT_TRAFFIC_BYTES: dict = {(20, 100): 1532.3e6 * 100 / 40}
+FFT_TRAFFIC_BYTES: dict = {(20, 100): 1533.6e6 * 100 / 40}
 # Thread instructions per nonce of the grind (one ncu capture of a full 26-bit round:
 # 499.9 M warp instructions x 32 / 16,973,824 nonces).
 POW_INSTR_PER_NONCE = 943

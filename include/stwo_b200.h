@@ -473,6 +473,13 @@ int32_t stwo_b200_autotune_table(stwo_b200_tune_entry* out, size_t cap, size_t* 
  * (armOwnershipTransferFailureForTesting, src/backends/metal/commit_backend.zig:69-71). */
 int32_t stwo_b200_arm_allocation_failure_for_testing(uint32_t nth);
 
+/* Makes the next launch of the bulk-staged DEEP quotient kernel (the quotient variant that copies
+ * column chunks into shared memory with bulk async copies) leave its first stage empty in every CTA:
+ * each bounded wait on it runs out after about a second, the kernel sets its timeout status and
+ * returns, and the proof (or the op) ends with STWO_B200_E_CUDA and a message saying so. No copy
+ * faults and no wait is unbounded; the context stays usable. */
+int32_t stwo_b200_arm_quotient_stage_timeout_for_testing(void);
+
 #ifdef __cplusplus
 }
 #endif

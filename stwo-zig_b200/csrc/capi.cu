@@ -409,17 +409,36 @@ int32_t stwo_b200_accumulate_quotients(stwo_b200_context* ctx, uint32_t log_size
   hb.sum_b = q(sum_b);
   hb.first = 0;
   hb.count = n_cols;
+  // The column pointers are read back so that 16-byte aligned columns may take the bulk-staged
+  // kernel, whose status word sits after the batch descriptor.
+  std::vector<const uint32_t*> hptr(n_cols);
+  cudaError_t e = cudaMemcpyAsync(hptr.data(), col_ptrs_dev, n_cols * sizeof(void*), cudaMemcpyDeviceToHost, st(stream));
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st(stream));
+  if (e != cudaSuccess) return cuda_status(e, "quotient column pointers");
+  bool aligned = true;
+  for (const uint32_t* p : hptr) aligned = aligned && (reinterpret_cast<uintptr_t>(p) & 15) == 0;
+  constexpr size_t STATUS_OFF = (sizeof(sb::QuotientBatchDev) + 15) & ~size_t(15);
   void* dbatch = nullptr;
-  cudaError_t e = cudaMallocAsync(&dbatch, sizeof(hb), st(stream));
+  e = cudaMallocAsync(&dbatch, STATUS_OFF + 16, st(stream));
   if (e != cudaSuccess) return cuda_status(e, "quotient batch");
+  uint32_t* dstatus = reinterpret_cast<uint32_t*>(static_cast<uint8_t*>(dbatch) + STATUS_OFF);
   e = cudaMemcpyAsync(dbatch, &hb, sizeof(hb), cudaMemcpyHostToDevice, st(stream));
+  if (e == cudaSuccess) e = cudaMemsetAsync(dstatus, 0, sizeof(uint32_t), st(stream));
   if (e == cudaSuccess)
     e = sb::accumulate_quotients(ctx->ctx.tables, log_size, 1, n_cols, static_cast<sb::QuotientBatchDev*>(dbatch), col_ptrs_dev,
-                                 reinterpret_cast<const sb::QM31*>(c_dev), out, out_stride, st(stream));
+                                 reinterpret_cast<const sb::QM31*>(c_dev), out, out_stride, st(stream),
+                                 aligned ? dstatus : nullptr);
+  uint32_t status = 0;
+  if (e == cudaSuccess) e = cudaMemcpyAsync(&status, dstatus, sizeof(status), cudaMemcpyDeviceToHost, st(stream));
   cudaError_t e2 = cudaStreamSynchronize(st(stream));  // the batch descriptor lives on this host frame
   cudaFreeAsync(dbatch, st(stream));
   if (e != cudaSuccess) return cuda_status(e, "accumulate_quotients");
-  return cuda_status(e2, "accumulate_quotients sync");
+  if (e2 != cudaSuccess) return cuda_status(e2, "accumulate_quotients sync");
+  if (status != 0)
+    return set_error(STWO_B200_E_CUDA, (status & sb::QUOT_STATUS_TIMEOUT)
+                                           ? "a staged column load of the quotient kernel ran out of time"
+                                           : "the quotient batches do not fit the staged kernel's item table");
+  return STWO_B200_OK;
 }
 
 int32_t stwo_b200_wide_fib_trace(stwo_b200_context* ctx, uint32_t log_n_rows, uint32_t sequence_len,
@@ -659,6 +678,11 @@ int32_t stwo_b200_autotune_table(stwo_b200_tune_entry* out, size_t cap, size_t* 
   if (t.size() > cap || (t.size() && !out)) return set_error(STWO_B200_E_BUFFER_TOO_SMALL, "autotune table buffer too small");
   static_assert(sizeof(sb::TuneEntry) == sizeof(stwo_b200_tune_entry), "tune entry layout");
   if (!t.empty()) std::memcpy(out, t.data(), t.size() * sizeof(sb::TuneEntry));
+  return STWO_B200_OK;
+}
+
+int32_t stwo_b200_arm_quotient_stage_timeout_for_testing(void) {
+  sb::arm_quotient_stage_timeout_for_testing();
   return STWO_B200_OK;
 }
 

@@ -105,10 +105,18 @@ struct QuotientBatchDev {
 };
 // Single-size quotient: all columns have log size `log_size` (the lifting size).
 // col_ptrs/coeff_c are device arrays of length n_entries; batches device array.
+// `status` (device word, may be null): a caller that passes one vouches that every column pointer is
+// 16-byte aligned, which makes the bulk-staged kernel one of the tuned variants; that kernel ORs
+// QUOT_STATUS_* bits into it when a staged load runs out of time or the batches do not fit its
+// item table, and its output is then not valid.
+constexpr uint32_t QUOT_STATUS_TIMEOUT = 2, QUOT_STATUS_LAYOUT = 4;
 cudaError_t accumulate_quotients(const DeviceTables& t, uint32_t log_size, uint32_t n_batches, uint32_t n_entries,
                                  const QuotientBatchDev* batches, const uint32_t* const* col_ptrs,
                                  const QM31* coeff_c, uint32_t* out, uint64_t out_stride,
-                                 cudaStream_t stream);
+                                 cudaStream_t stream, uint32_t* status = nullptr);
+// Test hook: the next bulk-staged quotient launch leaves its first stage empty in every CTA, so that
+// its bounded waits run out (status QUOT_STATUS_TIMEOUT).
+void arm_quotient_stage_timeout_for_testing();
 
 // ---- FRI folds (src/core/fri/folding.zig:352-602) --------------------------
 cudaError_t fold_circle_into_line(const DeviceTables& t, uint32_t src_log, const uint32_t* src,
@@ -136,7 +144,8 @@ struct FriChannelDev {
   uint32_t digest[8];
   uint32_t n_draws;
   uint32_t status;  // nonzero: a draw was rejected FRI_DRAW_TRIES times in a row
-  uint32_t pad[2];
+  uint32_t quot_status;  // QUOT_STATUS_* of the proof's quotient launch (cleared before it)
+  uint32_t pad;
   QM31 alpha[FRI_MAX_LAYERS];
   uint32_t roots[FRI_MAX_LAYERS][8];
 };

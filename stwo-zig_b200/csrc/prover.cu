@@ -439,7 +439,10 @@ int32_t WideFibProver::prove(const ProveRequest& req, std::string& out, StageTim
     SB_CK(cudaMemcpyAsync(b.col_ptrs, hp, nq * sizeof(void*), cudaMemcpyHostToDevice, fs));
     SB_CK(cudaMemcpyAsync(b.batch, hb, sizeof(QuotientBatchDev), cudaMemcpyHostToDevice, fs));
   }
-  SB_CK(accumulate_quotients(T, l.L, 1, W + 8, b.batch, b.col_ptrs, b.quot_c, b.quot, l.NL, fs));
+  // The workspace columns start 16-byte aligned: the bulk-staged quotient kernel may run, its status
+  // read back with the FRI channel.
+  SB_CK(cudaMemsetAsync(&b.chan->quot_status, 0, sizeof(uint32_t), fs));
+  SB_CK(accumulate_quotients(T, l.L, 1, W + 8, b.batch, b.col_ptrs, b.quot_c, b.quot, l.NL, fs, &b.chan->quot_status));
   SB_CK(cudaEventRecord(ev_[7], fs));
 
   // FRI, last layer, proof of work and queries.

@@ -55,6 +55,11 @@ int32_t fri_pow_queries(const DeviceTables& T, int sm_count, Channel& ch, const 
     out.gap_start = Clock::now();
     FriChannelDev dc;
     std::memcpy(&dc, pin, sizeof(dc));
+    if (dc.quot_status != 0) {
+      err = (dc.quot_status & QUOT_STATUS_TIMEOUT) ? "a staged column load of the quotient kernel ran out of time"
+                                                    : "the quotient batches do not fit the staged kernel's item table";
+      return E_CUDA;
+    }
     for (uint32_t k = 0; k <= n_inner; ++k) {
       std::array<uint8_t, 32> r;
       std::memcpy(r.data(), dc.roots[k], 32);

@@ -5,6 +5,8 @@
 // Sums of QM31 x M31 products are accumulated lazily per coordinate in 64-bit
 // registers (each product < 2^62, folded every third term) and reduced once,
 // which gives the same canonical result as the reference's term-by-term adds.
+#include <atomic>
+
 #include "blake2s.cuh"
 #include "kernels.cuh"
 #include "tuner.hpp"
@@ -228,12 +230,14 @@ __device__ QM31 subset_product(const OodsFactors& F, uint32_t bits, uint32_t fir
   return r;
 }
 
-// A CTA owns one column and a strided set of its 4096-coefficient chunks. Thread t
-// sums its 16 coefficients of a chunk against the subset products of F_0..F_3,
-// multiplies by the chunk's product of F_12.. (a table built in shared memory by
-// doubling) and accumulates; at the end it multiplies by its own factor (F_4..F_11
-// subset selected by t) and the CTA reduces with warp shuffles to one partial.
-constexpr uint32_t OODS_SMEM_CHUNKS = 1024;  // hi-factor table entries kept in shared memory
+// A CTA owns one column and a strided set of its 4096-coefficient chunks: chunk = blockIdx.x +
+// k * gridDim.x with gridDim.x a power of two, so a chunk's product of F_12.. splits over disjoint
+// bits into the CTA's part (the bits of blockIdx.x, multiplied in once at the end) and k's part
+// (a table hk[k] in shared memory, each entry a direct product computed by one thread: one barrier).
+// Thread t sums its 16 coefficients of a chunk against the subset products of F_0..F_3, multiplies
+// by hk[k] and accumulates; at the end it multiplies by the CTA's factor and its own (F_4..F_11
+// subset selected by t), and the CTA reduces with warp shuffles to one partial.
+constexpr uint32_t OODS_SMEM_CHUNKS = 1024;  // per-CTA chunk-factor table entries kept in shared memory
 
 __device__ __forceinline__ QM31 shfl_down_q(QM31 v, int d) {
   return qmake(__shfl_down_sync(0xffffffffu, v.c0.a, d), __shfl_down_sync(0xffffffffu, v.c0.b, d),
@@ -243,11 +247,13 @@ __device__ __forceinline__ QM31 shfl_down_q(QM31 v, int d) {
 __global__ void __launch_bounds__(OODS_THREADS) k_oods_chunks(OodsFactors F, const uint32_t* __restrict__ coeffs,
                                                               uint64_t stride, QM31* partial, uint32_t n_chunks) {
   __shared__ QM31 b4[3][16];
-  __shared__ QM31 hi[OODS_SMEM_CHUNKS];
+  __shared__ QM31 hk[OODS_SMEM_CHUNKS];
   __shared__ QM31 wsum[OODS_THREADS / 32];
   const uint32_t col = blockIdx.y;
   const uint32_t L = F.log_size;
   const uint32_t chunk_bits = L < OODS_CHUNK_BITS ? L : OODS_CHUNK_BITS;
+  const uint32_t g_bits = __ffs(gridDim.x) - 1;  // gridDim.x = 2^g_bits
+  const uint32_t k_first = chunk_bits + g_bits;   // factor index of k's bit 0
   if (threadIdx.x < 48) {
     uint32_t lvl = threadIdx.x / 16, r = threadIdx.x % 16;
     // factors beyond log_size do not exist; mask them out
@@ -255,21 +261,17 @@ __global__ void __launch_bounds__(OODS_THREADS) k_oods_chunks(OodsFactors F, con
     uint32_t valid_bits = first >= chunk_bits ? 0 : (chunk_bits - first >= 4 ? 4 : chunk_bits - first);
     b4[lvl][r] = (r >> valid_bits) ? qzero() : subset_product(F, r, first);
   }
-  // hi[c] = prod of F[chunk_bits + b] over the set bits b of c, by doubling.
-  const uint32_t n_tab = n_chunks < OODS_SMEM_CHUNKS ? n_chunks : OODS_SMEM_CHUNKS;
-  if (threadIdx.x == 0) hi[0] = qone();
+  const uint32_t n_k = blockIdx.x < n_chunks ? (n_chunks - 1 - blockIdx.x) / gridDim.x + 1 : 0;
+  const uint32_t n_tab = n_k < OODS_SMEM_CHUNKS ? n_k : OODS_SMEM_CHUNKS;
+  for (uint32_t k = threadIdx.x; k < n_tab; k += blockDim.x) hk[k] = subset_product(F, k, k_first);
   __syncthreads();
-  for (uint32_t half = 1, b = 0; half < n_tab; half <<= 1, ++b) {
-    for (uint32_t i = threadIdx.x; i < half; i += blockDim.x) hi[half + i] = qmul(hi[i], F.f[chunk_bits + b]);
-    __syncthreads();
-  }
   const uint32_t n_in = 1u << chunk_bits;
   const uint32_t t = threadIdx.x;
   const bool active = 16 * t < n_in;
   const uint32_t nw = active ? (n_in - 16 * t < 16 ? n_in - 16 * t : 16) : 0;
   QM31 acc = qzero();
-  for (uint32_t chunk = blockIdx.x; chunk < n_chunks; chunk += gridDim.x) {
-    if (!active) break;
+  for (uint32_t k = 0; k < n_k && active; ++k) {
+    const uint32_t chunk = blockIdx.x + k * gridDim.x;
     const uint32_t* c = coeffs + col * stride + ((uint64_t)chunk << chunk_bits) + 16 * t;
     uint32_t w[16];
     if (nw == 16) {
@@ -292,17 +294,19 @@ __global__ void __launch_bounds__(OODS_THREADS) k_oods_chunks(OodsFactors F, con
     }
     QM31 v = qmake(mreduce64(a0), mreduce64(a1), mreduce64(a2), mreduce64(a3));
     QM31 h;
-    if (chunk < OODS_SMEM_CHUNKS) {
-      h = hi[chunk];
-    } else {  // chunks beyond the table: low bits from the table, the rest multiplied in
-      h = hi[chunk & (OODS_SMEM_CHUNKS - 1)];
-      uint32_t bits = chunk >> 10;
-      for (uint32_t b = 10; bits; ++b, bits >>= 1)
-        if (bits & 1) h = qmul(h, F.f[chunk_bits + b]);
+    if (k < OODS_SMEM_CHUNKS) {
+      h = hk[k];
+    } else {  // beyond the table: its low bits from the table, the rest multiplied in
+      h = hk[k & (OODS_SMEM_CHUNKS - 1)];
+      uint32_t bits = k >> 10;
+      for (uint32_t b = k_first + 10; bits; ++b, bits >>= 1)
+        if (bits & 1) h = qmul(h, F.f[b]);
     }
     acc = qadd(acc, qmul(v, h));
   }
-  // own factor: subset of F_4..F_7 by bits 0-3 of t, of F_8..F_11 by bits 4-7
+  // the CTA's factor (bits of blockIdx.x), then the thread's own: subset of F_4..F_7 by bits 0-3
+  // of t, of F_8..F_11 by bits 4-7
+  acc = qmul(acc, subset_product(F, blockIdx.x, chunk_bits));
   acc = qmul(acc, qmul(b4[1][t & 15], b4[2][t >> 4]));
 #pragma unroll
   for (int d = 16; d >= 1; d >>= 1) acc = qadd(acc, shfl_down_q(acc, d));
@@ -373,6 +377,40 @@ __global__ void __launch_bounds__(256) k_quotients(PointTable pts, uint32_t log_
     out[out_stride + row] = acc.c0.b;
     out[2 * out_stride + row] = acc.c1.a;
     out[3 * out_stride + row] = acc.c1.b;
+  }
+}
+
+// Adds one batch's quotient to R rows: the numerators accumulated in `a` (lazy 64-bit sums of
+// c_i v_i(row)) minus the batch's linear term, times the inverse denominators, the R rows'
+// denominators inverted together.
+template <int R>
+__device__ __forceinline__ void quot_batch_finish(const QuotientBatchDev& bt, const PointM (&dp)[R],
+                                                  const uint64_t (&a)[R][4], QM31 (&acc)[R]) {
+  CM31 prx = bt.point.x.c0, pry = bt.point.y.c0, pix = bt.point.x.c1, piy = bt.point.y.c1;
+  CM31 den[R], pre[R];
+#pragma unroll
+  for (int j = 0; j < R; ++j) {
+    den[j] = csub(cmul(csub(prx, CM31{dp[j].x, 0}), piy), cmul(csub(pry, CM31{dp[j].y, 0}), pix));
+    pre[j] = j == 0 ? den[0] : cmul(pre[j - 1], den[j]);
+  }
+  CM31 inv[R];
+  if (pre[R - 1].a == 0 && pre[R - 1].b == 0) {
+#pragma unroll
+    for (int j = 0; j < R; ++j) inv[j] = cinv(den[j]);
+  } else {
+    CM31 t = cinv(pre[R - 1]);
+#pragma unroll
+    for (int j = R - 1; j >= 1; --j) {
+      inv[j] = cmul(t, pre[j - 1]);
+      t = cmul(t, den[j]);
+    }
+    inv[0] = t;
+  }
+#pragma unroll
+  for (int j = 0; j < R; ++j) {
+    QM31 num = qmake(mreduce64(a[j][0]), mreduce64(a[j][1]), mreduce64(a[j][2]), mreduce64(a[j][3]));
+    num = qsub(num, qadd(qmulm(bt.sum_a, dp[j].y), bt.sum_b));
+    acc[j] = qadd(acc[j], qmulc(num, inv[j]));
   }
 }
 
@@ -456,32 +494,7 @@ __global__ void __launch_bounds__(256, MINB) k_quotients_v(PointTable pts, uint3
         step(load(sptr[e0 + i] + row0), sqe[e0 + i]);
         if (t % 3 == 2) fold();
       }
-      CM31 prx = bt.point.x.c0, pry = bt.point.y.c0, pix = bt.point.x.c1, piy = bt.point.y.c1;
-      CM31 den[R], pre[R];
-#pragma unroll
-      for (int j = 0; j < R; ++j) {
-        den[j] = csub(cmul(csub(prx, CM31{dp[j].x, 0}), piy), cmul(csub(pry, CM31{dp[j].y, 0}), pix));
-        pre[j] = j == 0 ? den[0] : cmul(pre[j - 1], den[j]);
-      }
-      CM31 inv[R];
-      if (pre[R - 1].a == 0 && pre[R - 1].b == 0) {
-#pragma unroll
-        for (int j = 0; j < R; ++j) inv[j] = cinv(den[j]);
-      } else {
-        CM31 t = cinv(pre[R - 1]);
-#pragma unroll
-        for (int j = R - 1; j >= 1; --j) {
-          inv[j] = cmul(t, pre[j - 1]);
-          t = cmul(t, den[j]);
-        }
-        inv[0] = t;
-      }
-#pragma unroll
-      for (int j = 0; j < R; ++j) {
-        QM31 num = qmake(mreduce64(a[j][0]), mreduce64(a[j][1]), mreduce64(a[j][2]), mreduce64(a[j][3]));
-        num = qsub(num, qadd(qmulm(bt.sum_a, dp[j].y), bt.sum_b));
-        acc[j] = qadd(acc[j], qmulc(num, inv[j]));
-      }
+      quot_batch_finish<R>(bt, dp, a, acc);
     }
     uint32_t w[R];
 #pragma unroll
@@ -497,6 +510,254 @@ __global__ void __launch_bounds__(256, MINB) k_quotients_v(PointTable pts, uint3
     for (int j = 0; j < R; ++j) w[j] = acc[j].c1.b;
     V::store(out + 3 * out_stride + row0, w);
   }
+}
+
+// ---- Quotients with the column words staged in shared memory by bulk async copies ----------
+// Warp-specialized: eight consumer warps own a tile of QB_ROWS rows (two per thread); a ninth,
+// producer warp streams the tile's column chunks (2 KB each) into a ring of QB_STAGES stages of
+// QB_GROUP columns with 1-D bulk copies (cp.async.bulk global -> shared, one chunk per lane,
+// completing on the stage's `full` mbarrier with the stage's byte count). A consumer warp waits on
+// `full`, reads its threads' two words of each column, and arrives on the stage's `empty` mbarrier;
+// the producer refills a stage once all eight consumer warps have arrived. The loads of the stages
+// ahead stay in flight while one is consumed, without the registers the register kernel's loads in
+// flight take, and the producer never holds the consumers at a block barrier. Items run batch by
+// batch (a batch's entries in groups of at most QB_GROUP); the last group of a batch adds the
+// batch's quotient. Each wait is bounded (about a second of the global timer): a side that runs out
+// sets QUOT_STATUS_TIMEOUT in *status and a shared abort flag that ends the other side's loop; the
+// producer then waits (again bounded) for the copies it issued. Batches that reach past the
+// n_entries columns, or more groups than the item table holds, set QUOT_STATUS_LAYOUT before any
+// copy is issued.
+constexpr uint32_t QB_ROWS = 512, QB_GROUP = 8, QB_STAGES = 4, QB_MAX_BATCHES = 64;
+constexpr uint32_t QB_CONSUMER_WARPS = QB_ROWS / 2 / 32, QB_THREADS = (QB_CONSUMER_WARPS + 1) * 32;
+constexpr uint64_t QB_WAIT_NS = 1000000000ull;
+// A test hook: the next bulk quotient launch issues no copy for its first item, so that every wait
+// on that stage runs out.
+std::atomic<bool> g_quot_skip_first_item{false};
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+__device__ __forceinline__ uint64_t global_ns() {
+  uint64_t t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t* bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+// 1-D bulk copy of `bytes` (a multiple of 16, both addresses 16-byte aligned) into this CTA's shared
+// memory; its completion counts against the barrier's expected bytes.
+__device__ __forceinline__ void bulk_load(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
+               ::"r"(smem_u32(dst)), "l"(src), "r"(bytes), "r"(smem_u32(bar)) : "memory");
+}
+// Waits for the completion of phase `parity` of the barrier for at most QB_WAIT_NS, or until *abort
+// is set; false unless the phase completed.
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity, const volatile int* abort) {
+  const uint32_t a = smem_u32(bar);
+  const uint64_t t0 = global_ns();
+  for (uint32_t it = 0;; ++it) {
+    uint32_t done;
+    asm volatile("{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+                 "selp.u32 %0, 1, 0, p;\n\t}"
+                 : "=r"(done) : "r"(a), "r"(parity) : "memory");
+    if (done) return true;
+    // The clock and the abort flag are looked at every 64th try only (try_wait itself suspends).
+    if ((it & 63) == 63 && ((abort && *abort) || global_ns() - t0 > QB_WAIT_NS)) return false;
+  }
+}
+
+struct QbItem {
+  uint32_t e0;     // first entry of the group
+  uint16_t ne;     // entries in the group (0 .. QB_GROUP; 0 only for a batch without entries)
+  uint16_t batch;  // 1 + the batch index when the group is its batch's last, else 0
+};
+
+template <int MINB>
+__global__ void __launch_bounds__(QB_THREADS, MINB) k_quotients_bulk(PointTable pts, uint32_t log_size,
+                                                                     uint32_t n_batches,
+                                                                     const QuotientBatchDev* __restrict__ batches,
+                                                                     const uint32_t* const* __restrict__ col_ptrs,
+                                                                     const QM31* __restrict__ coeff_c,
+                                                                     uint32_t n_entries, uint32_t item_cap,
+                                                                     uint32_t* out, uint64_t out_stride,
+                                                                     uint32_t* status, int skip_first_item) {
+  constexpr int R = 2;
+  extern __shared__ __align__(16) uint8_t qsm[];
+  uint32_t* ring = reinterpret_cast<uint32_t*>(qsm);                     // QB_STAGES x QB_GROUP x QB_ROWS words
+  uint4* sq = reinterpret_cast<uint4*>(ring + QB_STAGES * QB_GROUP * QB_ROWS);  // n_entries coefficients
+  const uint32_t** sptr = reinterpret_cast<const uint32_t**>(sq + n_entries);  // n_entries column pointers
+  QbItem* items = reinterpret_cast<QbItem*>(sptr + n_entries);                 // item_cap groups of one tile
+  __shared__ uint64_t full[QB_STAGES], empty[QB_STAGES];
+  __shared__ QuotientBatchDev sbt[QB_MAX_BATCHES];
+  __shared__ int s_abort;
+  __shared__ uint32_t s_items;
+  const uint32_t tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  for (uint32_t i = tid; i < n_entries; i += blockDim.x) {
+    const QM31 c = coeff_c[i];
+    sq[i] = make_uint4(c.c0.a, c.c0.b, c.c1.a, c.c1.b);
+    sptr[i] = col_ptrs[i];
+  }
+  for (uint32_t b = tid; b < n_batches; b += blockDim.x) sbt[b] = batches[b];
+  if (tid == 0) {
+    uint32_t k = 0;
+    bool bad = n_batches > QB_MAX_BATCHES;
+    for (uint32_t b = 0; b < n_batches && !bad; ++b) {
+      const uint32_t first = batches[b].first, count = batches[b].count;
+      if (first > n_entries || count > n_entries - first) {
+        bad = true;
+        break;
+      }
+      // A batch without entries still adds its linear term: one empty group.
+      for (uint32_t g = 0; g < count || (count == 0 && g == 0); g += QB_GROUP) {
+        if (k == item_cap) {
+          bad = true;
+          break;
+        }
+        const uint32_t ne = min(QB_GROUP, count - g);
+        items[k++] = QbItem{first + g, (uint16_t)ne, (uint16_t)(g + ne == count ? b + 1 : 0)};
+      }
+    }
+    for (uint32_t s = 0; s < QB_STAGES; ++s) {
+      mbar_init(&full[s], 1);
+      mbar_init(&empty[s], QB_CONSUMER_WARPS);
+    }
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    s_items = k;
+    s_abort = bad ? 1 : 0;
+    if (bad) atomicOr(status, QUOT_STATUS_LAYOUT);
+  }
+  __syncthreads();
+  if (s_abort) return;  // nothing issued
+  const uint32_t n_items = s_items;
+  const uint32_t n_tiles = (1u << log_size) / QB_ROWS;
+  const uint32_t my_tiles = blockIdx.x < n_tiles ? (n_tiles - 1 - blockIdx.x) / gridDim.x + 1 : 0;
+  const uint64_t total = (uint64_t)my_tiles * n_items;
+  volatile int* abort = &s_abort;
+
+  if (warp == QB_CONSUMER_WARPS) {
+    // Producer warp: item i (tile-major, groups minor) into stage i % QB_STAGES, lane k copying the
+    // group's k-th column chunk.
+    uint64_t i = 0;
+    bool ok = true;
+    for (; i < total; ++i) {
+      const uint32_t s = (uint32_t)(i % QB_STAGES);
+      // Every lane waits (each acquires the consumers' release); the warp decides together.
+      const bool got = i < QB_STAGES || mbar_wait_bounded(&empty[s], (uint32_t)(i / QB_STAGES - 1) & 1, abort);
+      if (!__all_sync(0xffffffffu, got)) {
+        ok = false;
+        break;
+      }
+      if (skip_first_item && i == 0) continue;
+      const uint32_t tile = blockIdx.x + (uint32_t)(i / n_items) * gridDim.x;
+      const QbItem it = items[i % n_items];
+      uint32_t* dst = ring + s * (QB_GROUP * QB_ROWS);
+      if (lane == 0) {
+        // The stage's words were last read through the generic proxy; order those reads before the
+        // async-proxy writes of its refill.
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        mbar_arrive_expect_tx(&full[s], it.ne * QB_ROWS * 4);
+      }
+      __syncwarp();
+      if (lane < it.ne)
+        bulk_load(dst + lane * QB_ROWS, sptr[it.e0 + lane] + (uint64_t)tile * QB_ROWS, QB_ROWS * 4, &full[s]);
+    }
+    if (lane == 0) {
+      if (!ok) {
+        *abort = 1;
+        atomicOr(status, QUOT_STATUS_TIMEOUT);
+      }
+      // Items i - QB_STAGES .. i - 1 are the last ones issued (earlier ones were consumed before
+      // their stages were refilled): let their copies land before the CTA's shared memory is
+      // released, also when the consumers stopped early (bounded, the abort flag ignored).
+      const uint64_t from = i > QB_STAGES ? i - QB_STAGES : 0;
+      for (uint64_t j = from; j < i; ++j)
+        if (!(skip_first_item && j == 0)) mbar_wait_bounded(&full[j % QB_STAGES], (uint32_t)(j / QB_STAGES) & 1, nullptr);
+    }
+  } else {
+    const CircleDomain dom = canonic_domain(log_size);
+    uint64_t item = 0;
+    bool ok = true;
+    for (uint32_t q = 0; q < my_tiles && ok; ++q) {
+      const uint32_t row0 = (blockIdx.x + q * gridDim.x) * QB_ROWS + R * tid;
+      PointM dp[R];
+#pragma unroll
+      for (int j = 0; j < R; ++j) dp[j] = pts.at(dom.index_at(bitrev(row0 + j, log_size)));
+      QM31 acc[R];
+#pragma unroll
+      for (int j = 0; j < R; ++j) acc[j] = qzero();
+      uint64_t a[R][4];
+#pragma unroll
+      for (int j = 0; j < R; ++j)
+#pragma unroll
+        for (int c = 0; c < 4; ++c) a[j][c] = 0;
+      for (uint32_t g = 0; g < n_items; ++g, ++item) {
+        const uint32_t s = (uint32_t)(item % QB_STAGES);
+        // Every lane waits (each acquires the copies' completion); the warp decides together.
+        if (!__all_sync(0xffffffffu, mbar_wait_bounded(&full[s], (uint32_t)(item / QB_STAGES) & 1, abort))) {
+          ok = false;
+          break;
+        }
+        const QbItem it = items[g];
+        const uint32_t* col = ring + s * (QB_GROUP * QB_ROWS) + R * tid;
+        const uint4* cq = sq + it.e0;
+        // Terms of a group are folded after its entries 2, 5 and 7 (and after its last): at most
+        // three products (< 2^62 each) on top of a folded value (< 2^34) between folds.
+        auto term = [&](uint32_t k) {
+          const uint2 v = *reinterpret_cast<const uint2*>(col + k * QB_ROWS);
+          const uint4 c = cq[k];
+          a[0][0] += (uint64_t)c.x * v.x; a[0][1] += (uint64_t)c.y * v.x;
+          a[0][2] += (uint64_t)c.z * v.x; a[0][3] += (uint64_t)c.w * v.x;
+          a[1][0] += (uint64_t)c.x * v.y; a[1][1] += (uint64_t)c.y * v.y;
+          a[1][2] += (uint64_t)c.z * v.y; a[1][3] += (uint64_t)c.w * v.y;
+        };
+        auto fold = [&]() {
+#pragma unroll
+          for (int j = 0; j < R; ++j)
+#pragma unroll
+            for (int c4 = 0; c4 < 4; ++c4) a[j][c4] = mfold64(a[j][c4]);
+        };
+        if (it.ne == QB_GROUP) {
+#pragma unroll
+          for (uint32_t k = 0; k < QB_GROUP; ++k) {
+            term(k);
+            if (k == 2 || k == 5 || k == 7) fold();
+          }
+        } else {
+          for (uint32_t k = 0; k < it.ne; ++k) {
+            term(k);
+            if (k == 2 || k == 5 || k + 1 == it.ne) fold();
+          }
+        }
+        // This warp is done with the stage's words.
+        __syncwarp();
+        if (lane == 0) mbar_arrive(&empty[s]);
+        if (it.batch) {
+          quot_batch_finish<R>(sbt[it.batch - 1], dp, a, acc);
+#pragma unroll
+          for (int j = 0; j < R; ++j)
+#pragma unroll
+            for (int c4 = 0; c4 < 4; ++c4) a[j][c4] = 0;
+        }
+      }
+      if (!ok) break;
+      const uint32_t w0[4] = {acc[0].c0.a, acc[0].c0.b, acc[0].c1.a, acc[0].c1.b};
+      const uint32_t w1[4] = {acc[1].c0.a, acc[1].c0.b, acc[1].c1.a, acc[1].c1.b};
+#pragma unroll
+      for (int c4 = 0; c4 < 4; ++c4)
+        *reinterpret_cast<uint2*>(out + c4 * out_stride + row0) = make_uint2(w0[c4], w1[c4]);
+    }
+    if (!ok) {
+      *abort = 1;
+      if (lane == 0) atomicOr(status, QUOT_STATUS_TIMEOUT);
+    }
+  }
+  // The producer's bounded wait for its own copies ends before any thread of the CTA exits.
+  __syncthreads();
 }
 
 // ---------------------------------------------------------------------------
@@ -642,10 +903,10 @@ cudaError_t eval_at_point(const DeviceTables&, uint32_t log_size, uint32_t n_col
   }
   uint32_t chunk_bits = log_size < OODS_CHUNK_BITS ? log_size : OODS_CHUNK_BITS;
   uint32_t n_chunks = 1u << (log_size - chunk_bits);
-  // About 8 CTAs per SM over all columns, never more CTAs per column than chunks.
-  uint32_t per_col = (148 * 8 + n_cols - 1) / n_cols;
-  if (per_col > n_chunks) per_col = n_chunks;
-  if (per_col < 1) per_col = 1;
+  // A power of two of CTAs per column (the chunk factor splits over the CTA's bits): about four
+  // waves of five CTAs per SM over all columns, never more CTAs per column than chunks.
+  uint32_t per_col = 1;
+  while (per_col < n_chunks && (uint64_t)per_col * n_cols < 148ull * 5 * 4) per_col <<= 1;
   dim3 grid(per_col, n_cols);
   k_oods_chunks<<<grid, OODS_THREADS, 0, stream>>>(F, coeffs, stride, partial, n_chunks); note_launch();
   cudaError_t e = cudaGetLastError();
@@ -659,16 +920,28 @@ static void quotients_smem_attr(size_t smem_v) {
   cudaFuncSetAttribute(k_quotients_v<R, U, MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_v);
 }
 
+void arm_quotient_stage_timeout_for_testing() { g_quot_skip_first_item.store(true); }
+
 cudaError_t accumulate_quotients(const DeviceTables& t, uint32_t log_size, uint32_t n_batches, uint32_t n_entries,
                                  const QuotientBatchDev* batches, const uint32_t* const* col_ptrs, const QM31* coeff_c,
-                                 uint32_t* out, uint64_t out_stride, cudaStream_t stream) {
+                                 uint32_t* out, uint64_t out_stride, cudaStream_t stream, uint32_t* status) {
   size_t smem = QUOT_MAX_ENTRIES * 16;
   size_t smem_v = QUOT_MAX_ENTRIES * (16 + sizeof(void*));
+  // Bulk-staged kernel: the ring, the coefficients and pointers, and the item table (every batch
+  // adds at most one partial group).
+  const uint32_t item_cap = (n_entries + QB_GROUP - 1) / QB_GROUP + n_batches;
+  const size_t smem_b = (size_t)QB_STAGES * QB_GROUP * QB_ROWS * 4 + (size_t)n_entries * (16 + sizeof(void*)) +
+                        (size_t)item_cap * sizeof(QbItem);
+  constexpr size_t SMEM_B_MAX = (size_t)QB_STAGES * QB_GROUP * QB_ROWS * 4 +
+                                (size_t)QUOT_MAX_ENTRIES * (16 + sizeof(void*)) +
+                                (size_t)(QUOT_MAX_ENTRIES / QB_GROUP + QB_MAX_BATCHES) * sizeof(QbItem);
   static const bool attr = [&] {  // once per process (thread-safe static initialisation)
     cudaFuncSetAttribute(k_quotients, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     quotients_smem_attr<QUOT_R, QUOT_U, 3>(smem_v);
     quotients_smem_attr<QUOT_R, 3, 4>(smem_v);
     quotients_smem_attr<QUOT_R, 9, 2>(smem_v);
+    cudaFuncSetAttribute(k_quotients_bulk<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM_B_MAX);
+    cudaFuncSetAttribute(k_quotients_bulk<3>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM_B_MAX);
     return true;
   }();
   (void)attr;
@@ -680,8 +953,13 @@ cudaError_t accumulate_quotients(const DeviceTables& t, uint32_t log_size, uint3
     note_launch();
     return cudaGetLastError();
   }
-  // Variants: 6 loads in flight per thread at 3 CTAs per SM, 3 at 4, 9 at 2.
+  // The bulk-staged kernel takes whole 512-row tiles of 16-byte aligned columns (the caller vouches
+  // for the pointers by passing `status`).
+  const bool bulk = status != nullptr && log_size >= 16 && n_batches <= QB_MAX_BATCHES &&
+                    n_entries <= QUOT_MAX_ENTRIES;
+  // Variants: 6 loads in flight per thread at 3 CTAs per SM, 3 at 4, 9 at 2; bulk-staged.
   auto run = [&](int variant) -> cudaError_t {
+    if (variant == 3 && !bulk) variant = 0;  // a key tuned by a caller that could take it
     const dim3 grid(grid_for(1ull << log_size, 256 * QUOT_R));
     const PointTable pts{t.points};
     if (variant == 1)
@@ -690,14 +968,26 @@ cudaError_t accumulate_quotients(const DeviceTables& t, uint32_t log_size, uint3
     else if (variant == 2)
       k_quotients_v<QUOT_R, 9, 2><<<grid, 256, smem_v, stream>>>(pts, log_size, n_batches, batches, col_ptrs, coeff_c,
                                                                    out, out_stride);
-    else
+    else if (variant == 3) {
+      // Persistent: as many CTAs as stay resident (three per SM while the shared memory allows).
+      const int minb = smem_b <= 70 * 1024 ? 3 : 2;
+      const uint32_t n_tiles = (uint32_t)((1ull << log_size) / QB_ROWS);
+      const uint32_t g = std::min<uint32_t>(n_tiles, t.sm_count * (uint32_t)minb);
+      const int skip = g_quot_skip_first_item.exchange(false) ? 1 : 0;
+      if (minb == 3)
+        k_quotients_bulk<3><<<g, QB_THREADS, smem_b, stream>>>(pts, log_size, n_batches, batches, col_ptrs, coeff_c, n_entries,
+                                                        item_cap, out, out_stride, status, skip);
+      else
+        k_quotients_bulk<2><<<g, QB_THREADS, smem_b, stream>>>(pts, log_size, n_batches, batches, col_ptrs, coeff_c, n_entries,
+                                                        item_cap, out, out_stride, status, skip);
+    } else
       k_quotients_v<QUOT_R, QUOT_U, 3><<<grid, 256, smem_v, stream>>>(pts, log_size, n_batches, batches, col_ptrs,
                                                                       coeff_c, out, out_stride);
     note_launch();
     return cudaGetLastError();
   };
   // Reads the columns, writes `out`: re-runnable. Keyed by the committed columns read per row.
-  return tuned_run(TUNE_QUOTIENTS, log_size, n_entries, log_size >= 16 ? 3 : 1, true, stream, run);
+  return tuned_run(TUNE_QUOTIENTS, log_size, n_entries, log_size >= 16 ? (bulk ? 4 : 3) : 1, true, stream, run);
 }
 
 cudaError_t fold_circle_into_line(const DeviceTables& t, uint32_t src_log, const uint32_t* src, uint64_t src_stride,

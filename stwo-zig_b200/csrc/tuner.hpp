@@ -19,7 +19,7 @@ namespace sb {
 enum TuneOp : uint32_t {
   TUNE_LDE1 = 0,       // interpolate + blow-up-2 extension of 2^16 .. 2^22 columns: fused, generic high pass
   TUNE_LEAVES = 1,     // Merkle leaf kernel: 5, 6, 4 CTAs per SM
-  TUNE_QUOTIENTS = 2,  // DEEP quotients: 6 loads in flight at 3 CTAs/SM, 3 at 4, 9 at 2
+  TUNE_QUOTIENTS = 2,  // DEEP quotients: 6 loads in flight at 3 CTAs/SM, 3 at 4, 9 at 2; bulk-staged
   TUNE_OPS = 3,
 };
 constexpr int TUNE_MAX_VARIANTS = 4;

@@ -537,7 +537,13 @@ int32_t LogupXorProver::prove(const XorRequest& req, std::string& out) {
     SB_CK(cudaMemcpyAsync(b.quot_c, hc, at * sizeof(QM31), cudaMemcpyHostToDevice, fs));
     SB_CK(cudaMemcpyAsync(b.col_ptrs, hp, at * sizeof(void*), cudaMemcpyHostToDevice, fs));
     SB_CK(cudaMemcpyAsync(b.batch, hb, batches.size() * sizeof(QuotientBatchDev), cudaMemcpyHostToDevice, fs));
-    SB_CK(accumulate_quotients(T, LDE, (uint32_t)batches.size(), at, b.batch, b.col_ptrs, b.quot_c, b.quot, NL, fs));
+    // Columns that all start 16-byte aligned may go through the bulk-staged quotient kernel, its
+    // status read back with the FRI channel.
+    bool aligned = true;
+    for (uint32_t i = 0; i < at; ++i) aligned = aligned && (reinterpret_cast<uintptr_t>(hp[i]) & 15) == 0;
+    SB_CK(cudaMemsetAsync(&b.chan->quot_status, 0, sizeof(uint32_t), fs));
+    SB_CK(accumulate_quotients(T, LDE, (uint32_t)batches.size(), at, b.batch, b.col_ptrs, b.quot_c, b.quot, NL, fs,
+                               aligned ? &b.chan->quot_status : nullptr));
   }
 
   // Tail: FRI, proof of work, queries, decommitment.

@@ -134,6 +134,7 @@ _SIGS = {
     "stwo_b200_server_destroy": [_vp],
     "stwo_b200_server_set_request_timeout": [_vp, _u32],
     "stwo_b200_arm_allocation_failure_for_testing": [_u32],
+    "stwo_b200_arm_quotient_stage_timeout_for_testing": [],
     "stwo_b200_autotune_mode": [_i32],
     "stwo_b200_autotune_wide_fibonacci": [_vp, _u32, _u32, _u32],
     "stwo_b200_autotune_table": [_vp, ctypes.c_size_t, ctypes.POINTER(ctypes.c_size_t)],
@@ -609,8 +610,14 @@ def arm_allocation_failure_for_testing(nth: int) -> None:
     _check(_lib.stwo_b200_arm_allocation_failure_for_testing(nth))
 
 
+def arm_quotient_stage_timeout_for_testing() -> None:
+    """Makes the next bulk-staged quotient launch leave its first stage empty: its bounded waits run
+    out (about a second), and the proof or op fails with E_CUDA; no GPU fault is involved."""
+    _check(_lib.stwo_b200_arm_quotient_stage_timeout_for_testing())
+
+
 AUTOTUNE_OPS = {0: "interpolate+extend high pass (fused, generic)", 1: "Merkle leaves (5, 6, 4 CTAs/SM)",
-                2: "DEEP quotients (6, 3, 9 loads in flight)"}
+                2: "DEEP quotients (6, 3, 9 loads in flight; bulk-staged)"}
 
 
 def autotune_mode(mode: int) -> None:

@@ -34,7 +34,7 @@ def forced():
     sb.autotune_mode(-1)
 
 
-@pytest.mark.parametrize("variant", [0, 1, 2])
+@pytest.mark.parametrize("variant", [0, 1, 2, 3])
 def test_every_variant_is_exact(ctx, forced, variant):
     import torch
     forced(variant)

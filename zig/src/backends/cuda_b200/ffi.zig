@@ -323,3 +323,4 @@ pub extern fn stwo_b200_autotune_table(out: ?[*]TuneEntry, cap: usize, n: *usize
 // ---------------------------------------------------------------
 
 pub extern fn stwo_b200_arm_allocation_failure_for_testing(nth: u32) i32;
+pub extern fn stwo_b200_arm_quotient_stage_timeout_for_testing() i32;
