@@ -443,8 +443,10 @@ int32_t stwo_b200_pow_grind(stwo_b200_context* ctx, const uint8_t prefix_digest[
 
 /* Launch-shape autotuner of the kernels that come in variants writing the same bits (op 0: the
  * interpolate + blow-up-2 high pass, fused or generic; op 1: the Merkle leaf kernel at 5, 6 or 4 CTAs
- * per SM; op 2: the DEEP quotient kernel at 6, 3 or 9 loads in flight), keyed by (op, log_size,
- * n_cols) for the process. A key's first call times every variant on its own inputs with CUDA events
+ * per SM; op 2: the DEEP quotient kernel at 6, 3 or 9 loads in flight, and, for callers whose
+ * columns are 16-byte aligned (the provers, and the op-level call after it reads the column pointers
+ * back), the bulk-staged kernel that streams column chunks into shared memory with bulk async
+ * copies), keyed by (op, log_size, n_cols) for the process. A key's first call times every variant on its own inputs with CUDA events
  * and keeps the fastest; later calls run it. The north star's autotuner cached per
  * (log_size, n_columns); the reference has none (its Metal backend fixes its launch shapes).
  * mode -1 (the default) tunes; mode v >= 0 runs variant v of every op (the last one where an op has
