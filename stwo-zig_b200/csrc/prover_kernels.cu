@@ -656,12 +656,10 @@ __global__ void __launch_bounds__(QB_THREADS, MINB) k_quotients_bulk(PointTable 
       const uint32_t tile = blockIdx.x + (uint32_t)(i / n_items) * gridDim.x;
       const QbItem it = items[i % n_items];
       uint32_t* dst = ring + s * (QB_GROUP * QB_ROWS);
-      if (lane == 0) {
-        // The stage's words were last read through the generic proxy; order those reads before the
-        // async-proxy writes of its refill.
-        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-        mbar_arrive_expect_tx(&full[s], it.ne * QB_ROWS * 4);
-      }
+      // The stage's words were last read through the generic proxy; every lane that issues a copy
+      // orders those reads before the async-proxy writes of its refill.
+      asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+      if (lane == 0) mbar_arrive_expect_tx(&full[s], it.ne * QB_ROWS * 4);
       __syncwarp();
       if (lane < it.ne)
         bulk_load(dst + lane * QB_ROWS, sptr[it.e0 + lane] + (uint64_t)tile * QB_ROWS, QB_ROWS * 4, &full[s]);
