@@ -171,6 +171,8 @@ void DecommitPlan::add_tree(const uint8_t* layers, uint32_t max_log, const std::
   n_queries_ = queries.size();
   tp.word0 = words_.size();
   tp.n_cols = cols.size();
+  words_.reserve(words_.size() + cols.size() * queries.size());
+  if (!cols.empty()) hashes_.reserve(hashes_.size() + queries.size() * max_log);
   for (const uint32_t* c : cols)
     for (uint64_t q : queries) words_.push_back({c, q});
   tp.hash0 = hashes_.size();
@@ -186,6 +188,11 @@ void DecommitPlan::add_tree(const uint8_t* layers, uint32_t max_log, const std::
 
 void DecommitPlan::add_fri(const FriBuffers& fb, uint32_t L, uint32_t n_inner, const std::vector<uint64_t>& queries) {
   std::vector<uint64_t> lq = queries;
+  // At most two positions per query and layer: four coordinate words each, and their witnesses.
+  words_.reserve(words_.size() + (size_t)(n_inner + 1) * 8 * queries.size());
+  hashes_.reserve(hashes_.size() + (size_t)(n_inner + 1) * 2 * queries.size() * L);
+  std::vector<uint64_t> positions;
+  positions.reserve(2 * queries.size());
   for (uint32_t k = 0; k <= n_inner; ++k) {
     // k = 0: first layer (quotient column, log L); k >= 1: inner layer k-1.
     const uint32_t* colbase = k == 0 ? fb.quot : fb.line[k - 1];
@@ -193,7 +200,7 @@ void DecommitPlan::add_fri(const FriBuffers& fb, uint32_t L, uint32_t n_inner, c
     uint32_t lg = k == 0 ? L : L - k;
     const uint8_t* tree = k == 0 ? fb.tree_q : fb.line_tree[k - 1];
     LayerPlan lp{words_.size(), 0, hashes_.size(), 0};
-    std::vector<uint64_t> positions;
+    positions.clear();
     size_t q = 0;
     while (q < lq.size()) {
       uint64_t key = lq[q] >> 1;

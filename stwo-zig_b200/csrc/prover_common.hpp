@@ -206,6 +206,8 @@ class Json {
 // whose hashes are witnesses, in proof order (src/prover/vcs_lifted/decommit.zig:154-230).
 inline std::vector<uint64_t> witness_nodes(uint32_t max_log, const std::vector<uint64_t>& positions) {
   std::vector<uint64_t> out, prev = positions, cur;
+  out.reserve(positions.size() * max_log);
+  cur.reserve(positions.size());
   for (int layer = (int)max_log - 1; layer >= 0; --layer) {
     cur.clear();
     size_t q = 0;
