@@ -1,4 +1,4 @@
-"""The bulk-staged DEEP quotient kernel, the quotient op's fourth launch variant: a CTA streams
+"""The DEEP quotient op's launch variants, above all the bulk-staged kernel (the fourth): a CTA streams
 512-row chunks of its columns into a shared-memory ring with 1-D bulk async copies completing on
 mbarriers. Proofs through it equal the oracle's bytes (one batch of 24 to 1008 entries, entry counts
 that are not a multiple of the 8-column group, the XOR-lookup AIR's several batches), the op agrees
@@ -48,6 +48,20 @@ def test_xor_proofs_through_the_staged_kernel_equal_the_oracle(ctx, staged, log_
         oracle.prove_logup_xor(log_n, o, seed=seed, log_table=log_table, channel_seed=chan)
 
 
+@pytest.mark.parametrize("variant", [1, 2])
+def test_xor_proofs_through_the_other_quotient_variants_equal_the_oracle(ctx, variant):
+    """The XOR-lookup AIR's quotients come in several batches: the register variants with 3 and 9
+    loads in flight against the oracle's bytes."""
+    import stwo_b200 as sb
+    o, g = _cfg("functional")
+    try:
+        sb.autotune_mode(variant)
+        got = ctx.prove_logup_xor(16, g, seed=77, log_table=16, channel_seed=5)
+    finally:
+        sb.autotune_mode(-1)
+    assert got == oracle.prove_logup_xor(16, o, seed=77, log_table=16, channel_seed=5)
+
+
 def _quotient_case(n_cols, log):
     import torch
     rng = np.random.default_rng(4000 + n_cols)
@@ -60,14 +74,15 @@ def _quotient_case(n_cols, log):
 
 
 @pytest.mark.parametrize("n_cols", [1, 8, 13, 108])
-def test_quotient_op_staged_equals_register_kernel(ctx, n_cols):
+def test_quotient_op_variants_equal_the_register_kernel(ctx, n_cols):
+    """Every quotient variant writes the first variant's words at the op level."""
     import stwo_b200 as sb
     import torch
     log = 17
     cols, ptrs, coeffs, (px, py, sa, sbb) = _quotient_case(n_cols, log)
     outs = []
     try:
-        for v in (0, STAGED):
+        for v in (0, 1, 2, STAGED):
             sb.autotune_mode(v)
             out = torch.empty(4 << log, dtype=torch.int32, device="cuda")
             ctx.accumulate_quotients(log, ptrs, coeffs, px, py, sa, sbb, out, n_cols)
@@ -75,7 +90,8 @@ def test_quotient_op_staged_equals_register_kernel(ctx, n_cols):
             outs.append(out.cpu().numpy())
     finally:
         sb.autotune_mode(-1)
-    assert np.array_equal(outs[0], outs[1])
+    for o in outs[1:]:
+        assert np.array_equal(outs[0], o)
     del cols
 
 
