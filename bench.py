@@ -697,8 +697,14 @@ def run_serve(args, ctx):
 
     for shape in sorted({(r["log_n"], r["W"]) for r in stmts if not r["xor"]}):
         ctx.autotune_wide_fibonacci(shape[0], shape[1], cfg.fri_config.log_blowup_factor)
-    for r in stmts[:4]:
-        single(r)
+    # One untimed proof of every distinct request shape: the XOR-lookup shapes' launch variants are
+    # tuned here, not inside the timed single-proof pass.
+    seen = set()
+    for r in stmts:
+        key = (r["xor"], r["log_n"], r.get("W"))
+        if key not in seen:
+            seen.add(key)
+            single(r)
     t0 = time.perf_counter()
     alone = [single(r) for r in stmts]
     single_s = time.perf_counter() - t0
