@@ -215,7 +215,8 @@ int32_t stwo_b200_server_wait(stwo_b200_server* server, uint64_t ticket, uint8_t
 /* Sizes every slot for the largest shapes it will serve (the reference's warmup / initializeRuntime
  * hooks, src/prover/engine.zig): persistent workspaces grow to 2^max_log_n_rows x max_sequence_len
  * (within the memory budget), and the stream-ordered pool is pre-grown for transient workspaces and
- * XOR-lookup proofs of up to 2^max_xor_log_n rows (0: none). Call while the server is idle. */
+ * XOR-lookup proofs of up to 2^max_xor_log_n rows (0: none), whose provers' page-locked staging is
+ * allocated now. Call while the server is idle. */
 int32_t stwo_b200_server_warmup(stwo_b200_server* server, uint32_t max_log_n_rows, uint32_t max_sequence_len,
                                 uint32_t log_blowup, uint32_t max_xor_log_n);
 int32_t stwo_b200_server_snapshot_get(stwo_b200_server* server, stwo_b200_server_snapshot* out);

@@ -136,6 +136,8 @@ class LogupXorProver {
   explicit LogupXorProver(Context* ctx);
   ~LogupXorProver();
   int32_t prove(const XorRequest& req, std::string& proof_json);
+  // Allocates the pinned staging buffer now rather than at the first proof (E_OOM on failure).
+  int32_t reserve_staging();
   const std::string& error() const { return err_; }
   // Device workspace of one proof of this shape (bytes); 0 for an impossible shape.
   static size_t workspace_bytes(uint32_t log_n, uint32_t log_table, uint32_t log_blowup, uint32_t log_last_layer);

@@ -307,6 +307,17 @@ int32_t Server::warmup(uint32_t max_log_n_rows, uint32_t max_sequence_len, uint3
       held_[slot] = held;
     }
   }
+  // The XOR-lookup provers' pinned staging (a page-locked host allocation at a slot's first such
+  // proof otherwise, inside the serving run).
+  if (xr) {
+    for (auto* x : xor_provers_) {
+      int32_t rc = x->reserve_staging();
+      if (rc != OK) {
+        *err = x->error();
+        return rc;
+      }
+    }
+  }
   // Pre-grow the stream-ordered pool (kept: release threshold = unlimited) by what the transient
   // workspaces of a full set of slots can take at once.
   size_t per_slot = std::max(xr, persistent ? (size_t)0 : wf);

@@ -240,6 +240,17 @@ LogupXorProver::~LogupXorProver() {
   if (stream_) cudaStreamDestroy(stream_);
 }
 
+int32_t LogupXorProver::reserve_staging() {
+  if (pinned_) return OK;
+  cudaSetDevice(ctx_->device);
+  if (host_malloc_pinned(reinterpret_cast<void**>(&pinned_), PINNED_BYTES) != cudaSuccess) {
+    pinned_ = nullptr;
+    cudaGetLastError();
+    return fail(E_OOM, "pinned staging allocation failed");
+  }
+  return OK;
+}
+
 int32_t LogupXorProver::prove(const XorRequest& req, std::string& out) {
   const PcsConfig& cfg = req.config;
   const uint32_t B = cfg.log_blowup_factor;
@@ -253,11 +264,7 @@ int32_t LogupXorProver::prove(const XorRequest& req, std::string& out) {
   if (!stream_ || !fast_) return fail(E_CUDA, "stream creation failed");
   cudaSetDevice(ctx_->device);
   // Pinned staging on first use (a failed allocation leaves the prover usable for the next call).
-  if (!pinned_ && host_malloc_pinned(reinterpret_cast<void**>(&pinned_), PINNED_BYTES) != cudaSuccess) {
-    pinned_ = nullptr;
-    cudaGetLastError();
-    return fail(E_OOM, "pinned staging allocation failed");
-  }
+  if (int32_t rc = reserve_staging(); rc != OK) return rc;
   const uint64_t N = 1ull << L, NL = 1ull << LDE, NC = 1ull << CL;
   const uint32_t last_log = cfg.log_last_layer_degree_bound + B;
   const uint32_t n_inner = (LDE - 1) - last_log;
