@@ -284,7 +284,7 @@ int32_t WideFibProver::prove(const ProveRequest& req, std::string& out, StageTim
   struct TransientRelease {
     WideFibProver* p;
     ~TransientRelease() {
-      if (p->fast_) cudaStreamSynchronize(p->fast_);
+      if (p->fast_) stream_wait(p->fast_);
       if (p->transient_ && p->arena_) {
         cudaFreeAsync(p->arena_, p->stream_);
         p->arena_ = nullptr;
@@ -300,9 +300,9 @@ int32_t WideFibProver::prove(const ProveRequest& req, std::string& out, StageTim
   const DeviceTables& T = ctx_->tables;
   cudaStream_t s = stream_;
   uint8_t* pin = pinned_;
-  auto sync = [&]() -> cudaError_t { return cudaStreamSynchronize(s); };
+  auto sync = [&]() -> cudaError_t { return stream_wait(s); };
   cudaStream_t fs = fast_ ? fast_ : s;
-  auto fsync = [&]() -> cudaError_t { return cudaStreamSynchronize(fs); };
+  auto fsync = [&]() -> cudaError_t { return stream_wait(fs); };
 
   Channel ch;
   SB_CK(cudaEventRecord(ev_[0], s));
@@ -322,7 +322,7 @@ int32_t WideFibProver::prove(const ProveRequest& req, std::string& out, StageTim
     const size_t cols = first_two ? 2 : W;
     SB_CK(cudaMemcpyAsync(b.trace, req.trace_host, cols * l.N * 4, cudaMemcpyHostToDevice, s));
     SB_CK(cudaEventRecord(ev_[1], s));
-    SB_CK(cudaEventSynchronize(ev_[1]));
+    SB_CK(event_wait(ev_[1]));
   }
   if (!req.trace_host) SB_CK(cudaEventRecord(ev_[1], s));
   if (first_two || (!req.trace_device && !req.trace_host))

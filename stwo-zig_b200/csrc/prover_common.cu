@@ -51,7 +51,7 @@ int32_t fri_pow_queries(const DeviceTables& T, int sm_count, Channel& ch, const 
     // One copy back: the device channel (roots, alphas) and the last layer's values.
     SB_CKE(cudaMemcpyAsync(pin, fb.chan, sizeof(FriChannelDev), cudaMemcpyDeviceToHost, fs));
     SB_CKE(cudaMemcpyAsync(pin + LAST_OFF, fb.line[n_inner], 4 * m_last * 4, cudaMemcpyDeviceToHost, fs));
-    SB_CKE(cudaStreamSynchronize(fs));
+    SB_CKE(stream_wait(fs));
     out.gap_start = Clock::now();
     FriChannelDev dc;
     std::memcpy(&dc, pin, sizeof(dc));
@@ -136,7 +136,7 @@ int32_t fri_pow_queries(const DeviceTables& T, int sm_count, Channel& ch, const 
       for (int r = 0; r < 4 && base < max_nonce; ++r, base += per_round)
         SB_CKE(pow_round(pw, cfg.pow_bits, base, fb.pow_result, sm_count, s));
       SB_CKE(cudaMemcpyAsync(pin, fb.pow_result, 8, cudaMemcpyDeviceToHost, s));
-      SB_CKE(cudaStreamSynchronize(s));
+      SB_CKE(stream_wait(s));
       out.gap_start = Clock::now();
       std::memcpy(&nonce, pin, 8);
       if (nonce == ~0ull && deadline.passed()) {
@@ -247,7 +247,7 @@ int32_t DecommitPlan::gather(uint8_t* scratch, size_t scratch_bytes, uint8_t* pi
   SB_CKE(cudaMemcpyAsync(pin + o_outw, scratch + o_outw, o_outh - o_outw + out_hash_bytes, cudaMemcpyDeviceToHost,
                          fs));
   if (ev_done) SB_CKE(cudaEventRecord(ev_done, fs));
-  SB_CKE(cudaStreamSynchronize(fs));
+  SB_CKE(stream_wait(fs));
   gw_ = reinterpret_cast<const uint32_t*>(pin + o_outw);
   gh_ = pin + o_outh;
   return OK;

@@ -15,6 +15,7 @@
 #include <vector>
 
 #include "blake2s.cuh"
+#include "host_wait.hpp"
 #include "prover.hpp"
 
 namespace sb {

@@ -284,7 +284,7 @@ int32_t LogupXorProver::prove(const XorRequest& req, std::string& out) {
     uint8_t* p;
     cudaStream_t s, fs;
     ~Release() {
-      cudaStreamSynchronize(fs);
+      stream_wait(fs);
       cudaFreeAsync(p, s);
     }
   } release{arena_mem, s, fs};
@@ -325,7 +325,7 @@ int32_t LogupXorProver::prove(const XorRequest& req, std::string& out) {
   uint8_t roots[4][32];
   auto read_root = [&](int tr, uint64_t leaves) -> int32_t {
     SB_CK(cudaMemcpyAsync(pin, b.tree[tr] + (2 * leaves - 2) * 32, 32, cudaMemcpyDeviceToHost, s));
-    SB_CK(cudaStreamSynchronize(s));
+    SB_CK(stream_wait(s));
     std::memcpy(roots[tr], pin, 32);
     if (deadline_.passed()) return fail(E_TIMEOUT, "proof deadline passed after a commitment");
     ch.mix_root(roots[tr]);
@@ -389,7 +389,7 @@ int32_t LogupXorProver::prove(const XorRequest& req, std::string& out) {
     SB_CK(logup_interaction(lp, val(XS_ST), N, b.claimed + 1, b.logup_scratch, b.zero_flag, s));
     SB_CK(cudaMemcpyAsync(pin, b.claimed, 2 * sizeof(QM31), cudaMemcpyDeviceToHost, s));
     SB_CK(cudaMemcpyAsync(pin + 64, b.zero_flag, 4, cudaMemcpyDeviceToHost, s));
-    SB_CK(cudaStreamSynchronize(s));
+    SB_CK(stream_wait(s));
     std::memcpy(claimed, pin, 2 * sizeof(QM31));
     uint32_t zf;
     std::memcpy(&zf, pin + 64, 4);
@@ -475,7 +475,7 @@ int32_t LogupXorProver::prove(const XorRequest& req, std::string& out) {
   SB_CK(eval_at_point(T, L, 4, b.comp, NC, oods, nullptr, b.oods_partial, b.oods_out + 24, fs));
   SB_CK(eval_at_point(T, L, 4, b.comp + N, NC, oods, nullptr, b.oods_partial, b.oods_out + 28, fs));
   SB_CK(cudaMemcpyAsync(pin, b.oods_out, 32 * sizeof(QM31), cudaMemcpyDeviceToHost, fs));
-  SB_CK(cudaStreamSynchronize(fs));
+  SB_CK(stream_wait(fs));
   std::vector<QM31> at_p(32);
   std::memcpy(at_p.data(), pin, 32 * sizeof(QM31));
   auto cur_v = [&](uint32_t c) { return at_p[c]; };
