@@ -140,6 +140,16 @@ int32_t Context::init(int dev, uint32_t tower_log) {
   return OK;
 }
 
+StreamPriorities stream_priorities() {
+  StreamPriorities r;
+  if (cudaDeviceGetStreamPriorityRange(&r.least, &r.greatest) != cudaSuccess) {
+    cudaGetLastError();
+    r.least = r.greatest = 0;
+  }
+  r.bulk = r.greatest < r.least ? r.least - 1 : r.least;
+  return r;
+}
+
 WideFibProver* Context::acquire() {
   std::lock_guard<std::mutex> g(mu);
   if (!pool.empty()) {
@@ -149,7 +159,7 @@ WideFibProver* Context::acquire() {
   }
   cudaStream_t s;
   cudaSetDevice(device);
-  if (cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking) != cudaSuccess) return nullptr;
+  if (cudaStreamCreateWithPriority(&s, cudaStreamNonBlocking, stream_priorities().bulk) != cudaSuccess) return nullptr;
   return new WideFibProver(this, s);
 }
 
@@ -181,11 +191,14 @@ void Context::release_xor(LogupXorProver* p) {
 // ---------------------------------------------------------------------------
 WideFibProver::WideFibProver(Context* ctx, cudaStream_t stream) : ctx_(ctx), stream_(stream) {
   for (auto& e : ev_) cudaEventCreate(&e);
-  int least = 0, greatest = 0;
-  if (cudaDeviceGetStreamPriorityRange(&least, &greatest) != cudaSuccess ||
-      cudaStreamCreateWithPriority(&fast_, cudaStreamNonBlocking, greatest) != cudaSuccess) {
+  const StreamPriorities pr = stream_priorities();
+  if (cudaStreamCreateWithPriority(&fast_, cudaStreamNonBlocking, pr.greatest) != cudaSuccess) {
     cudaGetLastError();
     fast_ = nullptr;
+  }
+  if (cudaStreamCreateWithPriority(&pow_, cudaStreamNonBlocking, pr.least) != cudaSuccess) {
+    cudaGetLastError();
+    pow_ = nullptr;
   }
 }
 
@@ -193,6 +206,7 @@ WideFibProver::~WideFibProver() {
   release();
   for (auto& e : ev_) cudaEventDestroy(e);
   if (fast_) cudaStreamDestroy(fast_);
+  if (pow_) cudaStreamDestroy(pow_);
   if (stream_) cudaStreamDestroy(stream_);
 }
 
@@ -279,12 +293,14 @@ int32_t WideFibProver::prove(const ProveRequest& req, std::string& out, StageTim
   cudaSetDevice(ctx_->device);
   int32_t rc = ensure_workspace(n, W, B);
   if (rc != OK) return rc;
-  // On every exit path: the high-priority stream is drained (an early error return may leave
-  // its work in flight), then in transient mode the workspace goes back to the stream-ordered pool.
+  // On every exit path: the high-priority and grind streams are drained (an early error return may
+  // leave their work in flight), then in transient mode the workspace goes back to the
+  // stream-ordered pool.
   struct TransientRelease {
     WideFibProver* p;
     ~TransientRelease() {
       if (p->fast_) stream_wait(p->fast_);
+      if (p->pow_) stream_wait(p->pow_);
       if (p->transient_ && p->arena_) {
         cudaFreeAsync(p->arena_, p->stream_);
         p->arena_ = nullptr;
@@ -450,7 +466,7 @@ int32_t WideFibProver::prove(const ProveRequest& req, std::string& out, StageTim
   FriResult fr;
   {
     std::string ferr;
-    int32_t frc = fri_pow_queries(T, ctx_->sm_count, ch, cfg, l.L, l.n_inner, l.last_log, fbuf, pin, s, fs, ev_[8],
+    int32_t frc = fri_pow_queries(T, ctx_->sm_count, ch, cfg, l.L, l.n_inner, l.last_log, fbuf, pin, pow_ ? pow_ : s, fs, ev_[8],
                                   ev_[9], deadline_, fr, ferr);
     if (frc != OK) return fail(frc, ferr);
   }

@@ -108,6 +108,8 @@ class WideFibProver {
   // quotients, FRI layers with their root readbacks, decommitment): when several proofs
   // share the device, its kernels are scheduled ahead of other proofs' bulk work.
   cudaStream_t fast_ = nullptr;
+  // The proof-of-work grind's stream, at the least priority (StreamPriorities).
+  cudaStream_t pow_ = nullptr;
   std::string err_;
   // workspace
   uint8_t* arena_ = nullptr;
@@ -131,6 +133,16 @@ struct XorRequest {
 };
 
 // Prover of the LogUp XOR-lookup AIR; its workspace comes from the stream-ordered pool per proof.
+// Stream priorities of a proof's work when several proofs share the device: the latency-bound
+// chain after the composition commit at the greatest priority, the bulk stages (trace, FFTs,
+// commitments, composition) one level above the least, and the proof-of-work grind at the least,
+// so that the grind, whose launches fill every multiprocessor they are given, takes what the other
+// proofs' stages leave rather than holding them behind its waves.
+struct StreamPriorities {
+  int least = 0, greatest = 0, bulk = 0;
+};
+StreamPriorities stream_priorities();
+
 class LogupXorProver {
  public:
   explicit LogupXorProver(Context* ctx);
@@ -147,7 +159,7 @@ class LogupXorProver {
   static constexpr size_t PINNED_BYTES = (8 << 20) + (1 << 20);
   int32_t fail(int32_t code, const std::string& msg) { err_ = msg; return code; }
   Context* ctx_;
-  cudaStream_t stream_ = nullptr, fast_ = nullptr;
+  cudaStream_t stream_ = nullptr, fast_ = nullptr, pow_ = nullptr;
   uint8_t* pinned_ = nullptr;
   std::string err_;
   Deadline deadline_;

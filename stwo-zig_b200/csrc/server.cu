@@ -29,7 +29,7 @@ int32_t Server::start() {
   cudaSetDevice(ctx_->device);
   for (uint32_t i = 0; i < n_slots_; ++i) {
     cudaStream_t s;
-    if (cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking) != cudaSuccess) return E_CUDA;
+    if (cudaStreamCreateWithPriority(&s, cudaStreamNonBlocking, stream_priorities().bulk) != cudaSuccess) return E_CUDA;
     WideFibProver* p = new WideFibProver(ctx_, s);
     p->set_transient(!(flags_ & SERVER_PERSISTENT_WORKSPACES));
     provers_.push_back(p);

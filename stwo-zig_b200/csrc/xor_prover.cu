@@ -228,15 +228,16 @@ size_t LogupXorProver::workspace_bytes(uint32_t log_n, uint32_t log_table, uint3
 }
 
 LogupXorProver::LogupXorProver(Context* ctx) : ctx_(ctx) {
-  int least = 0, greatest = 0;
-  cudaDeviceGetStreamPriorityRange(&least, &greatest);
-  cudaStreamCreateWithPriority(&stream_, cudaStreamNonBlocking, least);
-  cudaStreamCreateWithPriority(&fast_, cudaStreamNonBlocking, greatest);
+  const StreamPriorities pr = stream_priorities();
+  cudaStreamCreateWithPriority(&stream_, cudaStreamNonBlocking, pr.bulk);
+  cudaStreamCreateWithPriority(&fast_, cudaStreamNonBlocking, pr.greatest);
+  cudaStreamCreateWithPriority(&pow_, cudaStreamNonBlocking, pr.least);
 }
 
 LogupXorProver::~LogupXorProver() {
   if (pinned_) cudaFreeHost(pinned_);
   if (fast_) cudaStreamDestroy(fast_);
+  if (pow_) cudaStreamDestroy(pow_);
   if (stream_) cudaStreamDestroy(stream_);
 }
 
@@ -261,7 +262,7 @@ int32_t LogupXorProver::prove(const XorRequest& req, std::string& out) {
   const uint32_t L = std::max(n, t), LDE = L + B, CL = L + 1;
   if (LDE > ctx_->tables.tower_log + 1 || cfg.log_last_layer_degree_bound + B + 1 > LDE)
     return fail(E_INVALID, "domain too large for the context or last layer too large");
-  if (!stream_ || !fast_) return fail(E_CUDA, "stream creation failed");
+  if (!stream_ || !fast_ || !pow_) return fail(E_CUDA, "stream creation failed");
   cudaSetDevice(ctx_->device);
   // Pinned staging on first use (a failed allocation leaves the prover usable for the next call).
   if (int32_t rc = reserve_staging(); rc != OK) return rc;
@@ -282,12 +283,13 @@ int32_t LogupXorProver::prove(const XorRequest& req, std::string& out) {
   }
   struct Release {
     uint8_t* p;
-    cudaStream_t s, fs;
+    cudaStream_t s, fs, ps;
     ~Release() {
       stream_wait(fs);
+      stream_wait(ps);
       cudaFreeAsync(p, s);
     }
-  } release{arena_mem, s, fs};
+  } release{arena_mem, s, fs, pow_};
   Arena arena{arena_mem, 0, need};
   XorBufs b = xor_carve(arena, shape);
   // Log size of each slot's column, and its slot pointers.
@@ -558,7 +560,7 @@ int32_t LogupXorProver::prove(const XorRequest& req, std::string& out) {
   FriResult fr;
   {
     std::string ferr;
-    int32_t frc = fri_pow_queries(T, ctx_->sm_count, ch, cfg, LDE, n_inner, last_log, fbuf, pin, s, fs, nullptr,
+    int32_t frc = fri_pow_queries(T, ctx_->sm_count, ch, cfg, LDE, n_inner, last_log, fbuf, pin, pow_ ? pow_ : s, fs, nullptr,
                                   nullptr, deadline_, fr, ferr);
     if (frc != OK) return fail(frc, ferr);
   }
