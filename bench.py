@@ -446,12 +446,12 @@ def main():
         "e2e_full_trace": {"value": world * n_full / (e2e_full_ms / 1e3), "unit": "proofs/s", "proofs": n_full,
                            "h2d_bytes_per_proof": 4 * n_words,
                            "input": "every trace column from pinned host memory (host-link bound)"},
-        "roofline": {"bound": "hbm", "kernel": "circle FFT pass: interpolate + blow-up extend (k_fft_low12<1>, "
-                     "k_fft_high16_lde1, k_fft_low12<0>)", "achieved": fft_gbs, "peak": hbm_peak, "unit": "GB/s",
+        "roofline": {"bound": "hbm", "kernel": "circle FFT pass: interpolate + blow-up extend (k_fft_low12<1, 0>, "
+                     "k_fft_high16_lde1, k_fft_low12<0, 1>)", "achieved": fft_gbs, "peak": hbm_peak, "unit": "GB/s",
                      "frac": fft_gbs / hbm_peak, "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)",
                      "traffic": FFT_TRAFFIC_BYTES.get((args.log_n, args.width)),
                      "algorithmic_bytes": fft_bytes, "ms": fft_ms},
-        "roofline_issue": ({"kernel": "circle FFT pass (k_fft_low12<1>, k_fft_high16_lde1, k_fft_low12<0>)",
+        "roofline_issue": ({"kernel": "circle FFT pass (k_fft_low12<1, 0>, k_fft_high16_lde1, k_fft_low12<0, 1>)",
                             "unit": "warp instructions/s",
                             "instructions": FFT_WARP_INSTR_PER_COL_2P20 * args.width,
                             "achieved": FFT_WARP_INSTR_PER_COL_2P20 * args.width / (fft_ms / 1e3),
@@ -786,9 +786,9 @@ def ceiling_block(measured, serial, pow_bound, note=None):
 
 
 # DRAM bytes (read + write) of one FFT pass (the 3-kernel interpolate+extend chain) from one ncu
-# capture of 2^20 rows x 40 columns (dram__bytes_read.sum + dram__bytes_write.sum = 1533.6 MB, k_fft_low12<1> + k_fft_high16_lde1<8> + k_fft_low12<0>),
-# scaled to 100 columns; traffic is linear in the column count.
-FFT_TRAFFIC_BYTES: dict = {(20, 100): 1533.6e6 * 100 / 40}
+# capture of 2^20 rows x 100 columns (dram__bytes_read.sum + dram__bytes_write.sum of k_fft_low12<1, 0>,
+# k_fft_high16_lde1<8> and k_fft_low12<0, 1>: 796.0 + 1620.3 + 1622.4 MB).
+FFT_TRAFFIC_BYTES: dict = {(20, 100): 4038.6e6}
 # Thread instructions per nonce of the grind (one ncu capture of a full 26-bit round:
 # 499.9 M warp instructions x 32 / 16,973,824 nonces).
 POW_INSTR_PER_NONCE = 943
@@ -796,8 +796,9 @@ POW_INSTR_PER_NONCE = 943
 # XORs and rotations; the additions run on the FMA pipe.
 POW_ALU_INSTR_PER_NONCE = 567
 # Warp instructions of one interpolate + blow-up extend of a 2^20 column (ncu smsp__inst_executed.sum
-# of k_fft_low12<1> + k_fft_high16_lde1<8> + k_fft_low12<0>: 203.2 M + 391.0 M + 408.4 M for 100 columns).
-FFT_WARP_INSTR_PER_COL_2P20 = 1_002_496_000 // 100
+# of k_fft_low12<1, 0> + k_fft_high16_lde1<8> + k_fft_low12<0, 1>: 203.2 M + 391.0 M + 411.7 M for 100
+# columns).
+FFT_WARP_INSTR_PER_COL_2P20 = 1_005_824_000 // 100
 
 if __name__ == "__main__":
     main()
