@@ -41,6 +41,29 @@ def test_interpolate_evaluate(ctx, log):
     assert np.array_equal(host(d).reshape(n_cols, -1), cols)
 
 
+@pytest.mark.parametrize("log", [16, 20])
+def test_interpolate_evaluate_padded_columns(ctx, log):
+    """Columns `stride` words apart with a gap between them (the forward pass stores its blocks with
+    a tensor copy whose map carries the stride): the transforms equal the oracle's and the gap words
+    keep their values."""
+    import torch
+    rng = np.random.default_rng(900 + log)
+    n_cols, pad = 3, 256
+    stride = (1 << log) + pad
+    cols = rand_cols(rng, n_cols, log)
+    buf = np.full((n_cols, stride), 0x5A5A5A5A, dtype=np.uint32)
+    buf[:, : 1 << log] = cols
+    d = torch.from_numpy(buf.reshape(-1).view(np.int32)).cuda()
+    ctx.interpolate(d, log, n_cols, stride)
+    got = host(d).reshape(n_cols, stride)
+    for c in range(n_cols):
+        assert np.array_equal(got[c, : 1 << log], oracle.interpolate(cols[c])), c
+    ctx.evaluate(d, log, n_cols, stride)
+    got = host(d).reshape(n_cols, stride)
+    assert np.array_equal(got[:, : 1 << log], cols)
+    assert (got[:, 1 << log:] == 0x5A5A5A5A).all()
+
+
 @pytest.mark.parametrize("log,blowup", [(1, 1), (3, 1), (10, 1), (11, 1), (12, 1), (15, 1), (16, 1), (17, 1),
                                         (18, 1), (19, 1), (20, 1), (21, 1), (22, 1), (12, 2), (16, 2), (18, 3),
                                         (5, 3)])
